@@ -1,0 +1,191 @@
+/*
+ * pytme_b200 C ABI: the exhaustive template-matching hot path of pyTME on
+ * NVIDIA B200 (sm_100a).
+ *
+ * Conventions
+ *   - Every function returns an int status: TM_OK (0) or a negative TM_E_* code;
+ *     tm_last_error() returns the message of the calling thread's last failure.
+ *   - Buffers are raw device pointers owned by the caller, C-contiguous,
+ *     float32 unless stated otherwise. Shapes are (axis 0, axis 1, axis 2) with
+ *     axis 2 fastest, the layout of a C-ordered NumPy array.
+ *   - Work is enqueued on the caller's CUDA stream (`stream`, a cudaStream_t
+ *     passed as void*; NULL is the legacy default stream) and is asynchronous
+ *     unless a function says it synchronises.
+ *   - A tm_scan plan owns its scratch memory and cuFFT plans; it may be used
+ *     from one host thread at a time.
+ *
+ * Each entry point names the reference interface (KosinskiLab/pyTME 0.3.b0,
+ * paths inside that project) whose behaviour it provides.
+ */
+#ifndef PYTME_B200_H
+#define PYTME_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TM_OK 0
+#define TM_E_INVALID (-1)     /* bad argument: null pointer, shape, size */
+#define TM_E_OOM (-2)         /* device allocation failed */
+#define TM_E_CUFFT (-3)       /* cuFFT plan or execution failed */
+#define TM_E_CUDA (-4)        /* CUDA runtime / launch error */
+#define TM_E_TIMEOUT (-5)     /* a bounded device wait gave up */
+#define TM_E_UNSUPPORTED (-6) /* valid request outside what this build implements */
+
+#define TM_SCORE_CC 0    /* tme/matching_scores.py cc_setup + corr_scoring */
+#define TM_SCORE_FLC 1   /* flc_setup + flc_scoring (rotated mask) */
+#define TM_SCORE_FLCSM 2 /* flcSphericalMask_setup + corr_scoring */
+
+#define TM_PREC_FP32 0  /* complex64 intermediate spectra */
+#define TM_PREC_MIXED 1 /* half2 intermediate spectra, FP32 arithmetic, FP64 denominator */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int tm_version(void);
+
+/* Copies the calling thread's last error message (NUL-terminated, truncated to
+ * len). Returns the full message length. */
+int tm_last_error(char* buf, size_t len);
+
+/* Order-1 rigid transform of `n_mat` copies of a (d0,d1,d2) volume.
+ * Replaces NumpyFFTWBackend.rigid_transform / _rigid_transform with order=1
+ * (tme/backends/npfftw_backend.py:357-449), i.e. scipy.ndimage.affine_transform
+ * in mode "constant": out[b][o] = interp(data, M_b[:3,:3] o + M_b[:3,3]), zero when
+ * a coordinate falls below 0 or above n-1 on any axis. `matrices` holds n_mat
+ * row-major 4x4 float32 pull matrices on the device. Output b is the (o0,o1,o2)
+ * array at out + b*o0*o1*o2; only its top-left (d0,d1,d2) box is written.
+ * `mask`/`out_mask` (optional, both or neither) are transformed with the same
+ * matrices, as the reference does for arr_mask. */
+int tm_rigid_transform(const float* data, const float* mask, int d0, int d1, int d2,
+                       const float* matrices, int n_mat, float* out, float* out_mask, int o0,
+                       int o1, int o2, void* stream);
+
+/* In-place masked standardisation of `batch` volumes of n elements:
+ * x = (x - mean) / std * mask with mean/std over mask weights, the reference's
+ * normalize_template (tme/matching_utils.py:61-99). n_obs > 0 is used as the
+ * observation count, otherwise sum(mask) is. mask_batch_stride is 0 to share one
+ * mask across the batch or n for one mask per volume. Reductions run in double.
+ * `workspace` must hold tm_normalize_template_workspace(batch) bytes of device
+ * memory. */
+int64_t tm_normalize_template_workspace(int batch);
+int tm_normalize_template(float* x, const float* mask, int64_t n, int batch,
+                          int64_t mask_batch_stride, double n_obs, void* workspace,
+                          void* stream);
+
+/* NumpyFFTWBackend.norm_scores (tme/backends/npfftw_backend.py:537-587) evaluated in
+ * double: sd = sqrt(max(exp_sq/n - (sq_exp/n)^2, 0)); sd < eps -> 1;
+ * out = arr / (sd * n). arr == NULL stands for the scalar 1. n_obs_dev, when not
+ * NULL, points to a device float32 n_obs that overrides n_obs. */
+int tm_norm_scores(const float* arr, const float* exp_sq, const float* sq_exp, double n_obs,
+                   const float* n_obs_dev, double eps, float* out, int64_t n, void* stream);
+
+/* NumpyFFTWBackend.max_score_over_rotations (tme/backends/npfftw_backend.py:503-535):
+ * where scores > max_scores (strict), copy the score and set rotations to
+ * rotation_index. Buffers must be 16-byte aligned. */
+int tm_max_score_over_rotations(const float* scores, float* max_scores, int32_t* rotations,
+                                int32_t rotation_index, int64_t n, void* stream);
+
+/* ---- FFT plans (cuFFT) for the backend's rfftn / irfftn
+ * (tme/backends/npfftw_backend.py:243-306). ndim in 1..3, shape is the real shape,
+ * batch leading. Forward is unnormalised; tm_fft_c2r multiplies by `scale`
+ * (pass 1/prod(shape) for NumPy's "backward" normalisation) and overwrites its
+ * input. double_precision selects D2Z/Z2D. */
+typedef struct tm_fft_plan tm_fft_plan;
+int tm_fft_plan_create(int ndim, const int* shape, int batch, int double_precision,
+                       tm_fft_plan** plan);
+int tm_fft_plan_destroy(tm_fft_plan* plan);
+int tm_fft_r2c(tm_fft_plan* plan, const void* in, void* out, void* stream);
+int tm_fft_c2r(tm_fft_plan* plan, void* in, void* out, double scale, void* stream);
+
+/* ---- rotation scan: the per-rotation loops of corr_scoring
+ * (tme/matching_scores.py:491-626) and flc_scoring (:629-759) with the
+ * MaxScoreOverRotations update (tme/analyzer/aggregation.py:142-189). */
+typedef struct {
+  int score;             /* TM_SCORE_* */
+  int precision;         /* TM_PREC_* */
+  int fast_shape[3];     /* transform shape (fast_shape of fourier_padding) */
+  int template_shape[3]; /* template / mask shape */
+  int batch;             /* rotations per launch group (fused path) */
+  int plain;             /* 1: one rotation at a time with full cuFFT transforms */
+  int has_template_filter; /* set by tm_scan_set_template */
+} tm_scan_desc;
+
+typedef struct tm_scan tm_scan;
+
+/* Creates a plan and allocates its device scratch. Returns TM_E_UNSUPPORTED for
+ * shapes the fused path does not handle (the plain path handles every shape). */
+int tm_scan_create(const tm_scan_desc* desc, tm_scan** plan);
+int tm_scan_destroy(tm_scan* plan);
+/* Device bytes held by the plan (scratch plus persistent spectra). */
+int64_t tm_scan_device_bytes(const tm_scan* plan);
+
+/* Template and mask as the scoring loops see them (already reversed along every
+ * axis, MatchingData.template, tme/matching_data.py:698-715), shape
+ * template_shape; mask may be NULL for CC. template_filter (optional) is the
+ * multiplicative filter at the template's rfft shape (t0, t1, t2//2+1), applied
+ * to each rotated template before normalisation (_create_filter_func,
+ * tme/matching_scores.py:44-150). Synchronises the stream. */
+int tm_scan_set_template(tm_scan* plan, const float* template_rev, const float* mask_rev,
+                         const float* template_filter, void* stream);
+
+/* Target of shape fast_shape (top-left padded and already filtered). Computes
+ * the target spectra and, for FLCSphericalMask, the inverse local-variance
+ * denominator in double precision (flcSphericalMask_setup,
+ * tme/matching_scores.py:390-450). Call after tm_scan_set_template.
+ * Synchronises the stream. */
+int tm_scan_set_target(tm_scan* plan, const float* target, void* stream);
+
+/* Scores n rotations given as row-major 4x4 float32 pull matrices on the device
+ * (NumpyFFTWBackend._rigid_transform_matrix of each rotation about the template
+ * centre) and folds them into the running state: max_scores (fast_shape float32)
+ * and argmax (fast_shape int32), updated where score > max_scores (strict), with
+ * rotation i recorded as first_index + i. */
+int tm_scan_run(tm_scan* plan, const float* matrices, int n, int32_t first_index,
+                float* max_scores, int32_t* argmax, void* stream);
+
+/* Per-stage timing of the fused path: when enabled, each stage of tm_scan_run is
+ * bracketed by CUDA events on the launching stream (and the host waits for each
+ * stage, so enable it only to measure). Stages: */
+#define TM_STAGE_PREPARE 0  /* rotation, template filter, normalisation */
+#define TM_STAGE_TEMPLATE 1 /* template transform along axes 2 and 1 */
+#define TM_STAGE_XPASS 2    /* axis-0 forward FFT, target product, axis-0 inverse FFT */
+#define TM_STAGE_YPASS 3    /* axis-1 inverse FFT */
+#define TM_STAGE_ZPASS 4    /* axis-2 c2r, score scaling, max/argmax update */
+#define TM_NUM_STAGES 5
+int tm_scan_set_timing(tm_scan* plan, int enable); /* also resets the counters */
+int tm_scan_get_timing(const tm_scan* plan, double* ms, int64_t* launches); /* TM_NUM_STAGES each */
+/* Algorithmic HBM bytes of one launch of `stage` for a group of nb rotations. */
+int64_t tm_scan_stage_bytes(const tm_scan* plan, int stage, int nb);
+
+/* ---- peak calling
+ * Box maximum filter of edge `size` with SciPy's constant mode (cval 0) and the
+ * peak test of NumpyFFTWBackend.max_filter_coordinates
+ * (tme/backends/npfftw_backend.py:200-206): mask[v] = (maxfilter(scores)[v] ==
+ * scores[v]). tmp_a / tmp_b are caller buffers of n0*n1*n2 floats. */
+int tm_max_filter_peaks(const float* scores, int n0, int n1, int n2, int size, float* tmp_a,
+                        float* tmp_b, uint8_t* mask, void* stream);
+
+/* Greedy minimum-distance filter of find_candidate_indices
+ * (tme/external/bindings.cpp:85-126) for n int64 (x, y, z) coordinates in the
+ * order given: point 0 is kept, point i is kept when floor(sqrt(d2)) >
+ * min_distance for every kept point. Writes the kept indices to out_idx (device,
+ * n int32) and their count to *out_count (device int32). Up to 2048 points run in
+ * shared memory; more need `workspace` of tm_find_candidate_indices_workspace(n)
+ * bytes of device memory (otherwise NULL). */
+int64_t tm_find_candidate_indices_workspace(int n);
+int tm_find_candidate_indices(const int64_t* coords, int n, int64_t min_distance,
+                              int32_t* out_idx, int32_t* out_count, void* workspace,
+                              void* stream);
+
+/* Diagnostic: `lines` complex FFTs of length n (dir -1 forward, +1 unnormalised
+ * inverse) with the shared-memory line-FFT routine of the fused scan.
+ * Synchronises. */
+int tm_line_fft_test(const void* x, void* y, int n, int lines, int dir, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYTME_B200_H */

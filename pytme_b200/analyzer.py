@@ -1,0 +1,333 @@
+"""Analyzers with the reference's callback API (tme/analyzer).
+
+``MaxScoreOverRotations`` keeps its (scores, rotations, mapping) state on the
+device; the fused scan updates it directly, any other caller goes through
+``__call__`` and ``tm_max_score_over_rotations``. ``result`` and ``merge`` follow
+tme/analyzer/aggregation.py:207-432. ``PeakCaller`` and its subclasses follow
+tme/analyzer/peaks.py:146-941 with the maximum filter, top-k and greedy
+distance filter running on the GPU (``pytme_b200.peaks``).
+"""
+from __future__ import annotations
+
+from typing import Dict, List, Tuple
+
+import numpy as np
+import torch
+
+from .backend import backend as be
+from .matching import apply_convolution_mode
+
+__all__ = [
+    "SharedAnalyzerProxy",
+    "MaxScoreOverRotations",
+    "PeakCaller",
+    "PeakCallerSort",
+    "PeakCallerMaximumFilter",
+]
+
+
+class SharedAnalyzerProxy:
+    """Holds an analyzer and its state so scoring loops can call
+    ``callback(scores, rotation_matrix=R)`` (tme/analyzer/proxy.py:92-123). Work
+    stays in one process, so the state is never shared."""
+
+    def __init__(self, analyzer_class, analyzer_params: Dict, shm_handler=None, **kwargs):
+        self._shared = False
+        self._analyzer = analyzer_class(**analyzer_params)
+        self._state = self._analyzer.init_state()
+
+    def __call__(self, *args, **kwargs):
+        self._state = self._analyzer(self._state, *args, **kwargs)
+
+    def result(self, **kwargs):
+        return self._analyzer.result(self._state, **kwargs)
+
+    def merge(self, *args, **kwargs):
+        return self._analyzer.merge(*args, **kwargs)
+
+
+class MaxScoreOverRotations:
+    """Maximum score over rotations per translation with the index of the rotation
+    that reached it (tme/analyzer/aggregation.py:31-432)."""
+
+    def __init__(self, shape, offset=None, score_threshold: float = 0,
+                 shm_handler=None, use_memmap: bool = False, inversion_mapping: bool = False,
+                 jax_mode: bool = False, **kwargs):
+        self._use_memmap = use_memmap
+        self._score_threshold = score_threshold
+        self._shape = tuple(int(x) for x in shape)
+        self._inversion_mapping = inversion_mapping
+        if offset is None:
+            offset = np.zeros(len(self._shape), dtype=int)
+        self._offset = np.asarray(offset).astype(int)
+
+    @property
+    def shareable(self):
+        return True
+
+    def init_state(self):
+        dev = torch.device("cuda", torch.cuda.current_device())
+        scores = torch.full(self._shape, float(self._score_threshold), dtype=torch.float32,
+                            device=dev)
+        rotations = torch.full(self._shape, -1, dtype=torch.int32, device=dev)
+        return scores, rotations, {}
+
+    def __call__(self, state, scores, rotation_matrix, **kwargs):
+        prev, rotations, mapping = state
+        index = len(mapping)
+        rot = np.asarray(be.to_numpy_array(rotation_matrix), dtype=np.float32)
+        if self._inversion_mapping:
+            mapping[index] = rot
+        else:
+            index = mapping.setdefault(rot.tobytes(), index)
+        if not isinstance(scores, torch.Tensor):
+            scores = torch.as_tensor(np.asarray(scores, dtype=np.float32), device=prev.device)
+        be.max_score_over_rotations(scores.to(torch.float32), prev, rotations, index)
+        return prev, rotations, mapping
+
+    @staticmethod
+    def _invert_rmap(mapping: dict) -> dict:
+        new_map, ndim = {}, None
+        for k, v in mapping.items():
+            rmat = np.frombuffer(k, dtype=np.float32)
+            if ndim is None:
+                ndim = int(np.sqrt(rmat.size))
+            new_map[v] = rmat.reshape(ndim, ndim)
+        return new_map
+
+    def result(self, state, targetshape=None, templateshape=None, convolution_shape=None,
+               fourier_shift=None, convolution_mode=None, **kwargs):
+        scores, rotations, mapping = state
+        if fourier_shift is not None:
+            axis = tuple(range(len(fourier_shift)))
+            scores = torch.roll(scores, shifts=tuple(int(s) for s in fourier_shift), dims=axis)
+            rotations = torch.roll(rotations, shifts=tuple(int(s) for s in fourier_shift),
+                                   dims=axis)
+        if convolution_mode is not None:
+            args = dict(s1=targetshape, s2=templateshape, convolution_mode=convolution_mode,
+                        convolution_shape=convolution_shape)
+            scores = apply_convolution_mode(scores, **args)
+            rotations = apply_convolution_mode(rotations, **args)
+        scores = scores.contiguous().cpu().numpy()
+        rotations = rotations.contiguous().cpu().numpy()
+        if self._inversion_mapping:
+            mapping = {np.asarray(v, dtype=np.float32).tobytes(): k for k, v in mapping.items()}
+        return scores, np.asarray(self._offset), rotations, self._invert_rmap(mapping)
+
+    @staticmethod
+    def _harmonize_states(states: List[Tuple]):
+        new_map, out_shape = {}, None
+        for i in range(len(states)):
+            if states[i] is None:
+                continue
+            scores, offset, rotations, mapping = states[i]
+            if out_shape is None:
+                out_shape = np.zeros(scores.ndim, int)
+            out_shape = np.maximum(out_shape, np.add(offset, scores.shape))
+            new_param = {}
+            for key, value in mapping.items():
+                b = np.asarray(value, dtype=np.float32).tobytes()
+                new_param[b] = key
+                if b not in new_map:
+                    new_map[b] = len(new_map)
+            states[i] = (scores, offset, rotations, new_param)
+        out_shape = None if out_shape is None else tuple(int(x) for x in out_shape)
+        return new_map, out_shape, states
+
+    @classmethod
+    def merge(cls, results: List[Tuple], **kwargs):
+        """tme/analyzer/aggregation.py:305-432 (in-memory)."""
+        results = [r for r in results]
+        if len(results) == 1:
+            return results[0]
+        master, out_shape, results = cls._harmonize_states(results)
+        if out_shape is None:
+            return None
+        sd, rd = results[0][0].dtype, results[0][2].dtype
+        scores_out = np.full(out_shape, fill_value=kwargs.get("score_threshold", 0), dtype=sd)
+        rot_out = np.full(out_shape, fill_value=-1, dtype=rd)
+        for i in range(len(results)):
+            if results[i] is None:
+                continue
+            scores, offset, rotations, mapping = results[i]
+            stops = np.add(offset, scores.shape).astype(int)
+            idx = tuple(slice(*pos) for pos in zip(offset, stops))
+            upd = scores > scores_out[idx]
+            scores_out[idx][upd] = scores[upd]
+            lut = np.arange(len(mapping) + 1, dtype=rot_out.dtype)
+            for key, value in mapping.items():
+                lut[value] = master[key]
+            ur = rotations[upd]
+            if len(ur):
+                rot_out[idx][upd] = lut[ur]
+            results[i] = None
+        return (scores_out, np.zeros(scores_out.ndim, dtype=int), rot_out,
+                cls._invert_rmap(master))
+
+
+class PeakCaller:
+    """Base class of the peak callers (tme/analyzer/peaks.py:146-620): candidate
+    peaks per score map, validity masking, greedy minimum-distance filtering and
+    top-k selection against the running state."""
+
+    def __init__(self, shape, num_peaks: int = 1000, min_distance: int = 1,
+                 min_boundary_distance: int = 0, min_score: float = None,
+                 max_score: float = None, batch_dims=None, shm_handler=None, **kwargs):
+        if num_peaks <= 0:
+            raise ValueError("num_peaks has to be larger than 0.")
+        if min_distance < 0:
+            raise ValueError("min_distance has to be non-negative.")
+        if min_boundary_distance < 0:
+            raise ValueError("min_boundary_distance has to be non-negative.")
+        if batch_dims is not None:
+            raise NotImplementedError("batched peak calling is not supported")
+        self.shape = shape
+        self.num_peaks = int(num_peaks)
+        self.min_distance = int(min_distance)
+        self.min_boundary_distance = int(min_boundary_distance)
+        self.batch_dims = None
+        self.min_score, self.max_score = min_score, max_score
+
+    @property
+    def shareable(self):
+        return False
+
+    def call_peaks(self, scores, **kwargs):
+        raise NotImplementedError
+
+    def init_state(self):
+        ndim = len(self.shape)
+        translations = np.full((self.num_peaks, ndim), -1, dtype=np.int32)
+        rotations = np.zeros((self.num_peaks, ndim, ndim), dtype=np.float32)
+        for i in range(ndim):
+            rotations[:, i, i] = 1.0
+        scores = np.full((self.num_peaks,), -1, dtype=np.float32)
+        details = np.full((self.num_peaks,), -1, dtype=np.float32)
+        return translations, rotations, scores, details
+
+    def _get_peak_mask(self, peaks: np.ndarray, scores: np.ndarray):
+        """tme/analyzer/peaks.py:241-290."""
+        from .peaks import topk_indices
+
+        if not len(peaks):
+            return None
+        upper = np.subtract(np.asarray(scores.shape), self.min_boundary_distance)
+        valid = np.multiply(peaks < upper, peaks >= self.min_boundary_distance)
+        valid = np.sum(valid, axis=1) == peaks.shape[1]
+        ps = scores[tuple(peaks.T)]
+        valid = np.multiply(ps == ps, valid)
+        if self.min_score is not None:
+            valid = np.multiply(ps >= self.min_score, valid)
+        if self.max_score is not None:
+            valid = np.multiply(ps <= self.max_score, valid)
+        if np.sum(valid) == 0:
+            return None
+        if np.sum(valid) > self.num_peaks or ps.shape[0] > self.num_peaks:
+            top = topk_indices(ps * valid, min(ps.size, 2 * self.num_peaks))
+            valid = np.full(ps.shape, 0, bool)
+            valid[top] = True
+            if self.min_score is not None:
+                valid = np.multiply(ps >= self.min_score, valid)
+            if self.max_score is not None:
+                valid = np.multiply(ps <= self.max_score, valid)
+        return valid
+
+    def __call__(self, state, scores, rotation_matrix, **kwargs):
+        """tme/analyzer/peaks.py:327-384 for one score map."""
+        positions, details = self.call_peaks(scores=scores, rotation_matrix=rotation_matrix,
+                                             min_score=self.min_score, max_score=self.max_score)
+        if positions is None or len(positions) == 0:
+            return state
+        positions = np.asarray(positions).astype(np.int64)
+        host = scores.detach().cpu().numpy() if isinstance(scores, torch.Tensor) else \
+            np.asarray(scores)
+        valid = self._get_peak_mask(positions, host)
+        if valid is None:
+            return state
+        positions = positions[valid]
+        pscores = host[tuple(positions.T)]
+        pdetails = np.full(pscores.shape, -1, dtype=np.float32) if details is None else \
+            np.asarray(details)[valid]
+        rot = np.asarray(be.to_numpy_array(rotation_matrix), dtype=np.float32)
+        rots = np.repeat(rot.reshape(1, *rot.shape), positions.shape[0], axis=0)
+        return self._update(state, positions, pdetails, pscores, rots)
+
+    def _update(self, state, peak_positions, peak_details, peak_scores, peak_rotations,
+                offset=None):
+        """tme/analyzer/peaks.py:531-583."""
+        from .peaks import filter_points_indices, topk_indices
+
+        translations, rotations, scores, details = state
+        peak_positions = np.asarray(peak_positions)
+        if offset is not None:
+            peak_positions = np.add(peak_positions, np.asarray(offset).astype(peak_positions.dtype))
+        positions = np.concatenate((translations, peak_positions))
+        rotations = np.concatenate((rotations, peak_rotations))
+        scores = np.concatenate((scores, np.asarray(peak_scores, dtype=np.float32)))
+        details = np.concatenate((details, np.asarray(peak_details, dtype=np.float32)))
+        order = filter_points_indices(positions, self.min_distance, scores=scores)
+        top = topk_indices(scores[order], min(len(order), self.num_peaks))
+        final = np.asarray(order)[top]
+        return positions[final], rotations[final], scores[final], details[final]
+
+    def result(self, state, fast_shape=None, targetshape=None, templateshape=None,
+               convolution_shape=None, fourier_shift=None, convolution_mode=None, **kwargs):
+        """tme/analyzer/peaks.py:585-620 with score_to_cart (tme/analyzer/_utils.py:120-191):
+        wrap by the Fourier shift, crop to the convolution mode's output box and drop
+        rows with negative coordinates."""
+        translations, rotations, scores, details = state
+        positions = np.asarray(translations).astype(np.int64)
+        valid = np.ones(positions.shape[0], dtype=bool)
+        if fourier_shift is not None:
+            positions = np.mod(positions + np.asarray(fourier_shift), np.asarray(fast_shape))
+        if convolution_mode is not None:
+            conv = np.asarray(convolution_shape)
+            if convolution_mode == "same":
+                out_shape = np.asarray(targetshape)
+            elif convolution_mode == "valid":
+                out_shape = np.subtract(targetshape, templateshape) + 1
+            else:
+                out_shape = conv
+            starts = np.divide(np.subtract(conv, out_shape), 2).astype(np.int32)
+            stops = starts + out_shape
+            valid = np.sum(np.multiply(positions >= starts, positions < stops), axis=1) \
+                == positions.shape[1]
+            positions = positions - starts
+        valid = np.multiply(np.sum(positions >= 0, axis=1) == positions.shape[1], valid)
+        valid = valid.astype(bool)
+        return positions[valid], rotations[valid], scores[valid], details[valid]
+
+    @classmethod
+    def merge(cls, results=List[Tuple], **kwargs):
+        """tme/analyzer/peaks.py:386-426."""
+        if "shape" not in kwargs:
+            kwargs["shape"] = tuple(1 for _ in range(results[0][0].shape[1]))
+        base = cls(**kwargs)
+        state = base.init_state()
+        for r in results:
+            if len(r) == 0:
+                continue
+            pos, rot, sc, det = r
+            state = base._update(state, np.asarray(pos), np.asarray(det), np.asarray(sc),
+                                 np.asarray(rot), offset=kwargs.get("offset", None))
+        return state
+
+
+class PeakCallerSort(PeakCaller):
+    """The ``num_peaks`` highest scores (tme/analyzer/peaks.py:641-659)."""
+
+    def call_peaks(self, scores, **kwargs):
+        from .peaks import topk_indices_device
+
+        coords = topk_indices_device(scores, min(self.num_peaks, int(np.prod(scores.shape))))
+        return coords, None
+
+
+class PeakCallerMaximumFilter(PeakCaller):
+    """Local maxima of a box maximum filter with edge ``min_distance``
+    (tme/analyzer/peaks.py:662-670)."""
+
+    def call_peaks(self, scores, **kwargs):
+        from .peaks import max_filter_coordinates
+
+        return max_filter_coordinates(scores, self.min_distance), None

@@ -1,0 +1,951 @@
+// Exhaustive rotation scan: the per-rotation loops of corr_scoring
+// (tme/matching_scores.py:600-624; CC and FLCSphericalMask) and flc_scoring
+// (tme/matching_scores.py:727-757; FLC), with MaxScoreOverRotations state updates
+// (tme/analyzer/aggregation.py:142-189, tme/backends/npfftw_backend.py:503-535).
+//
+// Two execution paths share one plan object:
+//
+//  * plain: one rotation at a time with full-size cuFFT r2c/c2r transforms of the
+//    zero-padded template and separate product/epilogue kernels. This is the
+//    straightforward FP32 GPU port of the reference loop and serves as the
+//    "plain" baseline.
+//
+//  * fused: B rotations per launch group through four kernels of this library.
+//      K1 tmpl_zy    template rows: direct real DFT along axis 2 (only t2 of n2
+//                    inputs are non-zero) and a zero-padded FFT along axis 1,
+//                    producing G[b][x < t0][k1][k2]
+//      K2 xpass      per (k1, k2-tile) column block: forward FFT along axis 0 of
+//                    the zero-padded G columns, product with the target spectrum
+//                    (held in registers for all B rotations), inverse FFT along
+//                    axis 0 -> H[b][x'][k1][k2]
+//      K3 ypass      inverse FFT along axis 1, in place on H
+//      K4 zpass      c2r along axis 2 (half-length complex FFT), score scaling and
+//                    the strict-> max/argmax over the B rotations in registers,
+//                    merged into the caller's state once per launch group
+//    H is complex64 ("fp32") or half2 with a fixed scale ("mixed").
+//
+// Target-side quantities (target spectra and the FLCSphericalMask denominator)
+// are computed once by set_target; the denominator and the target mean are
+// evaluated in double precision.
+#include "common.cuh"
+#include "fft_smem.cuh"
+#include "ops.cuh"
+#include "scan.cuh"
+
+#include <cuda_fp16.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace tmb {
+
+using fft::LinePlan;
+
+static int cufft_status(cufftResult r, const char* what) {
+  if (r == CUFFT_SUCCESS) return TM_OK;
+  set_error("%s: cuFFT error %d", what, (int)r);
+  return r == CUFFT_ALLOC_FAILED ? TM_E_OOM : TM_E_CUFFT;
+}
+
+LinePlan make_line_plan(int n) {
+  LinePlan p{};
+  p.n = n;
+  int m = n, e2 = 0;
+  while (m % 2 == 0) { m /= 2; ++e2; }
+  int k = 0;
+  int eights = e2 / 3, rem = e2 % 3;
+  if (rem == 1 && eights > 0) { eights -= 1; p.radix[k++] = 4; p.radix[k++] = 4; }
+  else if (rem == 1) { p.radix[k++] = 2; }
+  else if (rem == 2) { p.radix[k++] = 4; }
+  for (int i = 0; i < eights; ++i) p.radix[k++] = 8;
+  for (int q : {3, 5, 7, 11, 13}) {
+    while (m % q == 0) { m /= q; p.radix[k++] = q; }
+  }
+  p.npass = (m == 1) ? k : -1;
+  return p;
+}
+
+static bool line_supported(int n) {
+  if (n < 2 || n > 4096) return false;
+  LinePlan p = make_line_plan(n);
+  return p.npass > 0 && p.npass <= fft::kMaxPasses && fft::supported_radices(p);
+}
+
+static std::vector<float2> twiddle_table(int n) {
+  std::vector<float2> t(n);
+  for (int i = 0; i < n; ++i) {
+    double a = -2.0 * M_PI * (double)i / (double)n;
+    t[i] = make_float2((float)cos(a), (float)sin(a));
+  }
+  return t;
+}
+
+// ------------------------------------------------------------------ storage types
+template <typename T> struct Store;
+template <> struct Store<float2> {
+  static __device__ __forceinline__ float2 load(const float2* p) { return *p; }
+  static __device__ __forceinline__ void store(float2* p, float2 v) { *p = v; }
+};
+template <> struct Store<__half2> {
+  static __device__ __forceinline__ float2 load(const __half2* p) { return __half22float2(*p); }
+  static __device__ __forceinline__ void store(__half2* p, float2 v) { *p = __float22half2_rn(v); }
+};
+
+constexpr int kThreads = 512;
+constexpr int kMaxE = 8;             // complex elements per thread in a line-FFT tile
+constexpr int kTile = kThreads * kMaxE;  // elements per tile (4096)
+
+// ------------------------------------------------------------------ K1: template z/y
+// grid (ceil(h2/W), t0, B); tile: n1 lines-fast rows x W lines (k2).
+__global__ void __launch_bounds__(kThreads, 1)
+tmpl_zy_kernel(const float* __restrict__ tmpl, int t0, int t1, int t2, int n1, int n2, int h2,
+               int W, LinePlan p1, const float2* __restrict__ tw1_g, const float2* __restrict__ tw2_g,
+               float2* __restrict__ G) {
+  extern __shared__ float4 smem_raw[];
+  float2* tw1 = reinterpret_cast<float2*>(smem_raw);
+  float2* tw2 = tw1 + n1;
+  float2* buf = tw2 + n2;
+  float* plane = reinterpret_cast<float*>(buf + (int64_t)n1 * W);
+  const int tid = threadIdx.x;
+  const int k2_0 = blockIdx.x * W;
+  const int x = blockIdx.y;
+  const int b = blockIdx.z;
+  for (int i = tid; i < n1; i += kThreads) tw1[i] = tw1_g[i];
+  for (int i = tid; i < n2; i += kThreads) tw2[i] = tw2_g[i];
+  const float* src = tmpl + ((int64_t)b * t0 + x) * t1 * t2;
+  for (int i = tid; i < t1 * t2; i += kThreads) plane[i] = src[i];
+  __syncthreads();
+  // G1[y][k2] = sum_z plane[y][z] * exp(-2 pi i z k2 / n2), rows y >= t1 are zero
+  for (int e = tid; e < n1 * W; e += kThreads) {
+    int y = e / W, l = e % W;
+    int k2 = k2_0 + l;
+    float2 acc = make_float2(0.f, 0.f);
+    if (y < t1 && k2 < h2) {
+      const float* row = plane + y * t2;
+      int idx = 0;
+      for (int z = 0; z < t2; ++z) {
+        float v = row[z];
+        float2 w = tw2[idx];
+        acc.x += v * w.x;
+        acc.y += v * w.y;
+        idx += k2;
+        if (idx >= n2) idx -= n2;
+      }
+    }
+    buf[e] = acc;
+  }
+  __syncthreads();
+  fft::fft_lines<-1, kMaxE, true>(buf, p1, W, 1, W, tw1, n1, tid, kThreads);
+  float2* dst = G + ((int64_t)b * t0 + x) * n1 * h2;
+  for (int e = tid; e < n1 * W; e += kThreads) {
+    int k1 = e / W, l = e % W;
+    int k2 = k2_0 + l;
+    if (k2 < h2) dst[(int64_t)k1 * h2 + k2] = buf[e];
+  }
+}
+
+// ------------------------------------------------------------------ K2: x pass
+// grid (ceil(h2/W), n1); loops over the B rotations of the group.
+template <typename HT>
+__global__ void __launch_bounds__(kThreads, 1)
+xpass_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, int B, int t0, int n0,
+             int n1, int h2, int W, LinePlan p0, const float2* __restrict__ tw0_g, float scale,
+             HT* __restrict__ H) {
+  extern __shared__ float4 smem_raw[];
+  float2* tw0 = reinterpret_cast<float2*>(smem_raw);
+  float2* buf = tw0 + n0;
+  const int tid = threadIdx.x;
+  const int k2_0 = blockIdx.x * W;
+  const int k1 = blockIdx.y;
+  for (int i = tid; i < n0; i += kThreads) tw0[i] = tw0_g[i];
+  const int tile = n0 * W;
+  // target-spectrum tile: re-read through L1 for every rotation of the group
+  const float2* ft_col = Ft + (int64_t)k1 * h2 + k2_0;
+  const int64_t ft_row = (int64_t)n1 * h2;
+  const int64_t S = (int64_t)n0 * n1 * h2;
+  for (int b = 0; b < B; ++b) {
+    const float2* g = G + (int64_t)b * t0 * n1 * h2;
+    for (int e = tid; e < tile; e += kThreads) {
+      int x = e / W, l = e % W;
+      int k2 = k2_0 + l;
+      float2 v = make_float2(0.f, 0.f);
+      if (x < t0 && k2 < h2) v = g[((int64_t)x * n1 + k1) * h2 + k2];
+      buf[e] = v;
+    }
+    __syncthreads();
+    fft::fft_lines<-1, kMaxE, true>(buf, p0, W, 1, W, tw0, n0, tid, kThreads);
+    for (int e = tid; e < tile; e += kThreads) {
+      int k0 = e / W, l = e % W;
+      float2 f = make_float2(0.f, 0.f);
+      if (k2_0 + l < h2) f = __ldg(ft_col + k0 * ft_row + l);
+      buf[e] = fft::cmul(buf[e], make_float2(f.x * scale, f.y * scale));
+    }
+    __syncthreads();
+    fft::fft_lines<1, kMaxE, true>(buf, p0, W, 1, W, tw0, n0, tid, kThreads);
+    HT* h = H + (int64_t)b * S;
+    for (int e = tid; e < tile; e += kThreads) {
+      int x = e / W, l = e % W;
+      int k2 = k2_0 + l;
+      if (k2 < h2) Store<HT>::store(h + ((int64_t)x * n1 + k1) * h2 + k2, buf[e]);
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ K3: y pass
+// grid (ceil(h2/W), n0, B): inverse FFT along axis 1, in place.
+template <typename HT>
+__global__ void __launch_bounds__(kThreads, 1)
+ypass_kernel(HT* __restrict__ H, int n0, int n1, int h2, int W, LinePlan p1,
+             const float2* __restrict__ tw1_g) {
+  extern __shared__ float4 smem_raw[];
+  float2* tw1 = reinterpret_cast<float2*>(smem_raw);
+  float2* buf = tw1 + n1;
+  const int tid = threadIdx.x;
+  const int k2_0 = blockIdx.x * W;
+  const int x = blockIdx.y;
+  const int b = blockIdx.z;
+  for (int i = tid; i < n1; i += kThreads) tw1[i] = tw1_g[i];
+  const int tile = n1 * W;
+  HT* h = H + (int64_t)b * n0 * n1 * h2 + (int64_t)x * n1 * h2;
+  for (int e = tid; e < tile; e += kThreads) {
+    int y = e / W, l = e % W;
+    int k2 = k2_0 + l;
+    buf[e] = (k2 < h2) ? Store<HT>::load(h + (int64_t)y * h2 + k2) : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  fft::fft_lines<1, kMaxE, true>(buf, p1, W, 1, W, tw1, n1, tid, kThreads);
+  for (int e = tid; e < tile; e += kThreads) {
+    int y = e / W, l = e % W;
+    int k2 = k2_0 + l;
+    if (k2 < h2) Store<HT>::store(h + (int64_t)y * h2 + k2, buf[e]);
+  }
+}
+
+// ------------------------------------------------------------------ K4: z pass + epilogue
+// grid (ceil(n0*n1/R)); each CTA owns R consecutive (x', y') rows = R*n2 output voxels.
+// c2r of length n2 (even) via a complex inverse FFT of length m = n2/2:
+//   E[k] = X[k] + conj(X[m-k]),  O[k] = (X[k] - conj(X[m-k])) * exp(+2 pi i k / n2),
+//   z = IDFT_m(E + i O)  ->  x[2j] = Re z[j], x[2j+1] = Im z[j]
+// with the imaginary parts of X[0] and X[m] dropped, as numpy/pocketfft's c2r does.
+constexpr int kMaxV = 8;   // output voxels per thread
+
+template <typename HT>
+__global__ void __launch_bounds__(kThreads, 1)
+zpass_kernel(const HT* __restrict__ H, int B, int64_t rows, int n2, int h2, int R, LinePlan pm,
+             const float2* __restrict__ tw2_g, float scale, const float* __restrict__ inv_den,
+             int32_t first_index, float* __restrict__ state_max, int32_t* __restrict__ state_rot,
+             int64_t S) {
+  extern __shared__ float4 smem_raw[];
+  const int m = n2 / 2;
+  float2* tw2 = reinterpret_cast<float2*>(smem_raw);
+  float2* raw = tw2 + n2;
+  float2* buf = raw + (int64_t)R * h2;
+  const int tid = threadIdx.x;
+  const int64_t row0 = (int64_t)blockIdx.x * R;
+  const int nrows = (int)min((int64_t)R, rows - row0);
+  for (int i = tid; i < n2; i += kThreads) tw2[i] = tw2_g[i];
+  const int nout = nrows * n2;
+  const int64_t vox0 = row0 * n2;
+  float den[kMaxV], best[kMaxV];
+  int32_t arg[kMaxV];
+#pragma unroll
+  for (int c = 0; c < kMaxV; ++c) {
+    int v = tid + c * kThreads;
+    den[c] = (v < nout) ? (inv_den ? inv_den[vox0 + v] : 1.f) * scale : 0.f;
+    best[c] = -INFINITY;
+    arg[c] = -1;
+  }
+  for (int b = 0; b < B; ++b) {
+    const HT* src = H + (int64_t)b * S + row0 * h2;
+    for (int e = tid; e < nrows * h2; e += kThreads) raw[e] = Store<HT>::load(src + e);
+    __syncthreads();
+    for (int e = tid; e < nrows * m; e += kThreads) {
+      int r = e / m, k = e % m;
+      const float2* xr = raw + (int64_t)r * h2;
+      float2 a = xr[k], c = xr[m - k];
+      if (k == 0) { a.y = 0.f; c.y = 0.f; }
+      float2 cc = fft::cconj(c);
+      float2 E = fft::cadd(a, cc);
+      float2 O = fft::cmul(fft::csub(a, cc), fft::cconj(tw2[k]));
+      buf[e] = make_float2(E.x - O.y, E.y + O.x);
+    }
+    __syncthreads();
+    fft::fft_lines<1, kMaxE, false>(buf, pm, nrows, m, 1, tw2, n2, tid, kThreads);
+    const float* outv = reinterpret_cast<const float*>(buf);
+#pragma unroll
+    for (int c = 0; c < kMaxV; ++c) {
+      int v = tid + c * kThreads;
+      if (v < nout) {
+        float s = outv[v] * den[c];
+        if (s > best[c]) {
+          best[c] = s;
+          arg[c] = first_index + b;
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int c = 0; c < kMaxV; ++c) {
+    int v = tid + c * kThreads;
+    if (v < nout && arg[c] >= 0) {
+      int64_t g = vox0 + v;
+      if (best[c] > state_max[g]) {
+        state_max[g] = best[c];
+        state_rot[g] = arg[c];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ helpers
+__global__ void sum_double_kernel(const float* __restrict__ x, int64_t n, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    s += (double)x[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) sh[warp] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    out[blockIdx.x] = t;
+  }
+}
+
+__global__ void center_kernel(const float* __restrict__ x, const double* __restrict__ partial,
+                              int nparts, int64_t n, float* __restrict__ out_c,
+                              double* __restrict__ out_d, double* __restrict__ out_d2) {
+  __shared__ double mean;
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < nparts; ++i) s += partial[i];
+    mean = s / (double)n;
+  }
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double v = (double)x[i] - mean;
+    if (out_c) out_c[i] = (float)v;
+    if (out_d) out_d[i] = v;
+    if (out_d2) out_d2[i] = v * v;
+  }
+}
+
+__global__ void square_kernel(const float* __restrict__ x, float* __restrict__ y, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float v = x[i];
+    y[i] = v * v;
+  }
+}
+
+__global__ void zmul_kernel(const double2* __restrict__ a, const double2* __restrict__ b,
+                            double2* __restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double2 x = a[i], y = b[i];
+    out[i] = make_double2(x.x * y.x - x.y * y.y, x.x * y.y + x.y * y.x);
+  }
+}
+
+__global__ void pad_double_kernel(const float* __restrict__ src, int t0, int t1, int t2,
+                                  double* __restrict__ dst, int n1, int n2) {
+  const int64_t n = (int64_t)t0 * t1 * t2;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    int i2 = (int)(v % t2);
+    int64_t r = v / t2;
+    int i1 = (int)(r % t1);
+    int i0 = (int)(r / t1);
+    dst[((int64_t)i0 * n1 + i1) * n2 + i2] = (double)src[v];
+  }
+}
+
+// inverse denominator 1 / (n_obs * sd) from unnormalised double inverse transforms
+__global__ void inv_den_kernel(const double* __restrict__ cc1, const double* __restrict__ cc2,
+                               double invN, double n_obs, double eps, float* __restrict__ out,
+                               int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double e = cc1[i] * invN / n_obs;
+    double e2 = cc2[i] * invN / n_obs;
+    double var = e2 - e * e;
+    double sd = sqrt(var > 0 ? var : 0.0);
+    if (sd < eps) sd = 1.0;
+    out[i] = (float)(1.0 / (sd * n_obs));
+  }
+}
+
+static unsigned grid_for(int64_t n, int threads = 256, int64_t cap = 148 * 16) {
+  int64_t b = ceil_div(n, threads);
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (unsigned)b;
+}
+
+// ------------------------------------------------------------------ plan
+struct Scan {
+  tm_scan_desc d{};
+  int n0 = 0, n1 = 0, n2 = 0, h2 = 0, t0 = 0, t1 = 0, t2 = 0, th2 = 0;
+  int64_t N = 0, S = 0, T = 0, TS = 0;
+  bool fused = false, half = false;
+  int B = 1;
+  double mask_sum = 0.0, target_mean = 0.0;
+  bool target_ready = false, template_ready = false;
+  // persistent buffers
+  void* base = nullptr;
+  size_t bytes = 0;
+  float2* ft_target = nullptr;
+  float2* ft_target2 = nullptr;
+  float* inv_den = nullptr;
+  float* tmpl = nullptr;
+  float* mask = nullptr;
+  float* tfilter = nullptr;
+  float* mat = nullptr;  // B x 16 matrices for the current group (device copy)
+  // per-group scratch
+  float* rot_t = nullptr;
+  float* rot_m = nullptr;
+  double* stats_ws = nullptr;
+  float2* tspec = nullptr;   // template-shape spectra (filter)
+  float* arr = nullptr;      // plain: fast real buffers
+  float* arr_m = nullptr;
+  float* cc_m = nullptr;
+  float* cc_m2 = nullptr;
+  float2* spec = nullptr;
+  float2* spec_m = nullptr;
+  float2* G = nullptr;
+  void* H = nullptr;
+  float2* tw0 = nullptr;
+  float2* tw1 = nullptr;
+  float2* tw2 = nullptr;
+  LinePlan p0{}, p1{}, pm{};
+  int W1 = 1, W2 = 1, W3 = 1, R4 = 1;
+  size_t smem1 = 0, smem2 = 0, smem3 = 0, smem4 = 0;
+  cufftHandle fwd = 0, inv = 0, tfwd = 0, tinv = 0;
+  bool have_fwd = false, have_tfwd = false;
+  // optional per-stage timing with CUDA events on the launching stream
+  bool timing = false;
+  double stage_ms[TM_NUM_STAGES] = {0};
+  int64_t stage_launches[TM_NUM_STAGES] = {0};
+  cudaEvent_t ev[TM_NUM_STAGES + 1] = {};
+  bool have_events = false;
+};
+
+// Stage timing: record an event before a stage and accumulate after it.
+struct StageTimer {
+  Scan* s;
+  cudaStream_t st;
+  StageTimer(Scan* s_, cudaStream_t st_) : s(s_), st(st_) {}
+  void begin() { if (s->timing) cudaEventRecord(s->ev[0], st); }
+  void end(int stage) {
+    if (!s->timing) return;
+    cudaEventRecord(s->ev[1], st);
+    cudaEventSynchronize(s->ev[1]);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]);
+    s->stage_ms[stage] += ms;
+    s->stage_launches[stage] += 1;
+  }
+};
+
+static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static void destroy(Scan* s) {
+  if (!s) return;
+  if (s->have_events)
+    for (auto& e : s->ev) cudaEventDestroy(e);
+  if (s->have_fwd) { cufftDestroy(s->fwd); cufftDestroy(s->inv); }
+  if (s->have_tfwd) { cufftDestroy(s->tfwd); cufftDestroy(s->tinv); }
+  if (s->base) cudaFree(s->base);
+  delete s;
+}
+
+int scan_destroy(Scan* s) {
+  destroy(s);
+  return TM_OK;
+}
+
+int scan_create(const tm_scan_desc* desc, Scan** out) {
+  TM_REQUIRE(desc && out, "scan_create: null pointer");
+  *out = nullptr;
+  const tm_scan_desc& d = *desc;
+  TM_REQUIRE(d.score == TM_SCORE_CC || d.score == TM_SCORE_FLC || d.score == TM_SCORE_FLCSM,
+             "scan_create: unknown score %d", d.score);
+  TM_REQUIRE(d.precision == TM_PREC_FP32 || d.precision == TM_PREC_MIXED,
+             "scan_create: unknown precision %d", d.precision);
+  for (int a = 0; a < 3; ++a) {
+    TM_REQUIRE(d.fast_shape[a] > 0 && d.template_shape[a] > 0,
+               "scan_create: shapes must be positive");
+    TM_REQUIRE(d.template_shape[a] <= d.fast_shape[a],
+               "scan_create: template axis %d (%d) exceeds the transform length (%d)", a,
+               d.template_shape[a], d.fast_shape[a]);
+  }
+  TM_REQUIRE(d.batch >= 1 && d.batch <= 4096, "scan_create: batch must be in [1, 4096]");
+  Scan* s = new Scan();
+  s->d = d;
+  s->n0 = d.fast_shape[0]; s->n1 = d.fast_shape[1]; s->n2 = d.fast_shape[2];
+  s->h2 = s->n2 / 2 + 1;
+  s->t0 = d.template_shape[0]; s->t1 = d.template_shape[1]; s->t2 = d.template_shape[2];
+  s->th2 = s->t2 / 2 + 1;
+  s->N = (int64_t)s->n0 * s->n1 * s->n2;
+  s->S = (int64_t)s->n0 * s->n1 * s->h2;
+  s->T = (int64_t)s->t0 * s->t1 * s->t2;
+  s->TS = (int64_t)s->t0 * s->t1 * s->th2;
+  s->fused = !d.plain;
+  s->half = d.precision == TM_PREC_MIXED;
+  s->B = s->fused ? d.batch : 1;
+  if (s->fused) {
+    bool ok = line_supported(s->n0) && line_supported(s->n1) && (s->n2 % 2 == 0) &&
+              line_supported(s->n2 / 2) && s->n0 <= kTile && s->n1 <= kTile &&
+              s->n2 <= kThreads * kMaxV && d.score != TM_SCORE_FLC;
+    if (!ok) {
+      set_error("scan_create: fused path does not support shape (%d,%d,%d) / score %d",
+                s->n0, s->n1, s->n2, d.score);
+      delete s;
+      return TM_E_UNSUPPORTED;
+    }
+  } else {
+    TM_REQUIRE(!s->half, "scan_create: the plain path is FP32 only");
+  }
+
+  // ---- memory layout
+  const int B = s->B;
+  size_t off = 0;
+  auto take = [&](size_t nbytes) { size_t o = off; off = align_up(off + nbytes); return o; };
+  size_t o_ft = take(sizeof(float2) * s->S);
+  size_t o_ft2 = d.score == TM_SCORE_FLC ? take(sizeof(float2) * s->S) : 0;
+  size_t o_den = d.score == TM_SCORE_FLCSM ? take(sizeof(float) * s->N) : 0;
+  size_t o_tm = take(sizeof(float) * s->T);
+  size_t o_mk = take(sizeof(float) * s->T);
+  size_t o_tf = take(sizeof(float) * s->TS);
+  size_t o_mat = take(sizeof(float) * 16 * B);
+  size_t o_rt = take(sizeof(float) * s->T * B);
+  size_t o_rm = take(sizeof(float) * s->T * B);
+  size_t o_st = take(stats_workspace_bytes(B));
+  size_t o_ts = take(sizeof(float2) * s->TS * B);
+  size_t o_arr = 0, o_arrm = 0, o_ccm = 0, o_ccm2 = 0, o_spec = 0, o_specm = 0, o_G = 0, o_H = 0;
+  size_t o_tw0 = 0, o_tw1 = 0, o_tw2 = 0;
+  if (!s->fused) {
+    o_arr = take(sizeof(float) * s->N);
+    o_spec = take(sizeof(float2) * s->S);
+    if (d.score == TM_SCORE_FLC) {
+      o_arrm = take(sizeof(float) * s->N);
+      o_ccm = take(sizeof(float) * s->N);
+      o_ccm2 = take(sizeof(float) * s->N);
+      o_specm = take(sizeof(float2) * s->S);
+    }
+  } else {
+    o_G = take(sizeof(float2) * (size_t)B * s->t0 * s->n1 * s->h2);
+    o_H = take((s->half ? sizeof(__half2) : sizeof(float2)) * (size_t)B * s->S);
+    o_tw0 = take(sizeof(float2) * s->n0);
+    o_tw1 = take(sizeof(float2) * s->n1);
+    o_tw2 = take(sizeof(float2) * s->n2);
+  }
+  s->bytes = off;
+  cudaError_t e = cudaMalloc(&s->base, s->bytes);
+  if (e != cudaSuccess) {
+    set_error("scan_create: cudaMalloc of %zu bytes failed: %s", s->bytes, cudaGetErrorString(e));
+    delete s;
+    return TM_E_OOM;
+  }
+  char* b8 = static_cast<char*>(s->base);
+  s->ft_target = reinterpret_cast<float2*>(b8 + o_ft);
+  if (d.score == TM_SCORE_FLC) s->ft_target2 = reinterpret_cast<float2*>(b8 + o_ft2);
+  if (d.score == TM_SCORE_FLCSM) s->inv_den = reinterpret_cast<float*>(b8 + o_den);
+  s->tmpl = reinterpret_cast<float*>(b8 + o_tm);
+  s->mask = reinterpret_cast<float*>(b8 + o_mk);
+  s->tfilter = reinterpret_cast<float*>(b8 + o_tf);
+  s->mat = reinterpret_cast<float*>(b8 + o_mat);
+  s->rot_t = reinterpret_cast<float*>(b8 + o_rt);
+  s->rot_m = reinterpret_cast<float*>(b8 + o_rm);
+  s->stats_ws = reinterpret_cast<double*>(b8 + o_st);
+  s->tspec = reinterpret_cast<float2*>(b8 + o_ts);
+  if (!s->fused) {
+    s->arr = reinterpret_cast<float*>(b8 + o_arr);
+    s->spec = reinterpret_cast<float2*>(b8 + o_spec);
+    if (d.score == TM_SCORE_FLC) {
+      s->arr_m = reinterpret_cast<float*>(b8 + o_arrm);
+      s->cc_m = reinterpret_cast<float*>(b8 + o_ccm);
+      s->cc_m2 = reinterpret_cast<float*>(b8 + o_ccm2);
+      s->spec_m = reinterpret_cast<float2*>(b8 + o_specm);
+    }
+  } else {
+    s->G = reinterpret_cast<float2*>(b8 + o_G);
+    s->H = b8 + o_H;
+    s->tw0 = reinterpret_cast<float2*>(b8 + o_tw0);
+    s->tw1 = reinterpret_cast<float2*>(b8 + o_tw1);
+    s->tw2 = reinterpret_cast<float2*>(b8 + o_tw2);
+    auto t0v = twiddle_table(s->n0), t1v = twiddle_table(s->n1), t2v = twiddle_table(s->n2);
+    cudaMemcpy(s->tw0, t0v.data(), sizeof(float2) * s->n0, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->tw1, t1v.data(), sizeof(float2) * s->n1, cudaMemcpyHostToDevice);
+    e = cudaMemcpy(s->tw2, t2v.data(), sizeof(float2) * s->n2, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { int st = cuda_status(e, "scan_create: twiddles"); destroy(s); return st; }
+    s->p0 = make_line_plan(s->n0);
+    s->p1 = make_line_plan(s->n1);
+    s->pm = make_line_plan(s->n2 / 2);
+    s->W1 = std::max(1, std::min(s->h2, kTile / s->n1));
+    s->W2 = std::max(1, std::min(s->h2, kTile / s->n0));
+    s->W3 = s->W1;
+    s->R4 = std::max(1, std::min(kTile / std::max(1, s->n2 / 2), (kThreads * kMaxV) / s->n2));
+    s->smem1 = sizeof(float2) * (s->n1 + s->n2 + (size_t)s->n1 * s->W1) + sizeof(float) * s->t1 * s->t2;
+    s->smem2 = sizeof(float2) * (s->n0 + (size_t)s->n0 * s->W2);
+    s->smem3 = sizeof(float2) * (s->n1 + (size_t)s->n1 * s->W3);
+    s->smem4 = sizeof(float2) * (s->n2 + (size_t)s->R4 * s->h2 + (size_t)s->R4 * (s->n2 / 2));
+    size_t mx = std::max(std::max(s->smem1, s->smem2), std::max(s->smem3, s->smem4));
+    if (mx > 200 * 1024) {
+      set_error("scan_create: shared-memory tile of %zu bytes exceeds the limit", mx);
+      destroy(s);
+      return TM_E_UNSUPPORTED;
+    }
+    cudaFuncSetAttribute(tmpl_zy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem1);
+    cudaFuncSetAttribute(xpass_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem2);
+    cudaFuncSetAttribute(xpass_kernel<__half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem2);
+    cudaFuncSetAttribute(ypass_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem3);
+    cudaFuncSetAttribute(ypass_kernel<__half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem3);
+    cudaFuncSetAttribute(zpass_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem4);
+    cudaFuncSetAttribute(zpass_kernel<__half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem4);
+  }
+  // ---- cuFFT plans: fast-shape r2c/c2r (setup and plain path), template-shape (filter)
+  int r;
+  r = cufftPlan3d(&s->fwd, s->n0, s->n1, s->n2, CUFFT_R2C);
+  if (r == CUFFT_SUCCESS) r = cufftPlan3d(&s->inv, s->n0, s->n1, s->n2, CUFFT_C2R);
+  if (r != CUFFT_SUCCESS) { int st = cufft_status((cufftResult)r, "scan_create: fast plans"); destroy(s); return st; }
+  s->have_fwd = true;
+  int ts[3] = {s->t0, s->t1, s->t2};
+  r = cufftPlanMany(&s->tfwd, 3, ts, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, B);
+  if (r == CUFFT_SUCCESS)
+    r = cufftPlanMany(&s->tinv, 3, ts, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, B);
+  if (r != CUFFT_SUCCESS) { int st = cufft_status((cufftResult)r, "scan_create: template plans"); destroy(s); return st; }
+  s->have_tfwd = true;
+  *out = s;
+  return TM_OK;
+}
+
+int64_t scan_device_bytes(const Scan* s) { return (int64_t)s->bytes; }
+
+// target: fast-shaped (top-left padded, already filtered) float32 device array.
+int scan_set_target(Scan* s, const float* target, cudaStream_t stream) {
+  TM_REQUIRE(s && target, "scan_set_target: null pointer");
+  TM_TRY(cuda_status(cudaStreamSynchronize(stream), "scan_set_target: sync"));
+  cufftSetStream(s->fwd, stream);
+  cufftSetStream(s->inv, stream);
+  const int64_t N = s->N, S = s->S;
+  if (s->d.score == TM_SCORE_CC) {
+    // CC correlates the raw target (cc_setup, tme/matching_scores.py:153-189)
+    float* tmp = nullptr;
+    TM_TRY(cuda_status(cudaMallocAsync((void**)&tmp, sizeof(float) * N, stream), "scan_set_target: alloc"));
+    cudaMemcpyAsync(tmp, target, sizeof(float) * N, cudaMemcpyDeviceToDevice, stream);
+    int r = cufftExecR2C(s->fwd, tmp, (cufftComplex*)s->ft_target);
+    cudaFreeAsync(tmp, stream);
+    TM_TRY(cufft_status((cufftResult)r, "scan_set_target: r2c"));
+    s->target_ready = true;
+    return check_launch("scan_set_target");
+  }
+  // mean in double; the normalised scores are invariant to a constant target offset
+  // because the normalised template sums to zero, so the spectra are taken of the
+  // centred target, which keeps E[x^2] - E[x]^2 well conditioned.
+  const int nparts = 592;
+  double* partial = nullptr;
+  float* centred = nullptr;
+  TM_TRY(cuda_status(cudaMallocAsync((void**)&partial, sizeof(double) * nparts, stream), "alloc"));
+  TM_TRY(cuda_status(cudaMallocAsync((void**)&centred, sizeof(float) * N, stream), "alloc"));
+  sum_double_kernel<<<nparts, 256, 0, stream>>>(target, N, partial);
+  center_kernel<<<grid_for(N), 256, 0, stream>>>(target, partial, nparts, N, centred, nullptr, nullptr);
+  TM_TRY(check_launch("scan_set_target: centre"));
+  std::vector<double> hp(nparts);
+  cudaMemcpyAsync(hp.data(), partial, sizeof(double) * nparts, cudaMemcpyDeviceToHost, stream);
+  TM_TRY(cuda_status(cudaStreamSynchronize(stream), "scan_set_target: mean"));
+  double tot = 0.0;
+  for (double v : hp) tot += v;
+  s->target_mean = tot / (double)N;
+  int r;
+  if (s->d.score == TM_SCORE_FLC) {
+    // flc_setup (tme/matching_scores.py:357-387): spectra of f and f^2
+    float* sq = nullptr;
+    TM_TRY(cuda_status(cudaMallocAsync((void**)&sq, sizeof(float) * N, stream), "alloc"));
+    square_kernel<<<grid_for(N), 256, 0, stream>>>(centred, sq, N);
+    r = cufftExecR2C(s->fwd, centred, (cufftComplex*)s->ft_target);
+    if (r == CUFFT_SUCCESS) r = cufftExecR2C(s->fwd, sq, (cufftComplex*)s->ft_target2);
+    cudaFreeAsync(sq, stream);
+  } else {
+    // flcSphericalMask_setup (tme/matching_scores.py:390-450): the local-variance
+    // denominator from CC(f^2, m) and CC(f, m), here in double precision.
+    TM_REQUIRE(s->template_ready, "scan_set_target: FLCSphericalMask needs the template mask first");
+    cufftHandle dfwd, dinv;
+    r = cufftPlan3d(&dfwd, s->n0, s->n1, s->n2, CUFFT_D2Z);
+    if (r != CUFFT_SUCCESS) { cudaFreeAsync(centred, stream); cudaFreeAsync(partial, stream); return cufft_status((cufftResult)r, "scan_set_target: D2Z plan"); }
+    r = cufftPlan3d(&dinv, s->n0, s->n1, s->n2, CUFFT_Z2D);
+    if (r != CUFFT_SUCCESS) { cufftDestroy(dfwd); cudaFreeAsync(centred, stream); cudaFreeAsync(partial, stream); return cufft_status((cufftResult)r, "scan_set_target: Z2D plan"); }
+    cufftSetStream(dfwd, stream);
+    cufftSetStream(dinv, stream);
+    double *f = nullptr, *f2 = nullptr;
+    double2 *Ff = nullptr, *Ff2 = nullptr, *Fm = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&f, sizeof(double) * N, stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&f2, sizeof(double) * N, stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&Ff, sizeof(double2) * S, stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&Ff2, sizeof(double2) * S, stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&Fm, sizeof(double2) * S, stream);
+    if (e != cudaSuccess) {
+      cufftDestroy(dfwd); cufftDestroy(dinv);
+      return cuda_status(e, "scan_set_target: FP64 buffers");
+    }
+    center_kernel<<<grid_for(N), 256, 0, stream>>>(target, partial, nparts, N, nullptr, f, f2);
+    r = cufftExecD2Z(dfwd, f, Ff);
+    if (r == CUFFT_SUCCESS) r = cufftExecD2Z(dfwd, f2, Ff2);
+    // mask: top-left padded into f (reused)
+    cudaMemsetAsync(f, 0, sizeof(double) * N, stream);
+    pad_double_kernel<<<grid_for(s->T), 256, 0, stream>>>(s->mask, s->t0, s->t1, s->t2, f, s->n1, s->n2);
+    if (r == CUFFT_SUCCESS) r = cufftExecD2Z(dfwd, f, Fm);
+    zmul_kernel<<<grid_for(S), 256, 0, stream>>>(Ff, Fm, Ff, S);
+    zmul_kernel<<<grid_for(S), 256, 0, stream>>>(Ff2, Fm, Ff2, S);
+    if (r == CUFFT_SUCCESS) r = cufftExecZ2D(dinv, Ff, f);
+    if (r == CUFFT_SUCCESS) r = cufftExecZ2D(dinv, Ff2, f2);
+    inv_den_kernel<<<grid_for(N), 256, 0, stream>>>(f, f2, 1.0 / (double)N, s->mask_sum,
+                                                   (double)1.1920928955078125e-07, s->inv_den, N);
+    if (r == CUFFT_SUCCESS) r = cufftExecR2C(s->fwd, centred, (cufftComplex*)s->ft_target);
+    cudaFreeAsync(f, stream); cudaFreeAsync(f2, stream);
+    cudaFreeAsync(Ff, stream); cudaFreeAsync(Ff2, stream); cudaFreeAsync(Fm, stream);
+    cudaStreamSynchronize(stream);
+    cufftDestroy(dfwd);
+    cufftDestroy(dinv);
+  }
+  cudaFreeAsync(centred, stream);
+  cudaFreeAsync(partial, stream);
+  TM_TRY(cufft_status((cufftResult)r, "scan_set_target: transforms"));
+  s->target_ready = true;
+  return check_launch("scan_set_target");
+}
+
+// template/mask: reversed (t0,t1,t2) float32 device arrays; filter: (t0,t1,t2//2+1) or null.
+int scan_set_template(Scan* s, const float* tmpl, const float* mask, const float* filt,
+                      cudaStream_t stream) {
+  TM_REQUIRE(s && tmpl, "scan_set_template: null template");
+  TM_REQUIRE(s->d.score == TM_SCORE_CC || mask, "scan_set_template: this score needs a mask");
+  cudaMemcpyAsync(s->tmpl, tmpl, sizeof(float) * s->T, cudaMemcpyDeviceToDevice, stream);
+  if (mask) cudaMemcpyAsync(s->mask, mask, sizeof(float) * s->T, cudaMemcpyDeviceToDevice, stream);
+  s->d.has_template_filter = filt != nullptr;
+  if (filt) cudaMemcpyAsync(s->tfilter, filt, sizeof(float) * s->TS, cudaMemcpyDeviceToDevice, stream);
+  if (mask) {
+    // n_obs = sum(mask) in the backend float dtype (corr_scoring, matching_scores.py:573-576)
+    double* partial = nullptr;
+    const int nparts = 64;
+    TM_TRY(cuda_status(cudaMallocAsync((void**)&partial, sizeof(double) * nparts, stream), "alloc"));
+    sum_double_kernel<<<nparts, 256, 0, stream>>>(s->mask, s->T, partial);
+    std::vector<double> hp(nparts);
+    cudaMemcpyAsync(hp.data(), partial, sizeof(double) * nparts, cudaMemcpyDeviceToHost, stream);
+    cudaFreeAsync(partial, stream);
+    TM_TRY(cuda_status(cudaStreamSynchronize(stream), "scan_set_template: mask sum"));
+    double tot = 0.0;
+    for (double v : hp) tot += v;
+    s->mask_sum = tot;
+  }
+  s->template_ready = true;
+  return check_launch("scan_set_template");
+}
+
+// rotate, filter and normalise B templates of the current group into rot_t (and rot_m for FLC)
+static int prepare_templates(Scan* s, int nb, cudaStream_t stream) {
+  const bool flc = s->d.score == TM_SCORE_FLC;
+  TM_TRY(rigid_transform(s->tmpl, flc ? s->mask : nullptr, s->t0, s->t1, s->t2, s->mat, nb,
+                         s->rot_t, flc ? s->rot_m : nullptr, s->t0, s->t1, s->t2, stream));
+  if (s->d.has_template_filter) {
+    // _apply_filter_subset (tme/matching_scores.py:125-135): rfftn -> * filter -> irfftn
+    cufftSetStream(s->tfwd, stream);
+    cufftSetStream(s->tinv, stream);
+    TM_TRY(cufft_status(cufftExecR2C(s->tfwd, s->rot_t, (cufftComplex*)s->tspec), "filter r2c"));
+    TM_TRY(apply_real_filter(s->tspec, s->tfilter, s->TS, s->B, stream));
+    TM_TRY(cufft_status(cufftExecC2R(s->tinv, (cufftComplex*)s->tspec, s->rot_t), "filter c2r"));
+    TM_TRY(scale_real(s->rot_t, (float)(1.0 / (double)s->T), s->T * s->B, stream));
+  }
+  if (s->d.score == TM_SCORE_FLCSM) {
+    TM_TRY(normalize_template(s->rot_t, s->mask, 0, s->t0, s->t1, s->t2, s->t1, s->t2, s->T, nb,
+                              s->mask_sum, s->stats_ws, stream));
+  } else if (flc) {
+    TM_TRY(normalize_template(s->rot_t, s->rot_m, s->T, s->t0, s->t1, s->t2, s->t1, s->t2, s->T,
+                              nb, 0.0, s->stats_ws, stream));
+  }
+  return TM_OK;
+}
+
+static int run_plain(Scan* s, int n, int32_t first_index, float* state_max, int32_t* state_rot,
+                     const float* matrices, cudaStream_t stream) {
+  const int64_t N = s->N, S = s->S;
+  const float scale = (float)(1.0 / (double)N);
+  const double eps = 1.1920928955078125e-07;
+  const bool flc = s->d.score == TM_SCORE_FLC;
+  cufftSetStream(s->fwd, stream);
+  cufftSetStream(s->inv, stream);
+  for (int i = 0; i < n; ++i) {
+    cudaMemcpyAsync(s->mat, matrices + (int64_t)i * 16, sizeof(float) * 16,
+                    cudaMemcpyDeviceToDevice, stream);
+    TM_TRY(prepare_templates(s, 1, stream));
+    cudaMemsetAsync(s->arr, 0, sizeof(float) * N, stream);
+    TM_TRY(pad_box(s->rot_t, s->t0, s->t1, s->t2, s->arr, s->n1, s->n2, stream));
+    if (flc) {
+      cudaMemsetAsync(s->arr_m, 0, sizeof(float) * N, stream);
+      TM_TRY(pad_box(s->rot_m, s->t0, s->t1, s->t2, s->arr_m, s->n1, s->n2, stream));
+      TM_TRY(cufft_status(cufftExecR2C(s->fwd, s->arr_m, (cufftComplex*)s->spec_m), "r2c mask"));
+      TM_TRY(complex_multiply(s->ft_target, s->spec_m, s->spec, S, stream));
+      TM_TRY(cufft_status(cufftExecC2R(s->inv, (cufftComplex*)s->spec, s->cc_m), "c2r"));
+      TM_TRY(complex_multiply(s->ft_target2, s->spec_m, s->spec, S, stream));
+      TM_TRY(cufft_status(cufftExecC2R(s->inv, (cufftComplex*)s->spec, s->cc_m2), "c2r"));
+    }
+    TM_TRY(cufft_status(cufftExecR2C(s->fwd, s->arr, (cufftComplex*)s->spec), "r2c"));
+    TM_TRY(complex_multiply(s->ft_target, s->spec, s->spec, S, stream));
+    TM_TRY(cufft_status(cufftExecC2R(s->inv, (cufftComplex*)s->spec, s->arr), "c2r"));
+    const double* stats = s->stats_ws + (int64_t)1 * kStatChunks * 3;
+    TM_TRY(plain_epilogue(s->arr, s->inv_den, flc ? s->cc_m : nullptr, flc ? s->cc_m2 : nullptr,
+                          stats, eps, scale, state_max, state_rot, first_index + i, N, stream));
+  }
+  return TM_OK;
+}
+
+static int run_fused(Scan* s, int n, int32_t first_index, float* state_max, int32_t* state_rot,
+                     const float* matrices, cudaStream_t stream) {
+  const double Nd = (double)s->N;
+  // H holds the product after two inverse passes scaled by hs; the z pass divides by
+  // N * hs. hs keeps half2 storage in range (see the precision note in the header).
+  double hs = 1.0;
+  if (s->half) hs = 1.0 / (sqrt(Nd) * sqrt((double)s->n0) * sqrt(std::max(1.0, s->mask_sum)));
+  const float out_scale = (float)(1.0 / (Nd * hs));
+  for (int g0 = 0; g0 < n; g0 += s->B) {
+    const int nb = std::min(s->B, n - g0);
+    cudaMemcpyAsync(s->mat, matrices + (int64_t)g0 * 16, sizeof(float) * 16 * nb,
+                    cudaMemcpyDeviceToDevice, stream);
+    StageTimer tmr(s, stream);
+    tmr.begin();
+    TM_TRY(prepare_templates(s, nb, stream));
+    tmr.end(TM_STAGE_PREPARE);
+    dim3 g1(ceil_div(s->h2, s->W1), s->t0, nb);
+    tmr.begin();
+    tmpl_zy_kernel<<<g1, kThreads, s->smem1, stream>>>(s->rot_t, s->t0, s->t1, s->t2, s->n1,
+                                                       s->n2, s->h2, s->W1, s->p1, s->tw1,
+                                                       s->tw2, s->G);
+    TM_TRY(check_launch("tmpl_zy_kernel"));
+    tmr.end(TM_STAGE_TEMPLATE);
+    dim3 g2(ceil_div(s->h2, s->W2), s->n1);
+    dim3 g3(ceil_div(s->h2, s->W3), s->n0, nb);
+    const int64_t rows = (int64_t)s->n0 * s->n1;
+    dim3 g4(ceil_div(rows, s->R4));
+    if (s->half) {
+      __half2* H = static_cast<__half2*>(s->H);
+      tmr.begin();
+      xpass_kernel<__half2><<<g2, kThreads, s->smem2, stream>>>(s->G, s->ft_target, nb, s->t0, s->n0, s->n1, s->h2, s->W2, s->p0, s->tw0, (float)hs, H);
+      TM_TRY(check_launch("xpass_kernel"));
+      tmr.end(TM_STAGE_XPASS);
+      tmr.begin();
+      ypass_kernel<__half2><<<g3, kThreads, s->smem3, stream>>>(H, s->n0, s->n1, s->h2, s->W3, s->p1, s->tw1);
+      TM_TRY(check_launch("ypass_kernel"));
+      tmr.end(TM_STAGE_YPASS);
+      tmr.begin();
+      zpass_kernel<__half2><<<g4, kThreads, s->smem4, stream>>>(H, nb, rows, s->n2, s->h2, s->R4, s->pm, s->tw2, out_scale, s->inv_den, first_index + g0, state_max, state_rot, s->S);
+      TM_TRY(check_launch("zpass_kernel"));
+      tmr.end(TM_STAGE_ZPASS);
+    } else {
+      float2* H = static_cast<float2*>(s->H);
+      tmr.begin();
+      xpass_kernel<float2><<<g2, kThreads, s->smem2, stream>>>(s->G, s->ft_target, nb, s->t0, s->n0, s->n1, s->h2, s->W2, s->p0, s->tw0, (float)hs, H);
+      TM_TRY(check_launch("xpass_kernel"));
+      tmr.end(TM_STAGE_XPASS);
+      tmr.begin();
+      ypass_kernel<float2><<<g3, kThreads, s->smem3, stream>>>(H, s->n0, s->n1, s->h2, s->W3, s->p1, s->tw1);
+      TM_TRY(check_launch("ypass_kernel"));
+      tmr.end(TM_STAGE_YPASS);
+      tmr.begin();
+      zpass_kernel<float2><<<g4, kThreads, s->smem4, stream>>>(H, nb, rows, s->n2, s->h2, s->R4, s->pm, s->tw2, out_scale, s->inv_den, first_index + g0, state_max, state_rot, s->S);
+      TM_TRY(check_launch("zpass_kernel"));
+      tmr.end(TM_STAGE_ZPASS);
+    }
+  }
+  return TM_OK;
+}
+
+int scan_set_timing(Scan* s, int enable) {
+  TM_REQUIRE(s, "scan_set_timing: null plan");
+  if (enable && !s->have_events) {
+    for (auto& e : s->ev) TM_TRY(cuda_status(cudaEventCreate(&e), "scan_set_timing: event"));
+    s->have_events = true;
+  }
+  s->timing = enable != 0;
+  for (int i = 0; i < TM_NUM_STAGES; ++i) { s->stage_ms[i] = 0.0; s->stage_launches[i] = 0; }
+  return TM_OK;
+}
+
+int scan_get_timing(const Scan* s, double* ms, int64_t* launches) {
+  TM_REQUIRE(s && ms && launches, "scan_get_timing: null pointer");
+  for (int i = 0; i < TM_NUM_STAGES; ++i) { ms[i] = s->stage_ms[i]; launches[i] = s->stage_launches[i]; }
+  return TM_OK;
+}
+
+int64_t scan_stage_bytes(const Scan* s, int stage, int nb) {
+  // Algorithmic HBM bytes of one launch of a stage for a group of nb rotations:
+  // every array the stage must read or write once, at its storage width.
+  const int64_t e = s->half ? 4 : 8;
+  const int64_t G = (int64_t)nb * s->t0 * s->n1 * s->h2 * 8;
+  switch (stage) {
+    case TM_STAGE_TEMPLATE: return (int64_t)nb * s->T * 4 + G;
+    case TM_STAGE_XPASS: return G + s->S * 8 + (int64_t)nb * s->S * e;
+    case TM_STAGE_YPASS: return 2 * (int64_t)nb * s->S * e;
+    case TM_STAGE_ZPASS:
+      return (int64_t)nb * s->S * e + s->N * (s->inv_den ? 4 : 0) + s->N * 16;
+    default: return 0;
+  }
+}
+
+int scan_run(Scan* s, const float* matrices, int n, int32_t first_index, float* state_max,
+             int32_t* state_rot, cudaStream_t stream) {
+  TM_REQUIRE(s && state_max && state_rot, "scan_run: null pointer");
+  TM_REQUIRE(n == 0 || matrices, "scan_run: null matrices");
+  TM_REQUIRE(s->target_ready && s->template_ready, "scan_run: target and template must be set");
+  TM_REQUIRE(n >= 0, "scan_run: negative rotation count");
+  if (n == 0) return TM_OK;
+  return s->fused ? run_fused(s, n, first_index, state_max, state_rot, matrices, stream)
+                  : run_plain(s, n, first_index, state_max, state_rot, matrices, stream);
+}
+
+// Line-FFT self test: y[l][:] = FFT_dir(x[l][:]) for `lines` lines of length n
+// (interleaved smem tile), used by the test-suite to check the device FFT code.
+__global__ void line_fft_test_kernel(const float2* x, float2* y, int n, int lines, LinePlan p,
+                                     const float2* tw_g, int dir) {
+  extern __shared__ float4 smem_raw[];
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  float2* buf = tw + n;
+  for (int i = threadIdx.x; i < n; i += kThreads) tw[i] = tw_g[i];
+  for (int e = threadIdx.x; e < n * lines; e += kThreads) {
+    int i = e / lines, l = e % lines;
+    buf[e] = x[(int64_t)l * n + i];
+  }
+  __syncthreads();
+  if (dir < 0) fft::fft_lines<-1, kMaxE, true>(buf, p, lines, 1, lines, tw, n, threadIdx.x, kThreads);
+  else fft::fft_lines<1, kMaxE, true>(buf, p, lines, 1, lines, tw, n, threadIdx.x, kThreads);
+  for (int e = threadIdx.x; e < n * lines; e += kThreads) {
+    int i = e / lines, l = e % lines;
+    y[(int64_t)l * n + i] = buf[e];
+  }
+}
+
+int line_fft_test(const void* x, void* y, int n, int lines, int dir, cudaStream_t stream) {
+  TM_REQUIRE(line_supported(n), "line_fft_test: length %d not supported", n);
+  TM_REQUIRE(lines >= 1 && (int64_t)n * lines <= kTile, "line_fft_test: tile too large");
+  LinePlan p = make_line_plan(n);
+  auto tv = twiddle_table(n);
+  float2* tw = nullptr;
+  TM_TRY(cuda_status(cudaMalloc(&tw, sizeof(float2) * n), "line_fft_test: alloc"));
+  cudaMemcpy(tw, tv.data(), sizeof(float2) * n, cudaMemcpyHostToDevice);
+  size_t smem = sizeof(float2) * (n + (size_t)n * lines);
+  cudaFuncSetAttribute(line_fft_test_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  line_fft_test_kernel<<<1, kThreads, smem, stream>>>((const float2*)x, (float2*)y, n, lines, p, tw, dir);
+  int st = check_launch("line_fft_test_kernel");
+  cudaStreamSynchronize(stream);
+  cudaFree(tw);
+  return st;
+}
+
+}  // namespace tmb

@@ -1,0 +1,93 @@
+"""Peak-calling helpers: maximum-filter peaks and the greedy distance filter on the
+device, plus the reference's top-k ordering.
+
+``max_filter_coordinates`` follows NumpyFFTWBackend.max_filter_coordinates
+(tme/backends/npfftw_backend.py:200-206) through ``tm_max_filter_peaks``;
+``filter_points_indices`` follows tme/analyzer/peaks.py:68-106 with the greedy
+filter of find_candidate_indices (tme/external/bindings.cpp:85-126) running as
+``tm_find_candidate_indices``; ``topk_indices`` is the reference's
+argpartition/argsort ordering (tme/backends/npfftw_backend.py:177-182) on the
+small candidate arrays.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+__all__ = ["max_filter_coordinates", "find_candidate_indices", "filter_points_indices",
+           "topk_indices", "topk_indices_device"]
+
+
+def _dev():
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def max_filter_coordinates(scores, min_distance: int) -> np.ndarray:
+    """(n, 3) int64 coordinates where the box maximum filter of edge ``min_distance``
+    equals the score, in C order (as ``np.nonzero`` returns them)."""
+    s = scores if isinstance(scores, torch.Tensor) else torch.as_tensor(
+        np.ascontiguousarray(scores, dtype=np.float32))
+    s = s.to(device=_dev(), dtype=torch.float32).contiguous()
+    if s.ndim != 3:
+        raise NotImplementedError("peak calling is implemented for 3D score maps")
+    a = torch.empty_like(s)
+    b = torch.empty_like(s)
+    mask = torch.empty(s.shape, dtype=torch.uint8, device=s.device)
+    N.check(N.lib.tm_max_filter_peaks(N.ptr(s), *s.shape, int(min_distance), N.ptr(a), N.ptr(b),
+                                      N.ptr(mask), N.stream_ptr()), "tm_max_filter_peaks")
+    return torch.nonzero(mask).cpu().numpy().astype(np.int64)
+
+
+def find_candidate_indices(coordinates, min_distance: int) -> np.ndarray:
+    """Greedy filter on the device; returns the kept indices in input order."""
+    c = np.ascontiguousarray(np.asarray(coordinates), dtype=np.int64)
+    n = int(c.shape[0])
+    if n == 0:
+        return np.zeros(0, dtype=np.int64)
+    if c.ndim != 2 or c.shape[1] != 3:
+        raise NotImplementedError("the greedy filter is implemented for 3D coordinates")
+    dev = _dev()
+    ct = torch.as_tensor(c, device=dev)
+    out = torch.empty(n, dtype=torch.int32, device=dev)
+    cnt = torch.zeros(1, dtype=torch.int32, device=dev)
+    ws_bytes = int(N.lib.tm_find_candidate_indices_workspace(n))
+    ws = torch.empty(max(ws_bytes, 8), dtype=torch.uint8, device=dev)
+    N.check(N.lib.tm_find_candidate_indices(N.ptr(ct), n, int(min_distance), N.ptr(out),
+                                            N.ptr(cnt), N.ptr(ws), N.stream_ptr()),
+            "tm_find_candidate_indices")
+    k = int(cnt.item())
+    return out[:k].cpu().numpy().astype(np.int64)
+
+
+def filter_points_indices(coordinates, min_distance: float, scores=None) -> np.ndarray:
+    """tme/analyzer/peaks.py:68-106 (unbatched, below the bucketing cutoff)."""
+    coordinates = np.asarray(coordinates)
+    if min_distance <= 0:
+        return np.arange(coordinates.shape[0])
+    if coordinates.shape[0] == 0:
+        return np.zeros(0, dtype=np.int64)
+    if scores is not None:
+        order = np.argsort(-np.asarray(scores))
+        kept = find_candidate_indices(coordinates[order], int(min_distance))
+        return order[kept]
+    return find_candidate_indices(coordinates, int(min_distance))
+
+
+def topk_indices(arr, k: int) -> np.ndarray:
+    """Indices of the k largest entries of a 1D array, largest first."""
+    temp = np.asarray(arr).reshape(-1)
+    k = min(int(k), temp.size)
+    if k <= 0:
+        return np.zeros(0, dtype=np.int64)
+    idx = np.argpartition(temp, -k)[-k:][:k]
+    return idx[np.argsort(temp[idx])][::-1]
+
+
+def topk_indices_device(scores, k: int) -> np.ndarray:
+    """(k, ndim) coordinates of the k largest scores of a device score map."""
+    s = scores if isinstance(scores, torch.Tensor) else torch.as_tensor(np.asarray(scores))
+    s = s.to(device=_dev(), dtype=torch.float32)
+    vals, idx = torch.topk(s.reshape(-1), int(k), largest=True, sorted=True)
+    return np.stack(np.unravel_index(idx.cpu().numpy(), tuple(s.shape)), axis=1)

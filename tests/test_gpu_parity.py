@@ -1,0 +1,212 @@
+"""GPU parity: the CUDA path against the oracle and the reference's golden vectors.
+
+Tolerances: scores within 1e-4 absolute of the reference FP32 map and of the FP64
+map. Rotation indices must agree except at near-ties: with
+both maps within 1e-4, a different argmax means two rotations score within 2e-4,
+and such voxels must stay rare (<= 1e-4 of the map)."""
+import numpy as np
+import pytest
+
+from oracle import tm_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _scan(score, target, template, mask, rotations, precision="fp32", plain=False, batch=16,
+          template_filter=None, target_filter=None, pad=False, splits=None, callback=None,
+          callback_args=None):
+    import pytme_b200 as P
+    from pytme_b200.analyzer import MaxScoreOverRotations
+
+    P.backend.change_backend("b200", precision=precision, rotation_batch=batch, plain=plain)
+    md = P.MatchingData(target.copy(), template.copy())
+    if mask is not None:
+        md.template_mask = mask.copy()
+    md.rotations = rotations
+    md.template_filter = template_filter
+    md.target_filter = target_filter
+    setup, scoring = P.MATCHING_EXHAUSTIVE_REGISTER[score]
+    return P.scan_subsets(md, matching_score=scoring, matching_setup=setup,
+                          callback_class=callback or MaxScoreOverRotations,
+                          callback_class_args=callback_args or {"score_threshold": 0},
+                          job_schedule=(1, 1), interpolation_order=1,
+                          pad_target_edges=pad, target_splits=splits or {})
+
+
+@pytest.mark.parametrize("precision,plain", [("fp32", True), ("fp32", False), ("mixed", False)])
+def test_flcsm_config1_matches_reference(torch_cuda, golden, precision, plain):
+    g = golden("c1_flcsm.npz")
+    r = _scan("FLCSphericalMask", g["target"], g["template"], g["mask"], g["rotations"],
+              precision=precision, plain=plain)
+    s, rot = r[0], r[2]
+    assert s.shape == g["scores32"].shape
+    err32 = np.abs(s - g["scores32"]).max()
+    err64 = np.abs(s - g["scores64"]).max()
+    assert err32 <= TOL, err32
+    assert err64 <= TOL, err64
+    # a different argmax is only possible where two rotations score within 2*TOL of
+    # each other (both maps agree within TOL), i.e. at near-ties; there must be few
+    mism = rot != g["rot32"].astype(np.int32)
+    total = int(np.count_nonzero(mism))
+    assert total <= max(5, int(1e-4 * s.size)), total
+    # rotation mapping covers every rotation in order
+    assert len(r[3]) == g["rotations"].shape[0]
+    assert np.array_equal(r[3][5], g["rotations"][5])
+
+
+def test_cc_matches_reference(torch_cuda, golden):
+    g = golden("cc_small.npz")
+    for plain in (True, False):
+        r = _scan("CC", g["target"], g["template"], None, g["rotations"], plain=plain)
+        # CC scores are raw correlations (order 10-100): relative tolerance
+        scale = np.abs(g["scores32"]).max()
+        assert np.abs(r[0] - g["scores32"]).max() <= TOL * scale
+        assert np.count_nonzero(r[2] != g["rot32"]) <= 5
+
+
+def test_flc_filtered_matches_reference(torch_cuda, golden):
+    g = golden("flc_filt.npz")
+    r = _scan("FLC", g["target"], g["template"], g["mask"], g["rotations"], plain=True,
+              template_filter=g["template_filter"], target_filter=g["target_filter"])
+    assert np.abs(r[0] - g["scores32"]).max() <= TOL
+    assert np.abs(r[0] - g["scores64"]).max() <= TOL
+    assert np.count_nonzero(r[2] != g["rot64"]) <= 5
+
+
+@pytest.mark.parametrize("precision,plain", [("fp32", True), ("mixed", False)])
+def test_dc_offset_tracks_fp64(torch_cuda, golden, precision, plain):
+    g = golden("flcsm_dc.npz")
+    r = _scan("FLCSphericalMask", g["target"], g["template"], g["mask"], g["rotations"],
+              precision=precision, plain=plain)
+    # FP64 denominator and a centred target keep the error far below the reference's
+    # own FP32 error at this offset
+    err64 = np.abs(r[0] - g["scores64"]).max()
+    ref_err = np.abs(g["scores32"] - g["scores64"]).max()
+    assert err64 <= TOL, err64
+    assert err64 < ref_err
+
+
+@pytest.mark.parametrize("score", ["CC", "FLC", "FLCSphericalMask"])
+@pytest.mark.parametrize("pad", [False, True])
+def test_reference_box_kat(torch_cuda, golden, score, pad):
+    """tests/test_matching_exhaustive.py of the reference: exact peak [25, 17, 12]."""
+    from pytme_b200.analyzer import PeakCallerSort
+
+    g = golden("kat_exhaustive.npz")
+    target = np.zeros((80, 80, 80))
+    target[25:31, 22:28, 12:16] = 1
+    template = np.zeros((41, 41, 35))
+    template[20:26, 25:31, 17:21] = 1
+    mask = np.ones_like(template)
+    r = _scan(score, target, template, mask, np.eye(3, dtype=np.float32)[None], plain=True,
+              pad=pad, splits={0: 2}, callback=PeakCallerSort, callback_args={})
+    peak, sc = r[0][0], r[2][0]
+    assert np.array_equal(peak, [25, 17, 12])
+    assert np.array_equal(peak, g[f"{score}_{int(pad)}_peak"])
+    assert abs(float(sc) - float(g[f"{score}_{int(pad)}_score"])) <= 1e-3 * max(1, abs(float(sc)))
+    r = _scan(score, target, template, mask, np.eye(3, dtype=np.float32)[None], plain=True,
+              pad=pad)
+    m = r[0]
+    assert tuple(m.shape) == tuple(g[f"{score}_{int(pad)}_shape"])
+    assert tuple(np.unravel_index(np.argmax(m), m.shape)) == tuple(g[f"{score}_{int(pad)}_argmax"])
+
+
+def test_rigid_transform_matches_reference(torch_cuda, golden):
+    import pytme_b200 as P
+
+    g = golden("rigid.npz")
+    be = P.backend
+    be.change_backend("b200")
+    data = torch_cuda.as_tensor(g["data"], device="cuda")
+    for i in range(g["rotations"].shape[0]):
+        out, _ = be.rigid_transform(arr=data, rotation_matrix=torch_cuda.as_tensor(
+            g["matrices"][i], device="cuda"), order=1, out=torch_cuda.zeros_like(data))
+        np.testing.assert_allclose(out.cpu().numpy(), g["out"][i], rtol=0, atol=2e-6)
+        big = torch_cuda.zeros((16, 16, 16), device="cuda")
+        bigm = torch_cuda.zeros((16, 16, 16), device="cuda")
+        o2, om = be.rigid_transform(arr=data, arr_mask=torch_cuda.as_tensor(g["mask"], device="cuda"),
+                                    rotation_matrix=torch_cuda.as_tensor(g["rotations"][i], device="cuda"),
+                                    out=big, out_mask=bigm, use_geometric_center=True, order=1)
+        np.testing.assert_allclose(o2.cpu().numpy(), g["out_pad"][i][0], rtol=0, atol=2e-6)
+        np.testing.assert_allclose(om.cpu().numpy(), g["out_pad"][i][1], rtol=0, atol=2e-6)
+
+
+@pytest.mark.parametrize("n", [8, 16, 50, 64, 100, 128, 160, 200, 256, 320, 384, 512, 1000])
+def test_line_fft_matches_numpy(torch_cuda, n):
+    from pytme_b200 import _native as N
+
+    lines = max(1, min(8, 4096 // n))
+    rng = np.random.default_rng(n)
+    x = (rng.normal(size=(lines, n)) + 1j * rng.normal(size=(lines, n))).astype(np.complex64)
+    xt = torch_cuda.as_tensor(x, device="cuda")
+    for d in (-1, 1):
+        yt = torch_cuda.empty_like(xt)
+        N.check(N.lib.tm_line_fft_test(N.ptr(xt), N.ptr(yt), n, lines, d, N.stream_ptr()))
+        ref = np.fft.fft(x.astype(np.complex128), axis=1) if d < 0 else \
+            np.fft.ifft(x.astype(np.complex128), axis=1) * n
+        err = np.abs(yt.cpu().numpy() - ref).max() / np.abs(ref).max()
+        assert err < 2e-6, (n, d, err)
+
+
+def test_norm_scores_and_max_update(torch_cuda):
+    import pytme_b200 as P
+
+    be = P.backend
+    be.change_backend("b200")
+    rng = np.random.default_rng(3)
+    n = 4099
+    arr = rng.normal(size=n).astype(np.float32)
+    e2 = rng.uniform(1, 3, size=n).astype(np.float32) * 50
+    e1 = rng.normal(size=n).astype(np.float32) * 5
+    out = torch_cuda.empty(n, device="cuda")
+    be.norm_scores(torch_cuda.as_tensor(arr, device="cuda"), torch_cuda.as_tensor(e2, device="cuda"),
+                   torch_cuda.as_tensor(e1, device="cuda"), 50.0, 1.1920929e-07, out)
+    ref = O.norm_scores(arr.astype(np.float64), e2.astype(np.float64), e1.astype(np.float64), 50.0,
+                        1.1920929e-07, np.empty(n))
+    np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=1e-6, atol=1e-7)
+    mx = torch_cuda.zeros(n, device="cuda")
+    rt = torch_cuda.full((n,), -1, dtype=torch_cuda.int32, device="cuda")
+    s1 = torch_cuda.as_tensor(arr, device="cuda")
+    be.max_score_over_rotations(s1, mx, rt, 3)
+    be.max_score_over_rotations(s1, mx, rt, 4)  # equal scores keep the first index
+    h = arr > 0
+    assert np.array_equal(rt.cpu().numpy(), np.where(h, 3, -1))
+    assert np.array_equal(mx.cpu().numpy(), np.where(h, arr, 0))
+
+
+def test_peak_calling_matches_reference(torch_cuda, golden):
+    import pytme_b200 as P
+    from pytme_b200.analyzer import PeakCallerMaximumFilter
+
+    g = golden("c1_flcsm.npz")
+    pc = PeakCallerMaximumFilter(shape=g["scores32"].shape, num_peaks=int(g["peak_num"]),
+                                 min_distance=int(g["peak_min_distance"]))
+    state = pc.init_state()
+    state = pc(state, scores=torch_cuda.as_tensor(g["scores32"], device="cuda"),
+               rotation_matrix=np.eye(3, dtype=np.float32))
+    assert np.array_equal(state[0], g["peak_pos"])
+    assert np.array_equal(state[2], g["peak_scores"])
+
+
+def test_greedy_filter_matches_reference(torch_cuda, golden):
+    from pytme_b200.peaks import find_candidate_indices
+
+    g = golden("candidates.npz")
+    for i in range(4):
+        idx = find_candidate_indices(g[f"coords{i}"], int(g[f"md{i}"]))
+        assert np.array_equal(idx, g[f"idx{i}"])
+    # beyond the shared-memory capacity the workspace path is used
+    rng = np.random.default_rng(11)
+    c = rng.integers(0, 400, size=(5000, 3)).astype(np.int64)
+    assert np.array_equal(find_candidate_indices(c, 9), O.find_candidate_indices(c, 9))

@@ -1,0 +1,95 @@
+"""Host-side logic of the package (no GPU): shapes, padding, rotation matrices,
+splits, analyzer merges, synthetic inputs."""
+import numpy as np
+import pytest
+
+from oracle import tm_oracle as O
+from pytme_b200 import matching as M
+from pytme_b200 import synthetic as syn
+
+
+@pytest.mark.parametrize("n", [1, 7, 11, 13, 17, 23, 48, 49, 97, 121, 143, 200, 1000, 2187])
+def test_next_fast_len_matches_oracle(n):
+    assert M.next_fast_len(n) == O.next_fast_len(n)
+
+
+@pytest.mark.parametrize("tshape,mshape,pad", [
+    ((64, 64, 64), (16, 16, 16), False), ((80, 80, 80), (41, 41, 35), False),
+    ((80, 80, 80), (41, 41, 35), True), ((512, 512, 200), (48, 48, 48), False),
+    ((10, 12, 14), (17, 5, 3), False)])
+def test_fourier_padding(tshape, mshape, pad):
+    with np.errstate(all="ignore"):
+        import warnings
+
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            assert M.fourier_padding(tshape, mshape, pad) == O.fourier_padding(tshape, mshape, pad)
+
+
+def test_rigid_transform_matrices_match_reference_construction():
+    rng = np.random.default_rng(7)
+    rots = np.concatenate([syn.random_rotation_matrices(200, rng),
+                           syn.super_fibonacci_rotations(100),
+                           np.eye(3, dtype=np.float32)[None]])
+    for shape in ((16, 16, 16), (48, 48, 48), (41, 41, 35)):
+        c = np.divide(np.asarray(shape) - 1, 2)
+        got = M.rigid_transform_matrices(rots, c)
+        for i in range(rots.shape[0]):
+            ref = O.rigid_transform_matrix(rots[i], c)
+            # float32 construction; identical up to the last bit of the offset column
+            assert np.array_equal(got[i, :3, :3], ref[:3, :3])
+            np.testing.assert_allclose(got[i, :3, 3], ref[:3, 3], rtol=0, atol=4e-6)
+
+
+def test_split_shape():
+    s = M.split_shape((80, 80, 80), {0: 2})
+    assert len(s) == 2
+    assert s[0][0] == slice(0, 40) and s[1][0] == slice(40, 80)
+    assert M.split_shape((81, 10, 10), {0: 2})[1][0] == slice(40, 81)
+
+
+def test_subset_reflect_padding_uses_neighbours():
+    t = np.arange(10 * 4 * 4, dtype=np.float32).reshape(10, 4, 4)
+    md = M.MatchingData(t, np.ones((3, 3, 3), np.float32))
+    sub, off = md.subset_by_slice(target_slice=(slice(5, 10), slice(0, 4), slice(0, 4)),
+                                  target_pad=(2, 2, 2))
+    assert off == (5, 0, 0)
+    # left pad of 1 on axis 0 comes from the real neighbour row 4
+    assert np.array_equal(sub.target[0, 1:5, 1:5], t[4])
+
+
+def test_apply_convolution_mode():
+    a = np.arange(20 * 20 * 20).reshape(20, 20, 20)
+    assert M.apply_convolution_mode(a, "same", (16, 16, 16), (5, 5, 5)).shape == (16, 16, 16)
+    assert M.apply_convolution_mode(a, "valid", (16, 16, 16), (5, 5, 5),
+                                    convolution_shape=(20, 20, 20)).shape == (12, 12, 12)
+
+
+def test_max_score_merge_follows_reference():
+    from pytme_b200.analyzer import MaxScoreOverRotations
+
+    r = np.eye(3, dtype=np.float32)
+    r2 = np.array([[0, -1, 0], [1, 0, 0], [0, 0, 1]], np.float32)
+    s1 = np.zeros((4, 4, 4), np.float32)
+    s1[1, 1, 1] = 0.5
+    s2 = np.zeros((4, 4, 4), np.float32)
+    s2[1, 1, 1] = 0.7
+    a = (s1, np.array([0, 0, 0]), np.where(s1 > 0, 0, -1).astype(np.int32), {0: r})
+    b = (s2, np.array([2, 0, 0]), np.where(s2 > 0, 0, -1).astype(np.int32), {0: r2})
+    out = MaxScoreOverRotations.merge([a, b])
+    assert out[0].shape == (6, 4, 4)
+    assert out[0][1, 1, 1] == np.float32(0.5) and out[0][3, 1, 1] == np.float32(0.7)
+    assert out[2][3, 1, 1] == 1 and np.array_equal(out[3][1], r2)
+
+
+def test_synthetic_generators():
+    rng = np.random.default_rng(0)
+    t = syn.blob_template(16, rng)
+    assert t.shape == (16, 16, 16) and t.dtype == np.float32 and t.max() > 0.5
+    m = syn.spherical_mask((16, 16, 16), 8, center=(7.5, 7.5, 7.5))
+    assert m.sum() > 0 and set(np.unique(m)) <= {0.0, 1.0}
+    R = syn.super_fibonacci_rotations(1000)
+    np.testing.assert_allclose(R @ R.transpose(0, 2, 1), np.broadcast_to(np.eye(3), R.shape),
+                               atol=1e-6)
+    assert syn.rotation_count_for_angle(7) == 27672
+    assert syn.rotation_count_for_angle(30) == 360
