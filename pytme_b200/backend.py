@@ -159,6 +159,18 @@ class B200Backend:
     def free_cache(self):
         torch.cuda.empty_cache()
 
+    def get_fundamental_dtype(self, arr):
+        dt = arr.dtype if hasattr(arr, "dtype") else np.asarray(arr).dtype
+        if isinstance(dt, torch.dtype):
+            if dt.is_complex:
+                return complex
+            return float if dt.is_floating_point else int
+        if np.issubdtype(dt, np.integer):
+            return int
+        if np.issubdtype(dt, np.complexfloating):
+            return complex
+        return float
+
     # ------------------------------------------------------------ creation
     def zeros(self, shape, dtype=None):
         return torch.zeros(shape, dtype=_tdtype(dtype), device=self.device)

@@ -44,6 +44,29 @@ def _scan(score, target, template, mask, rotations, precision="fp32", plain=Fals
                           pad_target_edges=pad, target_splits=splits or {})
 
 
+def _assert_argmax_ties(g, rot, score="FLCSphericalMask"):
+    """Every voxel whose rotation index differs from the reference's is a documented
+    tie: the oracle's score for the GPU's rotation there is within 2*TOL of the
+    reference's best score (or, where the reference kept no rotation, the GPU's pick
+    scores at most 2*TOL above the zero threshold)."""
+    ref_rot = g["rot32"].astype(np.int32)
+    mism = np.argwhere(rot != ref_rot)
+    if len(mism) == 0:
+        return
+    picks = rot[tuple(mism.T)]
+    best = g["scores32"][tuple(mism.T)]
+    for j in np.unique(picks):
+        sel = picks == j
+        if j < 0:
+            assert np.all(best[sel] <= 2 * TOL)
+            continue
+        r = O.scan(g["target"], g["template"], g["rotations"][j:j + 1], score,
+                   template_mask=g["mask"], score_threshold=-np.inf)
+        sj = r["scores"][tuple(mism[sel].T)]
+        gap = best[sel] - sj
+        assert np.all(gap <= 2 * TOL), (int(j), float(gap.max()))
+
+
 @pytest.mark.parametrize("precision,plain", [("fp32", True), ("fp32", False), ("mixed", False)])
 def test_flcsm_config1_matches_reference(torch_cuda, golden, precision, plain):
     g = golden("c1_flcsm.npz")
@@ -55,11 +78,7 @@ def test_flcsm_config1_matches_reference(torch_cuda, golden, precision, plain):
     err64 = np.abs(s - g["scores64"]).max()
     assert err32 <= TOL, err32
     assert err64 <= TOL, err64
-    # a different argmax is only possible where two rotations score within 2*TOL of
-    # each other (both maps agree within TOL), i.e. at near-ties; there must be few
-    mism = rot != g["rot32"].astype(np.int32)
-    total = int(np.count_nonzero(mism))
-    assert total <= max(5, int(1e-4 * s.size)), total
+    _assert_argmax_ties(g, rot)
     # rotation mapping covers every rotation in order
     assert len(r[3]) == g["rotations"].shape[0]
     assert np.array_equal(r[3][5], g["rotations"][5])
