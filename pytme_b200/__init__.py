@@ -19,6 +19,7 @@ from ._native import lib as _lib  # noqa: F401  (fails loudly without the CUDA l
 from .backend import B200Backend, backend
 from .matching import MatchingData, fourier_padding, rigid_transform_matrices, scan, scan_subsets
 from .scores import MATCHING_EXHAUSTIVE_REGISTER, ScanPlan, register_matching_exhaustive
+from . import filters  # noqa: F401
 from .analyzer import (MaxScoreOverRotations, PeakCaller, PeakCallerMaximumFilter,
                        PeakCallerSort, SharedAnalyzerProxy)
 

@@ -38,7 +38,8 @@ EXPORTED = (
     "tm_scan_create", "tm_scan_destroy", "tm_scan_device_bytes", "tm_scan_set_template",
     "tm_scan_set_target", "tm_scan_run", "tm_scan_set_timing", "tm_scan_get_timing",
     "tm_scan_stage_bytes", "tm_max_filter_peaks",
-    "tm_find_candidate_indices_workspace", "tm_find_candidate_indices", "tm_line_fft_test",
+    "tm_find_candidate_indices_workspace", "tm_find_candidate_indices",
+    "tm_line_fft_test",
 )
 
 

@@ -1,0 +1,228 @@
+// Column FFTs of length N (a power of two, 64..1024) for the fused scan passes.
+//
+// A CTA transforms W columns (lines) of a tile at once; each line is handled by
+// T = N/8 threads that hold 8 complex values each, so a thread's data stay in
+// registers between stages and shared memory is only used to exchange them.
+//
+// The forward transform is an in-place decimation-in-frequency FFT with radix-8
+// stages (a final radix-4 or radix-2 stage when N is not a power of 8). Stage s
+// works on sub-problems of size L_s (L_0 = N, L_{s+1} = L_s / R_s): butterfly
+// (p, q) reads positions p*L + q + (L/R)*r, computes the R-point DFT, multiplies
+// output j by W_L^(j*q) and writes it back to position p*L + q + (L/R)*j. The same
+// thread reads and writes the same positions, so a stage needs no barrier between
+// its loads and stores. After the last stage position `pos` holds frequency
+// digitrev(pos) (the mixed-radix digits of pos in reverse order).
+//
+// The adjoint stages (conjugate twiddles applied before an inverse R-point DFT, in
+// reverse stage order) undo this: starting from digit-reversed data they return
+// natural order, i.e. an unnormalised inverse DFT. The fused x pass runs
+//   stage 0 (loads from global) ... last stage | product | adjoint last ... adjoint 0
+// with the product and both last stages in registers; the y pass runs the forward
+// stage structure with conjugate twiddles (an inverse DFT with digit-reversed
+// output) and stores rows at digitrev(pos).
+//
+// Shared-memory layout of a tile: element (line l, position pos) sits at
+// pos*W + l + W*(pos >> 3). With W lines spanning a warp this keeps every stage's
+// warp-wide access to the minimum number of wavefronts.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "fft_smem.cuh"
+
+namespace tmb {
+namespace colfft {
+
+using fft::cadd;
+using fft::cconj;
+using fft::cmul;
+using fft::csub;
+
+constexpr int num_stages(int n) {
+  int k = 0;
+  while (n >= 8) { n /= 8; ++k; }
+  return k + (n > 1 ? 1 : 0);
+}
+constexpr int stage_size(int n, int s) {
+  for (int i = 0; i < s; ++i) n /= 8;
+  return n;
+}
+constexpr int stage_radix(int n, int s) {
+  int l = stage_size(n, s);
+  return l >= 8 ? 8 : l;
+}
+
+// frequency index held at position pos after the forward stages
+template <int N>
+__device__ __forceinline__ int digitrev(int pos) {
+  constexpr int S = num_stages(N);
+  int k = 0, mul = 1;
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int R = stage_radix(N, s);
+    const int stride = stage_size(N, s) / R;  // N / (R_0 ... R_s)
+    const int digit = (pos / stride) % R;
+    k += digit * mul;
+    mul *= R;
+  }
+  return k;
+}
+
+template <int W>
+__device__ __forceinline__ int saddr(int l, int pos) {
+  return pos * W + l + W * (pos >> 3);
+}
+
+template <int N>
+constexpr int smem_elems(int W) {
+  return (N + N / 8) * W;
+}
+
+template <int R, int DIR>
+__device__ __forceinline__ void dftR(float2* v) {
+  if constexpr (R == 8) fft::dft8<DIR>(v);
+  else if constexpr (R == 4) fft::dft4<DIR>(v);
+  else fft::dft2<DIR>(v);
+}
+
+// One forward-structured DIF stage s (DIR -1: forward DFT, +1: inverse DFT with
+// conjugate twiddles) on values already in registers; twiddles applied after the
+// butterflies. v holds the thread's 8 values in the order (butterfly i, r).
+template <int N, int S, int DIR>
+__device__ __forceinline__ void dif_stage_regs(float2 (&v)[8], int t, const float2* tw) {
+  constexpr int L = stage_size(N, S);
+  constexpr int R = stage_radix(N, S);
+  constexpr int NB = 8 / R;
+  constexpr int LR = L / R;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    dftR<R, DIR>(&v[i * R]);
+    if constexpr (LR > 1) {
+      const int b = t * NB + i;
+      const int q = b % LR;
+#pragma unroll
+      for (int j = 1; j < R; ++j) {
+        float2 w = tw[j * q * (N / L)];
+        if (DIR > 0) w = cconj(w);
+        v[i * R + j] = cmul(v[i * R + j], w);
+      }
+    }
+  }
+}
+
+// Adjoint of a DIF stage: conjugate twiddles first, then the inverse DFT.
+template <int N, int S>
+__device__ __forceinline__ void dif_stage_adjoint_regs(float2 (&v)[8], int t, const float2* tw) {
+  constexpr int L = stage_size(N, S);
+  constexpr int R = stage_radix(N, S);
+  constexpr int NB = 8 / R;
+  constexpr int LR = L / R;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    if constexpr (LR > 1) {
+      const int b = t * NB + i;
+      const int q = b % LR;
+#pragma unroll
+      for (int j = 1; j < R; ++j) v[i * R + j] = cmul(v[i * R + j], cconj(tw[j * q * (N / L)]));
+    }
+    dftR<R, 1>(&v[i * R]);
+  }
+}
+
+// position of value (i, r) of thread t at stage S
+template <int N, int S>
+__device__ __forceinline__ int stage_pos(int t, int i, int r) {
+  constexpr int L = stage_size(N, S);
+  constexpr int R = stage_radix(N, S);
+  constexpr int NB = 8 / R;
+  constexpr int LR = L / R;
+  const int b = t * NB + i;
+  const int p = b / LR, q = b % LR;
+  return p * L + q + LR * r;
+}
+
+template <int N, int W, int S>
+__device__ __forceinline__ void load_stage(float2 (&v)[8], const float2* sm, int l, int t) {
+  constexpr int R = stage_radix(N, S);
+  constexpr int NB = 8 / R;
+#pragma unroll
+  for (int i = 0; i < NB; ++i)
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[i * R + r] = sm[saddr<W>(l, stage_pos<N, S>(t, i, r))];
+}
+
+template <int N, int W, int S>
+__device__ __forceinline__ void store_stage(const float2 (&v)[8], float2* sm, int l, int t) {
+  constexpr int R = stage_radix(N, S);
+  constexpr int NB = 8 / R;
+#pragma unroll
+  for (int i = 0; i < NB; ++i)
+#pragma unroll
+    for (int r = 0; r < R; ++r) sm[saddr<W>(l, stage_pos<N, S>(t, i, r))] = v[i * R + r];
+}
+
+// Forward (DIR=-1) or inverse (DIR=+1) DIF transform of the thread's line: v holds
+// the natural-order inputs x[t + T*r] on entry and the outputs at the last stage's
+// positions on exit (frequency/position digitrev(stage_pos<N, last>(t, i, r))).
+// Stage 0 runs on v directly; later stages exchange through shared memory.
+template <int N, int W, int DIR>
+__device__ __forceinline__ void dif_forward(float2 (&v)[8], float2* sm, const float2* tw, int l,
+                                            int t) {
+  constexpr int NS = num_stages(N);
+  dif_stage_regs<N, 0, DIR>(v, t, tw);
+  // stage 0 outputs j sit at positions t + T*j, i.e. stage_pos<N,0>(t, 0, j)
+  store_stage<N, W, 0>(v, sm, l, t);
+  __syncthreads();
+  if constexpr (NS > 1) {
+    load_stage<N, W, 1>(v, sm, l, t);
+    dif_stage_regs<N, 1, DIR>(v, t, tw);
+  }
+  if constexpr (NS > 2) {
+    store_stage<N, W, 1>(v, sm, l, t);
+    __syncthreads();
+    load_stage<N, W, 2>(v, sm, l, t);
+    dif_stage_regs<N, 2, DIR>(v, t, tw);
+  }
+  if constexpr (NS > 3) {
+    store_stage<N, W, 2>(v, sm, l, t);
+    __syncthreads();
+    load_stage<N, W, 3>(v, sm, l, t);
+    dif_stage_regs<N, 3, DIR>(v, t, tw);
+  }
+}
+
+// Adjoint of dif_forward<.., -1>: from the last stage's positions back to natural
+// order x[t + T*r] (unnormalised inverse DFT). Ends with v in natural order.
+template <int N, int W>
+__device__ __forceinline__ void dif_adjoint(float2 (&v)[8], float2* sm, const float2* tw, int l,
+                                            int t) {
+  constexpr int NS = num_stages(N);
+  if constexpr (NS > 3) {
+    dif_stage_adjoint_regs<N, 3>(v, t, tw);
+    store_stage<N, W, 3>(v, sm, l, t);
+    __syncthreads();
+    load_stage<N, W, 2>(v, sm, l, t);
+  }
+  if constexpr (NS > 2) {
+    dif_stage_adjoint_regs<N, 2>(v, t, tw);
+    store_stage<N, W, 2>(v, sm, l, t);
+    __syncthreads();
+    load_stage<N, W, 1>(v, sm, l, t);
+  }
+  if constexpr (NS > 1) {
+    dif_stage_adjoint_regs<N, 1>(v, t, tw);
+    store_stage<N, W, 1>(v, sm, l, t);
+    __syncthreads();
+    load_stage<N, W, 0>(v, sm, l, t);
+  }
+  dif_stage_adjoint_regs<N, 0>(v, t, tw);
+}
+
+template <int N>
+__device__ __forceinline__ int last_pos(int t, int i, int r) {
+  return stage_pos<N, num_stages(N) - 1>(t, i, r);
+}
+
+}  // namespace colfft
+}  // namespace tmb

@@ -199,6 +199,50 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int n, int Ns, int nl
   __syncthreads();
 }
 
+// Stockham pass with compile-time length, radix and span.
+template <int N, int R, int Ns, int DIR, int MAXE, bool LINES_FAST>
+__device__ __forceinline__ void stockham_pass_ct(float2* buf, int nlines, int ls, int es,
+                                                 const float2* tw, int tws, int table_n, int tid,
+                                                 int nthr) {
+  constexpr int MAXB = (MAXE + R - 1) / R;
+  constexpr int nb = N / R;
+  constexpr int tstep = N / (Ns * R);
+  const int total = nb * nlines;
+  float2 v[MAXB][R];
+#pragma unroll
+  for (int c = 0; c < MAXB; ++c) {
+    int w = tid + c * nthr;
+    if (w < total) {
+      int l, j;
+      if (LINES_FAST) { l = w % nlines; j = w / nlines; } else { j = w % nb; l = w / nb; }
+      const float2* base = buf + l * ls;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[c][r] = base[(j + r * nb) * es];
+      if constexpr (Ns > 1) {
+        const int k = j % Ns;
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[c][r] = cmul(v[c][r], twiddle<DIR>(tw, r * k * tstep * tws));
+      }
+      dft<R, DIR>(v[c], tw, table_n);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < MAXB; ++c) {
+    int w = tid + c * nthr;
+    if (w < total) {
+      int l, j;
+      if (LINES_FAST) { l = w % nlines; j = w / nlines; } else { j = w % nb; l = w / nb; }
+      float2* base = buf + l * ls;
+      const int k = j % Ns;
+      const int o = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) base[(o + r * Ns) * es] = v[c][r];
+    }
+  }
+  __syncthreads();
+}
+
 // Full transform of all lines: runs the plan's passes. Callers must
 // __syncthreads() before (data loaded) — the routine ends synchronised.
 // Radices 2, 3, 4, 5 and 8 are compiled in (every 5-smooth length); plans with
@@ -220,6 +264,59 @@ __device__ __forceinline__ void fft_lines(float2* buf, const LinePlan& p, int nl
     }
     Ns *= R;
   }
+}
+
+// ---- compile-time length: the radix list and every stride constant-fold.
+constexpr int ct_npass(int n) {
+  int m = n, e2 = 0, k = 0;
+  while (m % 2 == 0) { m /= 2; ++e2; }
+  int eights = e2 / 3, rem = e2 % 3;
+  if (rem == 1 && eights > 0) { eights -= 1; k += 2; }
+  else if (rem == 1) k += 1;
+  else if (rem == 2) k += 1;
+  k += eights;
+  while (m % 3 == 0) { m /= 3; ++k; }
+  while (m % 5 == 0) { m /= 5; ++k; }
+  return m == 1 ? k : -1;
+}
+
+constexpr int ct_radix(int n, int idx) {
+  int m = n, e2 = 0, k = 0;
+  int r[kMaxPasses] = {};
+  while (m % 2 == 0) { m /= 2; ++e2; }
+  int eights = e2 / 3, rem = e2 % 3;
+  if (rem == 1 && eights > 0) { eights -= 1; r[k++] = 4; r[k++] = 4; }
+  else if (rem == 1) r[k++] = 2;
+  else if (rem == 2) r[k++] = 4;
+  for (int i = 0; i < eights; ++i) r[k++] = 8;
+  while (m % 3 == 0) { m /= 3; r[k++] = 3; }
+  while (m % 5 == 0) { m /= 5; r[k++] = 5; }
+  return r[idx];
+}
+
+constexpr int ct_ns(int n, int idx) {
+  int ns = 1;
+  for (int i = 0; i < idx; ++i) ns *= ct_radix(n, i);
+  return ns;
+}
+
+template <int N, int P, int DIR, int MAXE, bool LINES_FAST>
+__device__ __forceinline__ void ct_passes(float2* buf, int nlines, int ls, int es, const float2* tw,
+                                          int table_n, int tid, int nthr) {
+  if constexpr (P < ct_npass(N)) {
+    constexpr int R = ct_radix(N, P);
+    constexpr int Ns = ct_ns(N, P);
+    stockham_pass_ct<N, R, Ns, DIR, MAXE, LINES_FAST>(buf, nlines, ls, es, tw, table_n / N,
+                                                     table_n, tid, nthr);
+    ct_passes<N, P + 1, DIR, MAXE, LINES_FAST>(buf, nlines, ls, es, tw, table_n, tid, nthr);
+  }
+}
+
+template <int N, int DIR, int MAXE, bool LINES_FAST>
+__device__ __forceinline__ void fft_lines_ct(float2* buf, int nlines, int ls, int es,
+                                             const float2* tw, int table_n, int tid, int nthr) {
+  static_assert(ct_npass(N) > 0, "length must be 5-smooth");
+  ct_passes<N, 0, DIR, MAXE, LINES_FAST>(buf, nlines, ls, es, tw, table_n, tid, nthr);
 }
 
 inline bool supported_radices(const LinePlan& p) {

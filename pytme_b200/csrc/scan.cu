@@ -27,6 +27,7 @@
 // Target-side quantities (target spectra and the FLCSphericalMask denominator)
 // are computed once by set_target; the denominator and the target mean are
 // evaluated in double precision.
+#include "colfft.cuh"
 #include "common.cuh"
 #include "fft_smem.cuh"
 #include "ops.cuh"
@@ -37,6 +38,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 namespace tmb {
@@ -224,6 +226,299 @@ ypass_kernel(HT* __restrict__ H, int n0, int n1, int h2, int W, LinePlan p1,
   }
 }
 
+// ------------------------------------------------------------------ register-resident passes
+// Power-of-two axis lengths use the column codelet of colfft.cuh: T = N/8 threads
+// per column, W columns per CTA (thread id = t*W + l, so a warp spans W columns and
+// each global row segment of W elements is one contiguous access).
+
+// Stage 0 of the forward DIF when only rows [0, nz) of the column are non-zero and
+// nz <= T: the radix-8 DFT of a single non-zero input is that input, so output j is
+// x[t] * W_N^(j*t).
+template <int N>
+__device__ __forceinline__ void stage0_single(float2 (&v)[8], int t, const float2* tw) {
+  const float2 x = v[0];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) v[j] = j == 0 ? x : fft::cmul(x, tw[j * t]);
+}
+
+template <int N, int W, int DIR>
+__device__ __forceinline__ void dif_rest(float2 (&v)[8], float2* sm, const float2* tw, int l,
+                                         int t) {
+  constexpr int NS = colfft::num_stages(N);
+  colfft::store_stage<N, W, 0>(v, sm, l, t);
+  __syncthreads();
+  if constexpr (NS > 1) {
+    colfft::load_stage<N, W, 1>(v, sm, l, t);
+    colfft::dif_stage_regs<N, 1, DIR>(v, t, tw);
+  }
+  if constexpr (NS > 2) {
+    colfft::store_stage<N, W, 1>(v, sm, l, t);
+    __syncthreads();
+    colfft::load_stage<N, W, 2>(v, sm, l, t);
+    colfft::dif_stage_regs<N, 2, DIR>(v, t, tw);
+  }
+  if constexpr (NS > 3) {
+    colfft::store_stage<N, W, 2>(v, sm, l, t);
+    __syncthreads();
+    colfft::load_stage<N, W, 3>(v, sm, l, t);
+    colfft::dif_stage_regs<N, 3, DIR>(v, t, tw);
+  }
+}
+
+// K1': template rows -> G. grid (ceil(h2/W), t0, B); N = n1.
+template <int N, int W>
+__global__ void __launch_bounds__(N / 8 * W, 1)
+tmpl_zy_reg_kernel(const float* __restrict__ tmpl, int t0, int t1, int t2, int n2, int h2,
+                   const float2* __restrict__ tw1_g, const float2* __restrict__ tw2_g,
+                   float2* __restrict__ G) {
+  constexpr int T = N / 8;
+  constexpr int NT = T * W;
+  extern __shared__ float4 smem_raw[];
+  float2* tw1 = reinterpret_cast<float2*>(smem_raw);
+  float2* sm = tw1 + N;
+  float2* tw2 = sm + colfft::smem_elems<N>(W);
+  float* plane = reinterpret_cast<float*>(tw2 + n2);
+  const int tid = threadIdx.x, l = tid % W, t = tid / W;
+  const int k2 = blockIdx.x * W + l;
+  const int x = blockIdx.y, b = blockIdx.z;
+  for (int i = tid; i < N; i += NT) tw1[i] = tw1_g[i];
+  for (int i = tid; i < n2; i += NT) tw2[i] = tw2_g[i];
+  const float* src = tmpl + ((int64_t)b * t0 + x) * t1 * t2;
+  for (int i = tid; i < t1 * t2; i += NT) plane[i] = src[i];
+  __syncthreads();
+  float2 v[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int y = t + T * r;
+    float2 acc = make_float2(0.f, 0.f);
+    if (y < t1 && k2 < h2) {
+      const float* row = plane + y * t2;
+      int idx = 0;
+      for (int z = 0; z < t2; ++z) {
+        const float a = row[z];
+        const float2 w = tw2[idx];
+        acc.x += a * w.x;
+        acc.y += a * w.y;
+        idx += k2;
+        if (idx >= n2) idx -= n2;
+      }
+    }
+    v[r] = acc;
+  }
+  if (t1 <= T) stage0_single<N>(v, t, tw1);
+  else colfft::dif_stage_regs<N, 0, -1>(v, t, tw1);
+  dif_rest<N, W, -1>(v, sm, tw1, l, t);
+  if (k2 < h2) {
+    float2* dst = G + ((int64_t)b * t0 + x) * N * h2;
+    constexpr int R = colfft::stage_radix(N, colfft::num_stages(N) - 1);
+#pragma unroll
+    for (int i = 0; i < 8 / R; ++i)
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int k1 = colfft::digitrev<N>(colfft::last_pos<N>(t, i, r));
+        dst[(int64_t)k1 * h2 + k2] = v[i * R + r];
+      }
+  }
+}
+
+// K2': x pass. grid (ceil(h2/W), n1); N = n0; loops over the rotations of the group.
+template <int N, int W, typename HT>
+__global__ void __launch_bounds__(N / 8 * W, 1)
+xpass_reg_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, int B, int t0,
+                 int n1, int h2, const float2* __restrict__ tw0_g, float scale,
+                 HT* __restrict__ H) {
+  constexpr int T = N / 8;
+  constexpr int NT = T * W;
+  constexpr int R = colfft::stage_radix(N, colfft::num_stages(N) - 1);
+  extern __shared__ float4 smem_raw[];
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  float2* sm = tw + N;
+  const int tid = threadIdx.x, l = tid % W, t = tid / W;
+  const int k2 = blockIdx.x * W + l;
+  const int k1 = blockIdx.y;
+  const bool valid = k2 < h2;
+  for (int i = tid; i < N; i += NT) tw[i] = tw0_g[i];
+  // the target-spectrum values this thread multiplies, for every rotation
+  float2 f[8];
+#pragma unroll
+  for (int i = 0; i < 8 / R; ++i)
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int k0 = colfft::digitrev<N>(colfft::last_pos<N>(t, i, r));
+      float2 v = valid ? __ldg(Ft + ((int64_t)k0 * n1 + k1) * h2 + k2) : make_float2(0.f, 0.f);
+      f[i * R + r] = make_float2(v.x * scale, v.y * scale);
+    }
+  __syncthreads();
+  const int64_t S = (int64_t)N * n1 * h2;
+  const int64_t row = (int64_t)n1 * h2;
+  const int64_t col = (int64_t)k1 * h2 + k2;
+  for (int b = 0; b < B; ++b) {
+    const float2* g = G + (int64_t)b * t0 * row + col;
+    float2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int x = t + T * r;
+      v[r] = (valid && x < t0) ? g[(int64_t)x * row] : make_float2(0.f, 0.f);
+    }
+    if (t0 <= T) stage0_single<N>(v, t, tw);
+    else colfft::dif_stage_regs<N, 0, -1>(v, t, tw);
+    dif_rest<N, W, -1>(v, sm, tw, l, t);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) v[e] = fft::cmul(v[e], f[e]);
+    colfft::dif_adjoint<N, W>(v, sm, tw, l, t);
+    if (valid) {
+      HT* h = H + (int64_t)b * S + col;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) Store<HT>::store(h + (int64_t)(t + T * r) * row, v[r]);
+    }
+  }
+}
+
+// K3': y pass (inverse FFT along axis 1, in place). grid (ceil(h2/W), n0, B); N = n1.
+template <int N, int W, typename HT>
+__global__ void __launch_bounds__(N / 8 * W, 1)
+ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ tw1_g) {
+  constexpr int T = N / 8;
+  constexpr int NT = T * W;
+  constexpr int R = colfft::stage_radix(N, colfft::num_stages(N) - 1);
+  extern __shared__ float4 smem_raw[];
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  float2* sm = tw + N;
+  const int tid = threadIdx.x, l = tid % W, t = tid / W;
+  const int k2 = blockIdx.x * W + l;
+  const int x = blockIdx.y, b = blockIdx.z;
+  const bool valid = k2 < h2;
+  for (int i = tid; i < N; i += NT) tw[i] = tw1_g[i];
+  __syncthreads();
+  HT* h = H + ((int64_t)b * n0 + x) * N * h2 + k2;
+  float2 v[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+    v[r] = valid ? Store<HT>::load(h + (int64_t)(t + T * r) * h2) : make_float2(0.f, 0.f);
+  colfft::dif_stage_regs<N, 0, 1>(v, t, tw);
+  dif_rest<N, W, 1>(v, sm, tw, l, t);
+  if (valid) {
+#pragma unroll
+    for (int i = 0; i < 8 / R; ++i)
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int y = colfft::digitrev<N>(colfft::last_pos<N>(t, i, r));
+        Store<HT>::store(h + (int64_t)y * h2, v[i * R + r]);
+      }
+  }
+}
+
+// K2'' (FLC): x pass with three outputs per rotation. The rotated mask's spectrum is
+// transformed once and multiplied by the spectra of f and f^2 (the local mean and
+// mean square under the mask, CC(f, m) and CC(f^2, m)); the normalised template's
+// spectrum is multiplied by the spectrum of f (the numerator). The two statistics
+// outputs are always complex64.
+template <int N, int W, typename HT>
+__global__ void __launch_bounds__(N / 8 * W, 1)
+xpass_flc_reg_kernel(const float2* __restrict__ Gt, const float2* __restrict__ Gm,
+                     const float2* __restrict__ Ft, const float2* __restrict__ Ft2, int B, int t0,
+                     int n1, int h2, const float2* __restrict__ tw0_g, float scale,
+                     HT* __restrict__ Ht, float2* __restrict__ Hm, float2* __restrict__ Hm2) {
+  constexpr int T = N / 8;
+  constexpr int NT = T * W;
+  constexpr int R = colfft::stage_radix(N, colfft::num_stages(N) - 1);
+  extern __shared__ float4 smem_raw[];
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  float2* sm = tw + N;
+  const int tid = threadIdx.x, l = tid % W, t = tid / W;
+  const int k2 = blockIdx.x * W + l;
+  const int k1 = blockIdx.y;
+  const bool valid = k2 < h2;
+  for (int i = tid; i < N; i += NT) tw[i] = tw0_g[i];
+  int64_t foff[8];
+#pragma unroll
+  for (int i = 0; i < 8 / R; ++i)
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int k0 = colfft::digitrev<N>(colfft::last_pos<N>(t, i, r));
+      foff[i * R + r] = ((int64_t)k0 * n1 + k1) * h2 + k2;
+    }
+  __syncthreads();
+  const int64_t S = (int64_t)N * n1 * h2;
+  const int64_t row = (int64_t)n1 * h2;
+  const int64_t col = (int64_t)k1 * h2 + k2;
+  for (int b = 0; b < B; ++b) {
+    // mask spectrum along axis 0
+    float2 vm[8], v[8];
+    const float2* gm = Gm + (int64_t)b * t0 * row + col;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int x = t + T * r;
+      vm[r] = (valid && x < t0) ? gm[(int64_t)x * row] : make_float2(0.f, 0.f);
+    }
+    if (t0 <= T) stage0_single<N>(vm, t, tw);
+    else colfft::dif_stage_regs<N, 0, -1>(vm, t, tw);
+    dif_rest<N, W, -1>(vm, sm, tw, l, t);
+    // CC(f, m)
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      float2 f = valid ? __ldg(Ft + foff[e]) : make_float2(0.f, 0.f);
+      v[e] = fft::cmul(vm[e], make_float2(f.x * scale, f.y * scale));
+    }
+    colfft::dif_adjoint<N, W>(v, sm, tw, l, t);
+    if (valid) {
+      float2* h = Hm + (int64_t)b * S + col;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) h[(int64_t)(t + T * r) * row] = v[r];
+    }
+    __syncthreads();
+    // CC(f^2, m)
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      float2 f = valid ? __ldg(Ft2 + foff[e]) : make_float2(0.f, 0.f);
+      v[e] = fft::cmul(vm[e], make_float2(f.x * scale, f.y * scale));
+    }
+    colfft::dif_adjoint<N, W>(v, sm, tw, l, t);
+    if (valid) {
+      float2* h = Hm2 + (int64_t)b * S + col;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) h[(int64_t)(t + T * r) * row] = v[r];
+    }
+    __syncthreads();
+    // numerator CC(f, t)
+    const float2* gt = Gt + (int64_t)b * t0 * row + col;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int x = t + T * r;
+      v[r] = (valid && x < t0) ? gt[(int64_t)x * row] : make_float2(0.f, 0.f);
+    }
+    if (t0 <= T) stage0_single<N>(v, t, tw);
+    else colfft::dif_stage_regs<N, 0, -1>(v, t, tw);
+    dif_rest<N, W, -1>(v, sm, tw, l, t);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      float2 f = valid ? __ldg(Ft + foff[e]) : make_float2(0.f, 0.f);
+      v[e] = fft::cmul(v[e], make_float2(f.x * scale, f.y * scale));
+    }
+    colfft::dif_adjoint<N, W>(v, sm, tw, l, t);
+    if (valid) {
+      HT* h = Ht + (int64_t)b * S + col;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) Store<HT>::store(h + (int64_t)(t + T * r) * row, v[r]);
+    }
+    __syncthreads();
+  }
+}
+
+template <int N>
+constexpr int reg_lines() { return N >= 512 ? 8 : 16; }
+
+template <int N>
+size_t reg_smem_bytes(int n2, int t1, int t2, bool with_plane) {
+  size_t b = sizeof(float2) * (N + colfft::smem_elems<N>(reg_lines<N>()));
+  if (with_plane) b += sizeof(float2) * n2 + sizeof(float) * t1 * t2;
+  return b;
+}
+
+static bool reg_supported(int n) {
+  return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024;
+}
+
 // ------------------------------------------------------------------ K4: z pass + epilogue
 // grid (ceil(n0*n1/R)); each CTA owns R consecutive (x', y') rows = R*n2 output voxels.
 // c2r of length n2 (even) via a complex inverse FFT of length m = n2/2:
@@ -232,7 +527,7 @@ ypass_kernel(HT* __restrict__ H, int n0, int n1, int h2, int W, LinePlan p1,
 // with the imaginary parts of X[0] and X[m] dropped, as numpy/pocketfft's c2r does.
 constexpr int kMaxV = 8;   // output voxels per thread
 
-template <typename HT>
+template <typename HT, int M = 0>
 __global__ void __launch_bounds__(kThreads, 1)
 zpass_kernel(const HT* __restrict__ H, int B, int64_t rows, int n2, int h2, int R, LinePlan pm,
              const float2* __restrict__ tw2_g, float scale, const float* __restrict__ inv_den,
@@ -273,7 +568,10 @@ zpass_kernel(const HT* __restrict__ H, int B, int64_t rows, int n2, int h2, int 
       buf[e] = make_float2(E.x - O.y, E.y + O.x);
     }
     __syncthreads();
-    fft::fft_lines<1, kMaxE, false>(buf, pm, nrows, m, 1, tw2, n2, tid, kThreads);
+    if constexpr (M > 0)
+      fft::fft_lines_ct<M, 1, kMaxE, false>(buf, nrows, M, 1, tw2, 2 * M, tid, kThreads);
+    else
+      fft::fft_lines<1, kMaxE, false>(buf, pm, nrows, m, 1, tw2, n2, tid, kThreads);
     const float* outv = reinterpret_cast<const float*>(buf);
 #pragma unroll
     for (int c = 0; c < kMaxV; ++c) {
@@ -297,6 +595,109 @@ zpass_kernel(const HT* __restrict__ H, int B, int64_t rows, int n2, int h2, int 
         state_max[g] = best[c];
         state_rot[g] = arg[c];
       }
+    }
+  }
+}
+
+// K4'' (FLC): c2r of the numerator and both statistics rows, then
+// norm_scores (tme/backends/npfftw_backend.py:537-587) in double precision with the
+// rotation's own n_obs = sum(rotated mask), and the strict-> update.
+template <int M>
+__device__ __forceinline__ void c2r_rows(float2* raw, float2* buf, const float2* tw2, int nrows,
+                                         int n2, int h2, const LinePlan& pm, int tid) {
+  const int m = n2 / 2;
+  for (int e = tid; e < nrows * m; e += kThreads) {
+    int r = e / m, k = e % m;
+    const float2* xr = raw + (int64_t)r * h2;
+    float2 a = xr[k], c = xr[m - k];
+    if (k == 0) { a.y = 0.f; c.y = 0.f; }
+    float2 cc = fft::cconj(c);
+    float2 E = fft::cadd(a, cc);
+    float2 O = fft::cmul(fft::csub(a, cc), fft::cconj(tw2[k]));
+    buf[e] = make_float2(E.x - O.y, E.y + O.x);
+  }
+  __syncthreads();
+  if constexpr (M > 0)
+    fft::fft_lines_ct<M, 1, kMaxE, false>(buf, nrows, M, 1, tw2, 2 * M, tid, kThreads);
+  else
+    fft::fft_lines<1, kMaxE, false>(buf, pm, nrows, m, 1, tw2, n2, tid, kThreads);
+}
+
+template <typename HT, int M = 0>
+__global__ void __launch_bounds__(kThreads, 1)
+zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
+                 const float2* __restrict__ Hm2, int B, int64_t rows, int n2, int h2, int R,
+                 LinePlan pm, const float2* __restrict__ tw2_g, float scale_t, float scale_m,
+                 const double* __restrict__ stats, double eps, int32_t first_index,
+                 float* __restrict__ state_max, int32_t* __restrict__ state_rot, int64_t S) {
+  extern __shared__ float4 smem_raw[];
+  const int m = n2 / 2;
+  float2* tw2 = reinterpret_cast<float2*>(smem_raw);
+  float2* raw = tw2 + n2;
+  float2* buf = raw + (int64_t)R * h2;
+  const int tid = threadIdx.x;
+  const int64_t row0 = (int64_t)blockIdx.x * R;
+  const int nrows = (int)min((int64_t)R, rows - row0);
+  for (int i = tid; i < n2; i += kThreads) tw2[i] = tw2_g[i];
+  const int nout = nrows * n2;
+  const int64_t vox0 = row0 * n2;
+  float best[kMaxV];
+  int32_t arg[kMaxV];
+  double e1[kMaxV];
+#pragma unroll
+  for (int c = 0; c < kMaxV; ++c) { best[c] = -INFINITY; arg[c] = -1; }
+  const float* outv = reinterpret_cast<const float*>(buf);
+  for (int b = 0; b < B; ++b) {
+    const double nobs = stats[b * 4 + 2];
+    // local mean
+    const float2* src = Hm + (int64_t)b * S + row0 * h2;
+    for (int e = tid; e < nrows * h2; e += kThreads) raw[e] = src[e];
+    __syncthreads();
+    c2r_rows<M>(raw, buf, tw2, nrows, n2, h2, pm, tid);
+#pragma unroll
+    for (int c = 0; c < kMaxV; ++c) {
+      int v = tid + c * kThreads;
+      e1[c] = v < nout ? (double)outv[v] * (double)scale_m / nobs : 0.0;
+    }
+    __syncthreads();
+    // local mean square -> variance
+    src = Hm2 + (int64_t)b * S + row0 * h2;
+    for (int e = tid; e < nrows * h2; e += kThreads) raw[e] = src[e];
+    __syncthreads();
+    c2r_rows<M>(raw, buf, tw2, nrows, n2, h2, pm, tid);
+#pragma unroll
+    for (int c = 0; c < kMaxV; ++c) {
+      int v = tid + c * kThreads;
+      if (v < nout) {
+        double e2 = (double)outv[v] * (double)scale_m / nobs;
+        double var = e2 - e1[c] * e1[c];
+        double sd = sqrt(var > 0 ? var : 0.0);
+        if (sd < eps) sd = 1.0;
+        e1[c] = sd * nobs;  // reuse as the denominator
+      }
+    }
+    __syncthreads();
+    // numerator
+    const HT* st = Ht + (int64_t)b * S + row0 * h2;
+    for (int e = tid; e < nrows * h2; e += kThreads) raw[e] = Store<HT>::load(st + e);
+    __syncthreads();
+    c2r_rows<M>(raw, buf, tw2, nrows, n2, h2, pm, tid);
+#pragma unroll
+    for (int c = 0; c < kMaxV; ++c) {
+      int v = tid + c * kThreads;
+      if (v < nout) {
+        float sc = (float)((double)outv[v] * (double)scale_t / e1[c]);
+        if (sc > best[c]) { best[c] = sc; arg[c] = first_index + b; }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int c = 0; c < kMaxV; ++c) {
+    int v = tid + c * kThreads;
+    if (v < nout && arg[c] >= 0) {
+      int64_t g = vox0 + v;
+      if (best[c] > state_max[g]) { state_max[g] = best[c]; state_rot[g] = arg[c]; }
     }
   }
 }
@@ -422,10 +823,14 @@ struct Scan {
   float2* spec_m = nullptr;
   float2* G = nullptr;
   void* H = nullptr;
+  float2* Gm = nullptr;   // FLC: rotated-mask rows
+  float2* Hm = nullptr;   // FLC: CC(f, m) spectra (complex64)
+  float2* Hm2 = nullptr;  // FLC: CC(f^2, m) spectra (complex64)
   float2* tw0 = nullptr;
   float2* tw1 = nullptr;
   float2* tw2 = nullptr;
   LinePlan p0{}, p1{}, pm{};
+  bool reg0 = false, reg1 = false;  // register-resident column kernels for n0 / n1
   int W1 = 1, W2 = 1, W3 = 1, R4 = 1;
   size_t smem1 = 0, smem2 = 0, smem3 = 0, smem4 = 0;
   cufftHandle fwd = 0, inv = 0, tfwd = 0, tinv = 0;
@@ -454,6 +859,165 @@ struct StageTimer {
     s->stage_launches[stage] += 1;
   }
 };
+
+// ---- z pass dispatch: compile-time half-lengths for the common sizes
+#define TM_DISPATCH_M(m, CALL)                                   \
+  switch (m) {                                                   \
+    case 32: { constexpr int MM = 32; CALL; } break;             \
+    case 50: { constexpr int MM = 50; CALL; } break;             \
+    case 64: { constexpr int MM = 64; CALL; } break;             \
+    case 80: { constexpr int MM = 80; CALL; } break;             \
+    case 100: { constexpr int MM = 100; CALL; } break;           \
+    case 128: { constexpr int MM = 128; CALL; } break;           \
+    case 160: { constexpr int MM = 160; CALL; } break;           \
+    default: { constexpr int MM = 0; CALL; } break;              \
+  }
+
+template <typename HT>
+static void launch_zpass_flc(Scan* s, dim3 g4, HT* H, int nb, int64_t rows, float out_scale,
+                             int32_t first, float* state_max, int32_t* state_rot,
+                             cudaStream_t st) {
+  const double* stats = s->stats_ws + (int64_t)nb * kStatChunks * 3;
+  TM_DISPATCH_M(s->n2 / 2, (zpass_flc_kernel<HT, MM><<<g4, kThreads, s->smem4, st>>>(
+                               H, s->Hm, s->Hm2, nb, rows, s->n2, s->h2, s->R4, s->pm, s->tw2,
+                               out_scale, out_scale, stats, 1.1920928955078125e-07, first,
+                               state_max, state_rot, s->S)));
+}
+
+static void set_zpass_attrs(int m, int smem) {
+  TM_DISPATCH_M(m, (cudaFuncSetAttribute(zpass_flc_kernel<float2, MM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                    cudaFuncSetAttribute(zpass_flc_kernel<__half2, MM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem)));
+  TM_DISPATCH_M(m, (cudaFuncSetAttribute(zpass_kernel<float2, MM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                    cudaFuncSetAttribute(zpass_kernel<__half2, MM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem)));
+}
+
+template <typename HT>
+static void launch_zpass(Scan* s, dim3 g4, HT* H, int nb, int64_t rows, float out_scale,
+                         int32_t first, float* state_max, int32_t* state_rot, cudaStream_t st) {
+  TM_DISPATCH_M(s->n2 / 2, (zpass_kernel<HT, MM><<<g4, kThreads, s->smem4, st>>>(
+                               H, nb, rows, s->n2, s->h2, s->R4, s->pm, s->tw2, out_scale,
+                               s->inv_den, first, state_max, state_rot, s->S)));
+}
+
+// ---- launch helpers for the register-resident kernels
+template <int N>
+static void set_reg_attrs(size_t zy_smem) {
+  constexpr int W = reg_lines<N>();
+  const int sm = (int)reg_smem_bytes<N>(0, 0, 0, false);
+  cudaFuncSetAttribute(xpass_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(xpass_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(ypass_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(ypass_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(tmpl_zy_reg_kernel<N, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zy_smem);
+  cudaFuncSetAttribute(xpass_flc_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(xpass_flc_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+static void set_reg_attrs_n(int n, size_t zy_smem) {
+  switch (n) {
+    case 64: set_reg_attrs<64>(zy_smem); break;
+    case 128: set_reg_attrs<128>(zy_smem); break;
+    case 256: set_reg_attrs<256>(zy_smem); break;
+    case 512: set_reg_attrs<512>(zy_smem); break;
+    case 1024: set_reg_attrs<1024>(zy_smem); break;
+    default: break;
+  }
+}
+
+template <int N>
+static void launch_tmpl_reg(Scan* s, int nb, cudaStream_t st, const float* in = nullptr,
+                            float2* out = nullptr) {
+  constexpr int W = reg_lines<N>();
+  dim3 g(ceil_div(s->h2, W), s->t0, nb);
+  size_t smem = reg_smem_bytes<N>(s->n2, s->t1, s->t2, true);
+  tmpl_zy_reg_kernel<N, W><<<g, N / 8 * W, smem, st>>>(in ? in : s->rot_t, s->t0, s->t1, s->t2,
+                                                       s->n2, s->h2, s->tw1, s->tw2,
+                                                       out ? out : s->G);
+}
+
+template <int N, typename HT>
+static void launch_xpass_flc_reg(Scan* s, int nb, float hs, HT* H, cudaStream_t st) {
+  constexpr int W = reg_lines<N>();
+  dim3 g(ceil_div(s->h2, W), s->n1);
+  xpass_flc_reg_kernel<N, W, HT><<<g, N / 8 * W, reg_smem_bytes<N>(0, 0, 0, false), st>>>(
+      s->G, s->Gm, s->ft_target, s->ft_target2, nb, s->t0, s->n1, s->h2, s->tw0, hs, H, s->Hm,
+      s->Hm2);
+}
+
+template <int N, typename HT>
+static void launch_xpass_reg(Scan* s, int nb, float hs, HT* H, cudaStream_t st) {
+  constexpr int W = reg_lines<N>();
+  dim3 g(ceil_div(s->h2, W), s->n1);
+  xpass_reg_kernel<N, W, HT><<<g, N / 8 * W, reg_smem_bytes<N>(0, 0, 0, false), st>>>(
+      s->G, s->ft_target, nb, s->t0, s->n1, s->h2, s->tw0, hs, H);
+}
+
+template <int N, typename HT>
+static void launch_ypass_reg(Scan* s, int nb, HT* H, cudaStream_t st) {
+  constexpr int W = reg_lines<N>();
+  dim3 g(ceil_div(s->h2, W), s->n0, nb);
+  ypass_reg_kernel<N, W, HT><<<g, N / 8 * W, reg_smem_bytes<N>(0, 0, 0, false), st>>>(
+      H, s->n0, s->h2, s->tw1);
+}
+
+#define TM_DISPATCH_N(n, CALL)      \
+  switch (n) {                      \
+    case 64: { constexpr int NN = 64; CALL; } break;    \
+    case 128: { constexpr int NN = 128; CALL; } break;  \
+    case 256: { constexpr int NN = 256; CALL; } break;  \
+    case 512: { constexpr int NN = 512; CALL; } break;  \
+    case 1024: { constexpr int NN = 1024; CALL; } break; \
+    default: break;                 \
+  }
+
+template <typename HT>
+static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr,
+                               cudaStream_t stream) {
+  const bool flc = s->d.score == TM_SCORE_FLC;
+  tmr.begin();
+  if (s->reg1) {
+    TM_DISPATCH_N(s->n1, (launch_tmpl_reg<NN>(s, nb, stream)));
+    if (flc) TM_DISPATCH_N(s->n1, (launch_tmpl_reg<NN>(s, nb, stream, s->rot_m, s->Gm)));
+  } else {
+    dim3 g1(ceil_div(s->h2, s->W1), s->t0, nb);
+    tmpl_zy_kernel<<<g1, kThreads, s->smem1, stream>>>(s->rot_t, s->t0, s->t1, s->t2, s->n1,
+                                                       s->n2, s->h2, s->W1, s->p1, s->tw1,
+                                                       s->tw2, s->G);
+  }
+  TM_TRY(check_launch("template pass"));
+  tmr.end(TM_STAGE_TEMPLATE);
+  tmr.begin();
+  if (flc) {
+    TM_DISPATCH_N(s->n0, (launch_xpass_flc_reg<NN, HT>(s, nb, hs, H, stream)));
+  } else if (s->reg0) {
+    TM_DISPATCH_N(s->n0, (launch_xpass_reg<NN, HT>(s, nb, hs, H, stream)));
+  } else {
+    dim3 g2(ceil_div(s->h2, s->W2), s->n1);
+    xpass_kernel<HT><<<g2, kThreads, s->smem2, stream>>>(s->G, s->ft_target, nb, s->t0, s->n0,
+                                                        s->n1, s->h2, s->W2, s->p0, s->tw0, hs, H);
+  }
+  TM_TRY(check_launch("x pass"));
+  tmr.end(TM_STAGE_XPASS);
+  tmr.begin();
+  if (s->reg1) {
+    TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, HT>(s, nb, H, stream)));
+    if (flc) {
+      TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, float2>(s, nb, s->Hm, stream)));
+      TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, float2>(s, nb, s->Hm2, stream)));
+    }
+  } else {
+    dim3 g3(ceil_div(s->h2, s->W3), s->n0, nb);
+    ypass_kernel<HT><<<g3, kThreads, s->smem3, stream>>>(H, s->n0, s->n1, s->h2, s->W3, s->p1,
+                                                        s->tw1);
+  }
+  TM_TRY(check_launch("y pass"));
+  tmr.end(TM_STAGE_YPASS);
+  return TM_OK;
+}
 
 static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -504,7 +1068,8 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
   if (s->fused) {
     bool ok = line_supported(s->n0) && line_supported(s->n1) && (s->n2 % 2 == 0) &&
               line_supported(s->n2 / 2) && s->n0 <= kTile && s->n1 <= kTile &&
-              s->n2 <= kThreads * kMaxV && d.score != TM_SCORE_FLC;
+              s->n2 <= kThreads * kMaxV &&
+              (d.score != TM_SCORE_FLC || (reg_supported(s->n0) && reg_supported(s->n1)));
     if (!ok) {
       set_error("scan_create: fused path does not support shape (%d,%d,%d) / score %d",
                 s->n0, s->n1, s->n2, d.score);
@@ -531,7 +1096,7 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
   size_t o_st = take(stats_workspace_bytes(B));
   size_t o_ts = take(sizeof(float2) * s->TS * B);
   size_t o_arr = 0, o_arrm = 0, o_ccm = 0, o_ccm2 = 0, o_spec = 0, o_specm = 0, o_G = 0, o_H = 0;
-  size_t o_tw0 = 0, o_tw1 = 0, o_tw2 = 0;
+  size_t o_tw0 = 0, o_tw1 = 0, o_tw2 = 0, o_Gm = 0, o_Hm = 0, o_Hm2 = 0;
   if (!s->fused) {
     o_arr = take(sizeof(float) * s->N);
     o_spec = take(sizeof(float2) * s->S);
@@ -544,6 +1109,11 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
   } else {
     o_G = take(sizeof(float2) * (size_t)B * s->t0 * s->n1 * s->h2);
     o_H = take((s->half ? sizeof(__half2) : sizeof(float2)) * (size_t)B * s->S);
+    if (d.score == TM_SCORE_FLC) {
+      o_Gm = take(sizeof(float2) * (size_t)B * s->t0 * s->n1 * s->h2);
+      o_Hm = take(sizeof(float2) * (size_t)B * s->S);
+      o_Hm2 = take(sizeof(float2) * (size_t)B * s->S);
+    }
     o_tw0 = take(sizeof(float2) * s->n0);
     o_tw1 = take(sizeof(float2) * s->n1);
     o_tw2 = take(sizeof(float2) * s->n2);
@@ -579,6 +1149,11 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
   } else {
     s->G = reinterpret_cast<float2*>(b8 + o_G);
     s->H = b8 + o_H;
+    if (d.score == TM_SCORE_FLC) {
+      s->Gm = reinterpret_cast<float2*>(b8 + o_Gm);
+      s->Hm = reinterpret_cast<float2*>(b8 + o_Hm);
+      s->Hm2 = reinterpret_cast<float2*>(b8 + o_Hm2);
+    }
     s->tw0 = reinterpret_cast<float2*>(b8 + o_tw0);
     s->tw1 = reinterpret_cast<float2*>(b8 + o_tw1);
     s->tw2 = reinterpret_cast<float2*>(b8 + o_tw2);
@@ -609,8 +1184,16 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     cudaFuncSetAttribute(xpass_kernel<__half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem2);
     cudaFuncSetAttribute(ypass_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem3);
     cudaFuncSetAttribute(ypass_kernel<__half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem3);
-    cudaFuncSetAttribute(zpass_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem4);
-    cudaFuncSetAttribute(zpass_kernel<__half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem4);
+    set_zpass_attrs(s->n2 / 2, (int)s->smem4);
+    s->reg0 = reg_supported(s->n0) && !getenv("PYTME_B200_GENERIC_FFT");
+    s->reg1 = reg_supported(s->n1) && !getenv("PYTME_B200_GENERIC_FFT");
+    size_t zy = 0;
+    if (s->reg1) {
+      TM_DISPATCH_N(s->n1, (zy = reg_smem_bytes<NN>(s->n2, s->t1, s->t2, true)));
+      if (zy > 200 * 1024) s->reg1 = false;
+    }
+    if (s->reg0) set_reg_attrs_n(s->n0, 0);
+    if (s->reg1) set_reg_attrs_n(s->n1, zy);
   }
   // ---- cuFFT plans: fast-shape r2c/c2r (setup and plain path), template-shape (filter)
   int r;
@@ -823,43 +1406,26 @@ static int run_fused(Scan* s, int n, int32_t first_index, float* state_max, int3
     tmr.begin();
     TM_TRY(prepare_templates(s, nb, stream));
     tmr.end(TM_STAGE_PREPARE);
-    dim3 g1(ceil_div(s->h2, s->W1), s->t0, nb);
-    tmr.begin();
-    tmpl_zy_kernel<<<g1, kThreads, s->smem1, stream>>>(s->rot_t, s->t0, s->t1, s->t2, s->n1,
-                                                       s->n2, s->h2, s->W1, s->p1, s->tw1,
-                                                       s->tw2, s->G);
-    TM_TRY(check_launch("tmpl_zy_kernel"));
-    tmr.end(TM_STAGE_TEMPLATE);
-    dim3 g2(ceil_div(s->h2, s->W2), s->n1);
-    dim3 g3(ceil_div(s->h2, s->W3), s->n0, nb);
     const int64_t rows = (int64_t)s->n0 * s->n1;
     dim3 g4(ceil_div(rows, s->R4));
     if (s->half) {
       __half2* H = static_cast<__half2*>(s->H);
+      TM_TRY(launch_template_x_y<__half2>(s, nb, (float)hs, H, tmr, stream));
       tmr.begin();
-      xpass_kernel<__half2><<<g2, kThreads, s->smem2, stream>>>(s->G, s->ft_target, nb, s->t0, s->n0, s->n1, s->h2, s->W2, s->p0, s->tw0, (float)hs, H);
-      TM_TRY(check_launch("xpass_kernel"));
-      tmr.end(TM_STAGE_XPASS);
-      tmr.begin();
-      ypass_kernel<__half2><<<g3, kThreads, s->smem3, stream>>>(H, s->n0, s->n1, s->h2, s->W3, s->p1, s->tw1);
-      TM_TRY(check_launch("ypass_kernel"));
-      tmr.end(TM_STAGE_YPASS);
-      tmr.begin();
-      zpass_kernel<__half2><<<g4, kThreads, s->smem4, stream>>>(H, nb, rows, s->n2, s->h2, s->R4, s->pm, s->tw2, out_scale, s->inv_den, first_index + g0, state_max, state_rot, s->S);
+      if (s->d.score == TM_SCORE_FLC)
+        launch_zpass_flc<__half2>(s, g4, H, nb, rows, out_scale, first_index + g0, state_max, state_rot, stream);
+      else
+        launch_zpass<__half2>(s, g4, H, nb, rows, out_scale, first_index + g0, state_max, state_rot, stream);
       TM_TRY(check_launch("zpass_kernel"));
       tmr.end(TM_STAGE_ZPASS);
     } else {
       float2* H = static_cast<float2*>(s->H);
+      TM_TRY(launch_template_x_y<float2>(s, nb, (float)hs, H, tmr, stream));
       tmr.begin();
-      xpass_kernel<float2><<<g2, kThreads, s->smem2, stream>>>(s->G, s->ft_target, nb, s->t0, s->n0, s->n1, s->h2, s->W2, s->p0, s->tw0, (float)hs, H);
-      TM_TRY(check_launch("xpass_kernel"));
-      tmr.end(TM_STAGE_XPASS);
-      tmr.begin();
-      ypass_kernel<float2><<<g3, kThreads, s->smem3, stream>>>(H, s->n0, s->n1, s->h2, s->W3, s->p1, s->tw1);
-      TM_TRY(check_launch("ypass_kernel"));
-      tmr.end(TM_STAGE_YPASS);
-      tmr.begin();
-      zpass_kernel<float2><<<g4, kThreads, s->smem4, stream>>>(H, nb, rows, s->n2, s->h2, s->R4, s->pm, s->tw2, out_scale, s->inv_den, first_index + g0, state_max, state_rot, s->S);
+      if (s->d.score == TM_SCORE_FLC)
+        launch_zpass_flc<float2>(s, g4, H, nb, rows, out_scale, first_index + g0, state_max, state_rot, stream);
+      else
+        launch_zpass<float2>(s, g4, H, nb, rows, out_scale, first_index + g0, state_max, state_rot, stream);
       TM_TRY(check_launch("zpass_kernel"));
       tmr.end(TM_STAGE_ZPASS);
     }
@@ -886,15 +1452,18 @@ int scan_get_timing(const Scan* s, double* ms, int64_t* launches) {
 
 int64_t scan_stage_bytes(const Scan* s, int stage, int nb) {
   // Algorithmic HBM bytes of one launch of a stage for a group of nb rotations:
-  // every array the stage must read or write once, at its storage width.
+  // every array the stage must read or write once, at its storage width. FLC
+  // carries two extra complex64 statistics spectra per rotation.
   const int64_t e = s->half ? 4 : 8;
+  const bool flc = s->d.score == TM_SCORE_FLC;
   const int64_t G = (int64_t)nb * s->t0 * s->n1 * s->h2 * 8;
+  const int64_t H = (int64_t)nb * s->S * e;
+  const int64_t Hs = flc ? 2 * (int64_t)nb * s->S * 8 : 0;
   switch (stage) {
-    case TM_STAGE_TEMPLATE: return (int64_t)nb * s->T * 4 + G;
-    case TM_STAGE_XPASS: return G + s->S * 8 + (int64_t)nb * s->S * e;
-    case TM_STAGE_YPASS: return 2 * (int64_t)nb * s->S * e;
-    case TM_STAGE_ZPASS:
-      return (int64_t)nb * s->S * e + s->N * (s->inv_den ? 4 : 0) + s->N * 16;
+    case TM_STAGE_TEMPLATE: return (flc ? 2 : 1) * ((int64_t)nb * s->T * 4 + G);
+    case TM_STAGE_XPASS: return (flc ? 2 : 1) * (G + s->S * 8) + H + Hs;
+    case TM_STAGE_YPASS: return 2 * (H + Hs);
+    case TM_STAGE_ZPASS: return H + Hs + s->N * (s->inv_den ? 4 : 0) + s->N * 16;
     default: return 0;
   }
 }

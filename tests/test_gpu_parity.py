@@ -229,3 +229,71 @@ def test_greedy_filter_matches_reference(torch_cuda, golden):
     rng = np.random.default_rng(11)
     c = rng.integers(0, 400, size=(5000, 3)).astype(np.int64)
     assert np.array_equal(find_candidate_indices(c, 9), O.find_candidate_indices(c, 9))
+
+
+def _filters_ctf_wedge(shape_t, shape_target):
+    from pytme_b200.filters import Compose, CTFReconstructed, WedgeReconstructed
+
+    wedge = WedgeReconstructed(angles=(60, 60), opening_axis=2, tilt_axis=0)
+    wedge_t = WedgeReconstructed(angles=(60, 60), opening_axis=2, tilt_axis=0)
+    ctf = CTFReconstructed(defocus_x=30000, amplitude_contrast=0.07, spherical_aberration=2.7e7,
+                           acceleration_voltage=300e3, sampling_rate=6.8)
+    tf = Compose([wedge, ctf])(shape=shape_t, return_real_fourier=True)["data"]
+    gf = Compose([wedge_t])(shape=shape_target, return_real_fourier=True)["data"]
+    return tf, gf
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_flc_fused_matches_oracle(torch_cuda, precision):
+    """Fused FLC (rotated mask, CTF x wedge template filter, wedge target filter) on
+    power-of-two x/y lengths against the oracle in FP32 and FP64."""
+    from pytme_b200 import synthetic as syn
+
+    rng = np.random.default_rng(21)
+    tmpl = syn.blob_template(12, rng, radius=3.5, sigma=1.2)
+    mask = syn.dilated_threshold_mask(tmpl, 0.1, 1)
+    target, _, _ = syn.make_tomogram((64, 64, 48), tmpl, 4, rng, snr=0.5, mask=mask)
+    rots = syn.random_rotation_matrices(20, rng)
+    tf, gf = _filters_ctf_wedge(tmpl.shape, target.shape)
+    r = _scan("FLC", target, tmpl, mask, rots, precision=precision, batch=8,
+              template_filter=tf, target_filter=gf)
+    ref = O.scan(target, tmpl, rots, "FLC", template_mask=mask, template_filter=tf,
+                 target_filter=gf)
+    ref64 = O.scan(target, tmpl, rots, "FLC", template_mask=mask, template_filter=tf,
+                   target_filter=gf, dtype=np.float64)
+    assert np.abs(r[0] - ref["scores"]).max() <= TOL
+    assert np.abs(r[0] - ref64["scores"]).max() <= TOL
+    assert np.count_nonzero(r[2] != ref64["rotations"]) <= int(2e-3 * r[2].size)
+
+
+def test_flc_config2_shape(torch_cuda):
+    """Config-2 geometry (256x256x128 target, 32^3 template, FLC with CTF x wedge) on a
+    few rotations: fused mixed precision within 1e-4 of the FP32 oracle."""
+    from pytme_b200 import synthetic as syn
+
+    rng = np.random.default_rng(22)
+    tmpl = syn.blob_template(32, rng, sigma=3.0, radius=10.0)
+    mask = syn.dilated_threshold_mask(tmpl, 0.1, 2)
+    target, _, _ = syn.make_tomogram((256, 256, 128), tmpl, 40, rng, snr=0.1, mask=mask)
+    rots = syn.random_rotation_matrices(3, rng)
+    tf, gf = _filters_ctf_wedge(tmpl.shape, target.shape)
+    r = _scan("FLC", target, tmpl, mask, rots, precision="mixed", batch=4,
+              template_filter=tf, target_filter=gf)
+    ref = O.scan(target, tmpl, rots, "FLC", template_mask=mask, template_filter=tf,
+                 target_filter=gf)
+    assert np.abs(r[0] - ref["scores"]).max() <= TOL
+
+
+def test_flcsm_config3_shape(torch_cuda):
+    """The headline geometry (512x512x200 target, 48^3 template, spherical mask) on two
+    rotations: fused mixed precision within 1e-4 of the FP32 oracle."""
+    from pytme_b200 import synthetic as syn
+
+    rng = np.random.default_rng(23)
+    tmpl = syn.blob_template(48, rng, sigma=4.5, radius=15.0)
+    mask = syn.spherical_mask((48,) * 3, 24, center=(23.5,) * 3)
+    target = rng.normal(size=(512, 512, 200)).astype(np.float32)
+    rots = syn.random_rotation_matrices(2, rng)
+    r = _scan("FLCSphericalMask", target, tmpl, mask, rots, precision="mixed", batch=2)
+    ref = O.scan(target, tmpl, rots, "FLCSphericalMask", template_mask=mask)
+    assert np.abs(r[0] - ref["scores"]).max() <= TOL
