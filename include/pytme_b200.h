@@ -179,6 +179,24 @@ int tm_find_candidate_indices(const int64_t* coords, int n, int64_t min_distance
                               int32_t* out_idx, int32_t* out_count, void* workspace,
                               void* stream);
 
+/* Allocation-free greedy minimum-distance filter. No counterpart in the
+ * reference: it is tm_find_candidate_indices for callers that cannot allocate
+ * device memory while they run (for example, hosts that own all device memory
+ * through their own pool, or that have a fixed memory budget agreed up front).
+ * Instead of a caller workspace it uses a fixed scratch array in the library's
+ * static device memory, 3 * TM_NOALLOC_MAX_POINTS int64 (1.5 MiB), which every
+ * GPU that loads the library holds until the process exits. It allocates nothing:
+ * no cudaMalloc, cudaFree or allocating library call. n above
+ * TM_NOALLOC_MAX_POINTS returns TM_E_INVALID. The first call on each device looks
+ * up the scratch address (cudaGetSymbolAddress) with that device current; make
+ * that first call before any stream capture. All calls share the one scratch
+ * array, so calls that overlap on the GPU (different streams, or different host
+ * threads on one device) race and must be serialised by the caller. Results are
+ * identical to tm_find_candidate_indices. */
+#define TM_NOALLOC_MAX_POINTS 65536
+int tm_find_candidate_indices_noalloc(const int64_t* coords, int n, int64_t min_distance,
+                                      int32_t* out_idx, int32_t* out_count, void* stream);
+
 /* Diagnostic: `lines` complex FFTs of length n (dir -1 forward, +1 unnormalised
  * inverse) with the shared-memory line-FFT routine of the fused scan.
  * Synchronises. */

@@ -39,7 +39,7 @@ EXPORTED = (
     "tm_scan_set_target", "tm_scan_run", "tm_scan_set_timing", "tm_scan_get_timing",
     "tm_scan_stage_bytes", "tm_max_filter_peaks",
     "tm_find_candidate_indices_workspace", "tm_find_candidate_indices",
-    "tm_line_fft_test",
+    "tm_find_candidate_indices_noalloc", "tm_line_fft_test",
 )
 
 
@@ -91,6 +91,7 @@ def _load():
         "tm_max_filter_peaks": (c_int, [f32p, c_int, c_int, c_int, c_int, f32p, f32p, vp, vp]),
         "tm_find_candidate_indices_workspace": (c_int64, [c_int]),
         "tm_find_candidate_indices": (c_int, [vp, c_int, c_int64, i32p, i32p, vp, vp]),
+        "tm_find_candidate_indices_noalloc": (c_int, [vp, c_int, c_int64, i32p, i32p, vp]),
         "tm_line_fft_test": (c_int, [vp, vp, c_int, c_int, c_int, vp]),
     }
     for name, (res, args) in sig.items():
