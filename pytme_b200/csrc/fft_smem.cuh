@@ -319,6 +319,93 @@ __device__ __forceinline__ void fft_lines_ct(float2* buf, int nlines, int ls, in
   ct_passes<N, 0, DIR, MAXE, LINES_FAST>(buf, nlines, ls, es, tw, table_n, tid, nthr);
 }
 
+// ---- small DFTs of compile-time size in registers (DIR -1 forward, +1 inverse)
+// 16 = 4 x 4 Cooley-Tukey with its constant twiddles; 6, 10, 12, 15, 20 = Good-Thomas
+// prime-factor forms (coprime factors, no twiddles).
+template <int DIR>
+__device__ __forceinline__ void dft16(float2* v) {
+  const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;
+  const float h = 0.70710678118654752440f;
+  const float sg = DIR < 0 ? -1.f : 1.f;
+  // w16^j for j = 0..9 (exp(DIR * 2 pi i j / 16))
+  const float2 w[10] = {make_float2(1.f, 0.f), make_float2(c1, sg * s1), make_float2(h, sg * h),
+                        make_float2(s1, sg * c1), make_float2(0.f, sg * 1.f),
+                        make_float2(-s1, sg * c1), make_float2(-h, sg * h),
+                        make_float2(-c1, sg * s1), make_float2(-1.f, 0.f),
+                        make_float2(-c1, -sg * s1)};
+  float2 a[4][4];
+#pragma unroll
+  for (int n1 = 0; n1 < 4; ++n1) {
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) a[n1][n2] = v[4 * n2 + n1];
+    dft4<DIR>(a[n1]);
+#pragma unroll
+    for (int k2 = 1; k2 < 4; ++k2) {
+      const int e = n1 * k2;
+      if (e) a[n1][k2] = cmul(a[n1][k2], w[e]);
+    }
+  }
+#pragma unroll
+  for (int k2 = 0; k2 < 4; ++k2) {
+    float2 b[4] = {a[0][k2], a[1][k2], a[2][k2], a[3][k2]};
+    dft4<DIR>(b);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) v[k2 + 4 * k1] = b[k1];
+  }
+}
+
+constexpr int modinv(int a, int m) {
+  for (int x = 1; x < m; ++x)
+    if ((a * x) % m == 1) return x;
+  return 1;
+}
+
+template <int R, int DIR>
+__device__ __forceinline__ void dft_prime_or_pow2(float2* v) {
+  if constexpr (R == 2) dft2<DIR>(v);
+  else if constexpr (R == 3) dft3<DIR>(v);
+  else if constexpr (R == 4) dft4<DIR>(v);
+  else if constexpr (R == 5) dft5<DIR>(v);
+  else if constexpr (R == 8) dft8<DIR>(v);
+  else dft16<DIR>(v);
+}
+
+template <int N1, int N2, int DIR>
+__device__ __forceinline__ void dft_pfa(float2* v) {
+  constexpr int N = N1 * N2;
+  constexpr int K1 = N2 * modinv(N2 % N1, N1);
+  constexpr int K2 = N1 * modinv(N1 % N2, N2);
+  float2 a[N2][N1];
+#pragma unroll
+  for (int n2 = 0; n2 < N2; ++n2) {
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) a[n2][n1] = v[(N2 * n1 + N1 * n2) % N];
+    dft_prime_or_pow2<N1, DIR>(a[n2]);
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < N1; ++k1) {
+    float2 b[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) b[n2] = a[n2][k1];
+    dft_prime_or_pow2<N2, DIR>(b);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) v[(K1 * k1 + K2 * k2) % N] = b[k2];
+  }
+}
+
+template <int N, int DIR>
+__device__ __forceinline__ void dft_small(float2* v) {
+  if constexpr (N == 1) {
+  } else if constexpr (N == 2 || N == 3 || N == 4 || N == 5 || N == 8 || N == 16) {
+    dft_prime_or_pow2<N, DIR>(v);
+  } else if constexpr (N == 6) dft_pfa<2, 3, DIR>(v);
+  else if constexpr (N == 10) dft_pfa<2, 5, DIR>(v);
+  else if constexpr (N == 12) dft_pfa<4, 3, DIR>(v);
+  else if constexpr (N == 15) dft_pfa<3, 5, DIR>(v);
+  else if constexpr (N == 20) dft_pfa<4, 5, DIR>(v);
+  else static_assert(N == 0, "unsupported small DFT size");
+}
+
 inline bool supported_radices(const LinePlan& p) {
   if (p.npass <= 0) return false;
   for (int i = 0; i < p.npass; ++i) {

@@ -702,6 +702,107 @@ zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
   }
 }
 
+// K4' (four-step): c2r along axis 2 for m = n2/2 = M1*M2 (M2 a multiple of M1).
+// Thread (row, j) of a row's M1 threads builds Z[k] = E + iO for k = j + M1*k2 straight
+// from global memory (the half-length c2r pre-twiddle), runs an inverse DFT of size M2
+// over k2 in registers, applies exp(+2 pi i n2 j / m), exchanges through padded shared
+// memory, and runs C = M2/M1 inverse DFTs of size M1, ending with the outputs
+// z[n2 + M2*n1] = x[2(n2 + M2 n1)] + i x[2(n2 + M2 n1) + 1]. Each thread keeps the
+// running max/argmax of its 2*M2 voxels in registers; the voxel pairs of a row's
+// threads are contiguous, so the state merge is coalesced.
+template <typename HT, int M1, int M2>
+__global__ void __launch_bounds__(M1 * (256 / M1), 2)
+zpass4_kernel(const HT* __restrict__ H, int B, int64_t rows, int h2,
+              const float2* __restrict__ tw2_g, float scale, const float* __restrict__ inv_den,
+              int32_t first_index, float* __restrict__ state_max,
+              int32_t* __restrict__ state_rot, int64_t S) {
+  constexpr int M = M1 * M2;
+  constexpr int N2 = 2 * M;
+  constexpr int C = M2 / M1;
+  constexpr int RW = 256 / M1;
+  constexpr int NT = M1 * RW;
+  constexpr int PITCH = M2 * (M1 + 1);
+  constexpr int V = 2 * M2;  // voxels per thread
+  extern __shared__ float4 smem_raw[];
+  float2* tw = reinterpret_cast<float2*>(smem_raw);
+  float2* sx = tw + N2;
+  const int tid = threadIdx.x;
+  const int rho = tid / M1, j = tid % M1;
+  for (int i = tid; i < N2; i += NT) tw[i] = tw2_g[i];
+  const int64_t row = (int64_t)blockIdx.x * RW + rho;
+  const bool active = rho < RW && row < rows;
+  float best[V];
+  int32_t arg[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) { best[v] = -INFINITY; arg[v] = -1; }
+  // voxel of output slot (c, n1, part): 2*(n2 + M2*n1) + part with n2 = j + M1*c
+  const int64_t vrow = row * N2;
+  float2* srow = sx + rho * PITCH;
+  __syncthreads();
+  for (int b = 0; b < B; ++b) {
+    float2 a[M2];
+    if (active) {
+      const HT* x = H + (int64_t)b * S + row * h2;
+#pragma unroll
+      for (int k2 = 0; k2 < M2; ++k2) {
+        const int k = j + M1 * k2;
+        float2 xa = Store<HT>::load(x + k), xc = Store<HT>::load(x + (M - k));
+        if (k == 0) { xa.y = 0.f; xc.y = 0.f; }
+        const float2 cc = fft::cconj(xc);
+        const float2 E = fft::cadd(xa, cc);
+        const float2 O = fft::cmul(fft::csub(xa, cc), fft::cconj(tw[k]));
+        a[k2] = make_float2(E.x - O.y, E.y + O.x);
+      }
+      fft::dft_small<M2, 1>(a);
+#pragma unroll
+      for (int n2 = 1; n2 < M2; ++n2) a[n2] = fft::cmul(a[n2], fft::cconj(tw[(2 * n2 * j) % N2]));
+#pragma unroll
+      for (int n2 = 0; n2 < M2; ++n2) srow[n2 * (M1 + 1) + j] = a[n2];
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int n2 = j + M1 * c;
+        float2 z[M1];
+#pragma unroll
+        for (int k1 = 0; k1 < M1; ++k1) z[k1] = srow[n2 * (M1 + 1) + k1];
+        fft::dft_small<M1, 1>(z);
+#pragma unroll
+        for (int n1 = 0; n1 < M1; ++n1) {
+          const int64_t vox = vrow + 2 * (n2 + M2 * n1);
+          const float d0 = inv_den ? __ldg(inv_den + vox) : 1.f;
+          const float d1 = inv_den ? __ldg(inv_den + vox + 1) : 1.f;
+          const float s0 = z[n1].x * scale * d0, s1 = z[n1].y * scale * d1;
+          const int slot = (c * M1 + n1) * 2;
+          if (s0 > best[slot]) { best[slot] = s0; arg[slot] = first_index + b; }
+          if (s1 > best[slot + 1]) { best[slot + 1] = s1; arg[slot + 1] = first_index + b; }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!active) return;
+#pragma unroll
+  for (int c = 0; c < C; ++c)
+#pragma unroll
+    for (int n1 = 0; n1 < M1; ++n1)
+#pragma unroll
+      for (int part = 0; part < 2; ++part) {
+        const int slot = (c * M1 + n1) * 2 + part;
+        const int64_t g = vrow + 2 * (j + M1 * c + M2 * n1) + part;
+        if (arg[slot] >= 0 && best[slot] > state_max[g]) {
+          state_max[g] = best[slot];
+          state_rot[g] = arg[slot];
+        }
+      }
+}
+
+template <int M1, int M2>
+constexpr size_t zpass4_smem() {
+  return sizeof(float2) * (2 * M1 * M2 + (256 / M1) * M2 * (M1 + 1));
+}
+
 // ------------------------------------------------------------------ helpers
 __global__ void sum_double_kernel(const float* __restrict__ x, int64_t n, double* __restrict__ out) {
   __shared__ double sh[32];
@@ -895,9 +996,51 @@ static void set_zpass_attrs(int m, int smem) {
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem)));
 }
 
+#define TM_DISPATCH_4STEP(m, CALL)                                  \
+  switch (m) {                                                      \
+    case 32: { constexpr int A1 = 4, A2 = 8; CALL; } break;         \
+    case 50: { constexpr int A1 = 5, A2 = 10; CALL; } break;        \
+    case 64: { constexpr int A1 = 8, A2 = 8; CALL; } break;         \
+    case 80: { constexpr int A1 = 4, A2 = 20; CALL; } break;        \
+    case 100: { constexpr int A1 = 10, A2 = 10; CALL; } break;      \
+    case 128: { constexpr int A1 = 8, A2 = 16; CALL; } break;       \
+    case 200: { constexpr int A1 = 10, A2 = 20; CALL; } break;      \
+    case 256: { constexpr int A1 = 16, A2 = 16; CALL; } break;      \
+    default: break;                                                 \
+  }
+
+static bool zpass4_supported(int m) {
+  return m == 32 || m == 50 || m == 64 || m == 80 || m == 100 || m == 128 || m == 200 ||
+         m == 256;
+}
+
+template <typename HT>
+static void launch_zpass4(Scan* s, HT* H, int nb, int64_t rows, float out_scale, int32_t first,
+                          float* state_max, int32_t* state_rot, cudaStream_t st) {
+  TM_DISPATCH_4STEP(s->n2 / 2, ({
+    constexpr int RW = 256 / A1;
+    dim3 g(ceil_div(rows, RW));
+    zpass4_kernel<HT, A1, A2><<<g, A1 * RW, zpass4_smem<A1, A2>(), st>>>(
+        H, nb, rows, s->h2, s->tw2, out_scale, s->inv_den, first, state_max, state_rot, s->S);
+  }));
+}
+
+static void set_zpass4_attrs(int m) {
+  TM_DISPATCH_4STEP(m, ({
+    cudaFuncSetAttribute(zpass4_kernel<float2, A1, A2>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zpass4_smem<A1, A2>());
+    cudaFuncSetAttribute(zpass4_kernel<__half2, A1, A2>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zpass4_smem<A1, A2>());
+  }));
+}
+
 template <typename HT>
 static void launch_zpass(Scan* s, dim3 g4, HT* H, int nb, int64_t rows, float out_scale,
                          int32_t first, float* state_max, int32_t* state_rot, cudaStream_t st) {
+  if (zpass4_supported(s->n2 / 2) && !getenv("PYTME_B200_GENERIC_FFT")) {
+    launch_zpass4<HT>(s, H, nb, rows, out_scale, first, state_max, state_rot, st);
+    return;
+  }
   TM_DISPATCH_M(s->n2 / 2, (zpass_kernel<HT, MM><<<g4, kThreads, s->smem4, st>>>(
                                H, nb, rows, s->n2, s->h2, s->R4, s->pm, s->tw2, out_scale,
                                s->inv_den, first, state_max, state_rot, s->S)));
@@ -1185,6 +1328,7 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     cudaFuncSetAttribute(ypass_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem3);
     cudaFuncSetAttribute(ypass_kernel<__half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem3);
     set_zpass_attrs(s->n2 / 2, (int)s->smem4);
+    set_zpass4_attrs(s->n2 / 2);
     s->reg0 = reg_supported(s->n0) && !getenv("PYTME_B200_GENERIC_FFT");
     s->reg1 = reg_supported(s->n1) && !getenv("PYTME_B200_GENERIC_FFT");
     size_t zy = 0;

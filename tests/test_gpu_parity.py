@@ -306,3 +306,21 @@ def test_flcsm_config3_shape(torch_cuda):
     r = _scan("FLCSphericalMask", target, tmpl, mask, rots, precision="mixed", batch=2)
     ref = O.scan(target, tmpl, rots, "FLCSphericalMask", template_mask=mask)
     assert np.abs(r[0] - ref["scores"]).max() <= TOL
+
+
+@pytest.mark.parametrize("n2", [64, 100, 128, 160, 200, 256, 400, 512])
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_zpass_lengths(torch_cuda, n2, precision):
+    """Every z-axis length with a dedicated c2r kernel (and the generic fallback for the
+    others) against the FP32 oracle on a small FLCSphericalMask scan."""
+    from pytme_b200 import synthetic as syn
+
+    rng = np.random.default_rng(n2)
+    tmpl = syn.blob_template(8, rng, radius=2.0, sigma=1.0)
+    mask = syn.spherical_mask((8,) * 3, 4, center=(3.5,) * 3)
+    target, _, _ = syn.make_tomogram((32, 32, n2), tmpl, 3, rng, scale=0.5)
+    rots = syn.random_rotation_matrices(6, rng)
+    r = _scan("FLCSphericalMask", target, tmpl, mask, rots, precision=precision, batch=4)
+    ref = O.scan(target, tmpl, rots, "FLCSphericalMask", template_mask=mask)
+    tol = TOL if precision == "fp32" else mixed_tol(ref["scores"])
+    assert np.abs(r[0] - ref["scores"]).max() <= tol
