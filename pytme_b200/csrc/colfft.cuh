@@ -142,24 +142,67 @@ __device__ __forceinline__ int stage_pos(int t, int i, int r) {
   return p * L + q + LR * r;
 }
 
+// Shared-memory address of value (i, r) of thread t at stage S, written as a per-thread
+// base plus a compile-time offset: positions p*L + q + LR*r with LR a multiple of 8 (or
+// LR = 1 on the last stage, where p*L is a multiple of 8 and q = 0) keep pos >> 3 affine
+// in (i, r), so the padded address is affine too.
+template <int N, int W, int S>
+__device__ __forceinline__ int stage_base(int l, int t) {
+  constexpr int L = stage_size(N, S);
+  constexpr int R = stage_radix(N, S);
+  constexpr int NB = 8 / R;
+  constexpr int LR = L / R;
+  const int b = t * NB;
+  const int pos = (b / LR) * L + (b % LR);
+  return saddr<W>(l, pos);
+}
+
+template <int N, int W, int S>
+__device__ __forceinline__ constexpr int stage_off(int i, int r) {
+  constexpr int L = stage_size(N, S);
+  constexpr int R = stage_radix(N, S);
+  constexpr int LR = L / R;
+  if constexpr (LR > 1) {
+    // radix-8 stage, one butterfly per thread (q < LR): (q + LR*r) >> 3 equals
+    // (q >> 3) + (LR*r >> 3) because LR*r is a multiple of 8 or q + (LR*r mod 8) < 8
+    return (LR * r) * W + W * ((LR * r) >> 3);
+  } else {
+    // LR == 1: positions b*L + r with b = t*NB + i; t*NB*L is a multiple of 8
+    const int d = i * L + r;
+    return d * W + W * (d >> 3);
+  }
+}
+
 template <int N, int W, int S>
 __device__ __forceinline__ void load_stage(float2 (&v)[8], const float2* sm, int l, int t) {
   constexpr int R = stage_radix(N, S);
   constexpr int NB = 8 / R;
+  const float2* base = sm + stage_base<N, W, S>(l, t);
 #pragma unroll
   for (int i = 0; i < NB; ++i)
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[i * R + r] = sm[saddr<W>(l, stage_pos<N, S>(t, i, r))];
+    for (int r = 0; r < R; ++r) v[i * R + r] = base[stage_off<N, W, S>(i, r)];
 }
 
 template <int N, int W, int S>
 __device__ __forceinline__ void store_stage(const float2 (&v)[8], float2* sm, int l, int t) {
   constexpr int R = stage_radix(N, S);
   constexpr int NB = 8 / R;
+  float2* base = sm + stage_base<N, W, S>(l, t);
 #pragma unroll
   for (int i = 0; i < NB; ++i)
 #pragma unroll
-    for (int r = 0; r < R; ++r) sm[saddr<W>(l, stage_pos<N, S>(t, i, r))] = v[i * R + r];
+    for (int r = 0; r < R; ++r) base[stage_off<N, W, S>(i, r)] = v[i * R + r];
+}
+
+// Frequency index of value (i, r) after the last forward stage: the last digit r is the
+// most significant frequency digit, so k = digitrev(p*R) + r*(N/R) with p = t*NB + i.
+template <int N>
+__device__ __forceinline__ int out_index(int t, int i, int r) {
+  constexpr int S = num_stages(N) - 1;
+  constexpr int R = stage_radix(N, S);
+  constexpr int NB = 8 / R;
+  return digitrev<N>((t * NB + i) * R) + r * (N / R);
 }
 
 // Forward (DIR=-1) or inverse (DIR=+1) DIF transform of the thread's line: v holds

@@ -95,6 +95,23 @@ template <> struct Store<__half2> {
   static __device__ __forceinline__ void store(__half2* p, float2 v) { *p = __float22half2_rn(v); }
 };
 
+// Asynchronous global -> shared copies (cp.async): the next tile is staged in shared
+// memory while the current one is transformed. Each thread later reads back only the
+// elements it copied, so a thread-local wait_group suffices.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (BYTES == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING));
+}
+
 constexpr int kThreads = 512;
 constexpr int kMaxE = 8;             // complex elements per thread in a line-FFT tile
 constexpr int kTile = kThreads * kMaxE;  // elements per tile (4096)
@@ -315,7 +332,7 @@ tmpl_zy_reg_kernel(const float* __restrict__ tmpl, int t0, int t1, int t2, int n
     for (int i = 0; i < 8 / R; ++i)
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int k1 = colfft::digitrev<N>(colfft::last_pos<N>(t, i, r));
+        const int k1 = colfft::out_index<N>(t, i, r);
         dst[(int64_t)k1 * h2 + k2] = v[i * R + r];
       }
   }
@@ -344,7 +361,7 @@ xpass_reg_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, in
   for (int i = 0; i < 8 / R; ++i)
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int k0 = colfft::digitrev<N>(colfft::last_pos<N>(t, i, r));
+      const int k0 = colfft::out_index<N>(t, i, r);
       float2 v = valid ? __ldg(Ft + ((int64_t)k0 * n1 + k1) * h2 + k2) : make_float2(0.f, 0.f);
       f[i * R + r] = make_float2(v.x * scale, v.y * scale);
     }
@@ -374,9 +391,13 @@ xpass_reg_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, in
   }
 }
 
-// K3': y pass (inverse FFT along axis 1, in place). grid (ceil(h2/W), n0, B); N = n1.
+// K3': y pass (inverse FFT along axis 1, in place). grid (ceil(h2/W), ceil(n0/XP), B);
+// each CTA walks XP consecutive x planes; the next plane's columns are staged in shared
+// memory with cp.async while the current plane is transformed. N = n1.
+constexpr int kYPlanes = 4;
+
 template <int N, int W, typename HT>
-__global__ void __launch_bounds__(N / 8 * W, 1)
+__global__ void __launch_bounds__(N / 8 * W, 1024 / (N / 8 * W))
 ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ tw1_g) {
   constexpr int T = N / 8;
   constexpr int NT = T * W;
@@ -384,27 +405,54 @@ ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ 
   extern __shared__ float4 smem_raw[];
   float2* tw = reinterpret_cast<float2*>(smem_raw);
   float2* sm = tw + N;
+  HT* stage = reinterpret_cast<HT*>(sm + colfft::smem_elems<N>(W));  // 2 x N*W staging
   const int tid = threadIdx.x, l = tid % W, t = tid / W;
   const int k2 = blockIdx.x * W + l;
-  const int x = blockIdx.y, b = blockIdx.z;
+  const int x0 = blockIdx.y * kYPlanes, b = blockIdx.z;
+  const int nx = min(kYPlanes, n0 - x0);
   const bool valid = k2 < h2;
   for (int i = tid; i < N; i += NT) tw[i] = tw1_g[i];
-  __syncthreads();
-  HT* h = H + ((int64_t)b * n0 + x) * N * h2 + k2;
-  float2 v[8];
-#pragma unroll
-  for (int r = 0; r < 8; ++r)
-    v[r] = valid ? Store<HT>::load(h + (int64_t)(t + T * r) * h2) : make_float2(0.f, 0.f);
-  colfft::dif_stage_regs<N, 0, 1>(v, t, tw);
-  dif_rest<N, W, 1>(v, sm, tw, l, t);
+  HT* base = H + ((int64_t)b * n0 + x0) * N * h2 + k2;
+  const int64_t plane = (int64_t)N * h2;
   if (valid) {
 #pragma unroll
-    for (int i = 0; i < 8 / R; ++i)
+    for (int r = 0; r < 8; ++r)
+      cp_async<sizeof(HT)>(stage + (t + T * r) * W + l, base + (int64_t)(t + T * r) * h2);
+  }
+  cp_async_commit();
+  __syncthreads();
+  for (int xi = 0; xi < nx; ++xi) {
+    HT* cur = stage + (xi & 1) * N * W;
+    if (xi + 1 < nx) {
+      HT* nb = stage + ((xi + 1) & 1) * N * W;
+      if (valid) {
+        const HT* hn = base + (int64_t)(xi + 1) * plane;
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int y = colfft::digitrev<N>(colfft::last_pos<N>(t, i, r));
-        Store<HT>::store(h + (int64_t)y * h2, v[i * R + r]);
+        for (int r = 0; r < 8; ++r)
+          cp_async<sizeof(HT)>(nb + (t + T * r) * W + l, hn + (int64_t)(t + T * r) * h2);
       }
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    float2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+      v[r] = valid ? Store<HT>::load(cur + (t + T * r) * W + l) : make_float2(0.f, 0.f);
+    colfft::dif_stage_regs<N, 0, 1>(v, t, tw);
+    dif_rest<N, W, 1>(v, sm, tw, l, t);
+    if (valid) {
+      HT* h = base + (int64_t)xi * plane;
+#pragma unroll
+      for (int i = 0; i < 8 / R; ++i)
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int y = colfft::out_index<N>(t, i, r);
+          Store<HT>::store(h + (int64_t)y * h2, v[i * R + r]);
+        }
+    }
+    __syncthreads();  // the next plane's stage-0 stores reuse the exchange buffer
   }
 }
 
@@ -435,7 +483,7 @@ xpass_flc_reg_kernel(const float2* __restrict__ Gt, const float2* __restrict__ G
   for (int i = 0; i < 8 / R; ++i)
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int k0 = colfft::digitrev<N>(colfft::last_pos<N>(t, i, r));
+      const int k0 = colfft::out_index<N>(t, i, r);
       foff[i * R + r] = ((int64_t)k0 * n1 + k1) * h2 + k2;
     }
   __syncthreads();
@@ -513,6 +561,11 @@ size_t reg_smem_bytes(int n2, int t1, int t2, bool with_plane) {
   size_t b = sizeof(float2) * (N + colfft::smem_elems<N>(reg_lines<N>()));
   if (with_plane) b += sizeof(float2) * n2 + sizeof(float) * t1 * t2;
   return b;
+}
+
+template <int N, typename HT>
+size_t ypass_smem_bytes() {
+  return reg_smem_bytes<N>(0, 0, 0, false) + 2 * sizeof(HT) * N * reg_lines<N>();
 }
 
 static bool reg_supported(int n) {
@@ -1053,8 +1106,8 @@ static void set_reg_attrs(size_t zy_smem) {
   const int sm = (int)reg_smem_bytes<N>(0, 0, 0, false);
   cudaFuncSetAttribute(xpass_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   cudaFuncSetAttribute(xpass_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(ypass_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(ypass_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(ypass_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ypass_smem_bytes<N, float2>());
+  cudaFuncSetAttribute(ypass_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ypass_smem_bytes<N, __half2>());
   cudaFuncSetAttribute(tmpl_zy_reg_kernel<N, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zy_smem);
   cudaFuncSetAttribute(xpass_flc_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   cudaFuncSetAttribute(xpass_flc_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
@@ -1102,8 +1155,8 @@ static void launch_xpass_reg(Scan* s, int nb, float hs, HT* H, cudaStream_t st) 
 template <int N, typename HT>
 static void launch_ypass_reg(Scan* s, int nb, HT* H, cudaStream_t st) {
   constexpr int W = reg_lines<N>();
-  dim3 g(ceil_div(s->h2, W), s->n0, nb);
-  ypass_reg_kernel<N, W, HT><<<g, N / 8 * W, reg_smem_bytes<N>(0, 0, 0, false), st>>>(
+  dim3 g(ceil_div(s->h2, W), ceil_div(s->n0, kYPlanes), nb);
+  ypass_reg_kernel<N, W, HT><<<g, N / 8 * W, ypass_smem_bytes<N, HT>(), st>>>(
       H, s->n0, s->h2, s->tw1);
 }
 

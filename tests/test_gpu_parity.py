@@ -324,3 +324,19 @@ def test_zpass_lengths(torch_cuda, n2, precision):
     ref = O.scan(target, tmpl, rots, "FLCSphericalMask", template_mask=mask)
     tol = TOL if precision == "fp32" else mixed_tol(ref["scores"])
     assert np.abs(r[0] - ref["scores"]).max() <= tol
+
+
+@pytest.mark.parametrize("shape", [(128, 128, 24), (256, 64, 24), (64, 256, 20), (1024, 128, 16)])
+def test_xy_lengths(torch_cuda, shape):
+    """Register-resident column kernels for every power-of-two x/y length (and mixed
+    x/y) against the FP32 oracle."""
+    from pytme_b200 import synthetic as syn
+
+    rng = np.random.default_rng(sum(shape))
+    tmpl = syn.blob_template(8, rng, radius=2.0, sigma=1.0)
+    mask = syn.spherical_mask((8,) * 3, 4, center=(3.5,) * 3)
+    target, _, _ = syn.make_tomogram(shape, tmpl, 3, rng, scale=0.5)
+    rots = syn.random_rotation_matrices(5, rng)
+    r = _scan("FLCSphericalMask", target, tmpl, mask, rots, precision="fp32", batch=3)
+    ref = O.scan(target, tmpl, rots, "FLCSphericalMask", template_mask=mask)
+    assert np.abs(r[0] - ref["scores"]).max() <= TOL
