@@ -86,6 +86,15 @@ __device__ __forceinline__ void dftR(float2* v) {
   else fft::dft2<DIR>(v);
 }
 
+// Twiddles w^j (j = 1..R-1) of one butterfly from a single table read: powers by
+// repeated complex multiplication (error ~j ulp, far below the FP32 FFT's own).
+template <int R>
+__device__ __forceinline__ void twiddle_powers(float2 (&w)[R], float2 w1) {
+  w[1] = w1;
+#pragma unroll
+  for (int j = 2; j < R; ++j) w[j] = cmul(w[j - 1], w1);
+}
+
 // One forward-structured DIF stage s (DIR -1: forward DFT, +1: inverse DFT with
 // conjugate twiddles) on values already in registers; twiddles applied after the
 // butterflies. v holds the thread's 8 values in the order (butterfly i, r).
@@ -101,12 +110,12 @@ __device__ __forceinline__ void dif_stage_regs(float2 (&v)[8], int t, const floa
     if constexpr (LR > 1) {
       const int b = t * NB + i;
       const int q = b % LR;
+      float2 w1 = tw[q * (N / L)];
+      if (DIR > 0) w1 = cconj(w1);
+      float2 w[R];
+      twiddle_powers<R>(w, w1);
 #pragma unroll
-      for (int j = 1; j < R; ++j) {
-        float2 w = tw[j * q * (N / L)];
-        if (DIR > 0) w = cconj(w);
-        v[i * R + j] = cmul(v[i * R + j], w);
-      }
+      for (int j = 1; j < R; ++j) v[i * R + j] = cmul(v[i * R + j], w[j]);
     }
   }
 }
@@ -123,8 +132,10 @@ __device__ __forceinline__ void dif_stage_adjoint_regs(float2 (&v)[8], int t, co
     if constexpr (LR > 1) {
       const int b = t * NB + i;
       const int q = b % LR;
+      float2 w[R];
+      twiddle_powers<R>(w, cconj(tw[q * (N / L)]));
 #pragma unroll
-      for (int j = 1; j < R; ++j) v[i * R + j] = cmul(v[i * R + j], cconj(tw[j * q * (N / L)]));
+      for (int j = 1; j < R; ++j) v[i * R + j] = cmul(v[i * R + j], w[j]);
     }
     dftR<R, 1>(&v[i * R]);
   }

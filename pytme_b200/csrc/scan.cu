@@ -253,9 +253,14 @@ ypass_kernel(HT* __restrict__ H, int n0, int n1, int h2, int W, LinePlan p1,
 // x[t] * W_N^(j*t).
 template <int N>
 __device__ __forceinline__ void stage0_single(float2 (&v)[8], int t, const float2* tw) {
-  const float2 x = v[0];
+  const float2 w1 = tw[t];
+  float2 x = v[0];
+  v[0] = x;
 #pragma unroll
-  for (int j = 0; j < 8; ++j) v[j] = j == 0 ? x : fft::cmul(x, tw[j * t]);
+  for (int j = 1; j < 8; ++j) {
+    x = fft::cmul(x, w1);
+    v[j] = x;
+  }
 }
 
 template <int N, int W, int DIR>
@@ -340,7 +345,7 @@ tmpl_zy_reg_kernel(const float* __restrict__ tmpl, int t0, int t1, int t2, int n
 
 // K2': x pass. grid (ceil(h2/W), n1); N = n0; loops over the rotations of the group.
 template <int N, int W, typename HT>
-__global__ void __launch_bounds__(N / 8 * W, 1)
+__global__ void __launch_bounds__(N / 8 * W, 1024 / (N / 8 * W))
 xpass_reg_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, int B, int t0,
                  int n1, int h2, const float2* __restrict__ tw0_g, float scale,
                  HT* __restrict__ H) {
@@ -355,20 +360,13 @@ xpass_reg_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, in
   const int k1 = blockIdx.y;
   const bool valid = k2 < h2;
   for (int i = tid; i < N; i += NT) tw[i] = tw0_g[i];
-  // the target-spectrum values this thread multiplies, for every rotation
-  float2 f[8];
-#pragma unroll
-  for (int i = 0; i < 8 / R; ++i)
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int k0 = colfft::out_index<N>(t, i, r);
-      float2 v = valid ? __ldg(Ft + ((int64_t)k0 * n1 + k1) * h2 + k2) : make_float2(0.f, 0.f);
-      f[i * R + r] = make_float2(v.x * scale, v.y * scale);
-    }
+  // offsets of the target-spectrum values this thread multiplies (through L1, reused
+  // by every rotation of the group)
+  const int64_t col = (int64_t)k1 * h2 + k2;
+  const int64_t row = (int64_t)n1 * h2;
+  const float2* fb = Ft + (int64_t)colfft::out_index<N>(t, 0, 0) * row + col;
   __syncthreads();
   const int64_t S = (int64_t)N * n1 * h2;
-  const int64_t row = (int64_t)n1 * h2;
-  const int64_t col = (int64_t)k1 * h2 + k2;
   for (int b = 0; b < B; ++b) {
     const float2* g = G + (int64_t)b * t0 * row + col;
     float2 v[8];
@@ -381,7 +379,15 @@ xpass_reg_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, in
     else colfft::dif_stage_regs<N, 0, -1>(v, t, tw);
     dif_rest<N, W, -1>(v, sm, tw, l, t);
 #pragma unroll
-    for (int e = 0; e < 8; ++e) v[e] = fft::cmul(v[e], f[e]);
+    for (int i = 0; i < 8 / R; ++i)
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        // out_index(t, i, r) = out_index(t, i, 0) + r * N/R; out_index(t, i, 0) - out_index(t, 0, 0)
+        // depends on i only through compile-time digits
+        const int dk = colfft::out_index<N>(t, i, r) - colfft::out_index<N>(t, 0, 0);
+        const float2 f = valid ? __ldg(fb + (int64_t)dk * row) : make_float2(0.f, 0.f);
+        v[i * R + r] = fft::cmul(v[i * R + r], make_float2(f.x * scale, f.y * scale));
+      }
     colfft::dif_adjoint<N, W>(v, sm, tw, l, t);
     if (valid) {
       HT* h = H + (int64_t)b * S + col;
