@@ -785,11 +785,23 @@ zpass4_kernel(const HT* __restrict__ H, int B, int64_t rows, int h2,
   extern __shared__ float4 smem_raw[];
   float2* tw = reinterpret_cast<float2*>(smem_raw);
   float2* sx = tw + N2;
+  HT* stage = reinterpret_cast<HT*>(sx + RW * PITCH);  // 2 x RW*h2 staged rows
   const int tid = threadIdx.x;
   const int rho = tid / M1, j = tid % M1;
   for (int i = tid; i < N2; i += NT) tw[i] = tw2_g[i];
-  const int64_t row = (int64_t)blockIdx.x * RW + rho;
-  const bool active = rho < RW && row < rows;
+  const int64_t row0 = (int64_t)blockIdx.x * RW;
+  const int nrows = (int)min((int64_t)RW, rows - row0);
+  const int64_t row = row0 + rho;
+  const bool active = rho < RW && rho < nrows;
+  const int nel = nrows * h2;
+  // rows of this CTA are contiguous in every rotation's H: stage them with cp.async,
+  // one rotation ahead of the transform
+  auto stage_copy = [&](int bb) {
+    const HT* src = H + (int64_t)bb * S + row0 * h2;
+    HT* dst = stage + (bb & 1) * RW * h2;
+    for (int e = tid; e < nel; e += NT) cp_async<sizeof(HT)>(dst + e, src + e);
+    cp_async_commit();
+  };
   float best[V];
   int32_t arg[V];
 #pragma unroll
@@ -797,11 +809,18 @@ zpass4_kernel(const HT* __restrict__ H, int B, int64_t rows, int h2,
   // voxel of output slot (c, n1, part): 2*(n2 + M2*n1) + part with n2 = j + M1*c
   const int64_t vrow = row * N2;
   float2* srow = sx + rho * PITCH;
-  __syncthreads();
+  if (B > 0) stage_copy(0);
   for (int b = 0; b < B; ++b) {
+    if (b + 1 < B) {
+      stage_copy(b + 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
     float2 a[M2];
     if (active) {
-      const HT* x = H + (int64_t)b * S + row * h2;
+      const HT* x = stage + (b & 1) * RW * h2 + rho * h2;
 #pragma unroll
       for (int k2 = 0; k2 < M2; ++k2) {
         const int k = j + M1 * k2;
@@ -857,9 +876,11 @@ zpass4_kernel(const HT* __restrict__ H, int B, int64_t rows, int h2,
       }
 }
 
-template <int M1, int M2>
+template <int M1, int M2, typename HT = float2>
 constexpr size_t zpass4_smem() {
-  return sizeof(float2) * (2 * M1 * M2 + (256 / M1) * M2 * (M1 + 1));
+  // twiddles + exchange + two staged row blocks (h2 = M1*M2 + 1)
+  return sizeof(float2) * (2 * M1 * M2 + (256 / M1) * M2 * (M1 + 1)) +
+         2 * sizeof(HT) * (256 / M1) * (M1 * M2 + 1);
 }
 
 // ------------------------------------------------------------------ helpers
@@ -1079,17 +1100,17 @@ static void launch_zpass4(Scan* s, HT* H, int nb, int64_t rows, float out_scale,
   TM_DISPATCH_4STEP(s->n2 / 2, ({
     constexpr int RW = 256 / A1;
     dim3 g(ceil_div(rows, RW));
-    zpass4_kernel<HT, A1, A2><<<g, A1 * RW, zpass4_smem<A1, A2>(), st>>>(
+    zpass4_kernel<HT, A1, A2><<<g, A1 * RW, zpass4_smem<A1, A2, HT>(), st>>>(
         H, nb, rows, s->h2, s->tw2, out_scale, s->inv_den, first, state_max, state_rot, s->S);
   }));
 }
 
 static void set_zpass4_attrs(int m) {
   TM_DISPATCH_4STEP(m, ({
-    cudaFuncSetAttribute(zpass4_kernel<float2, A1, A2>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zpass4_smem<A1, A2>());
-    cudaFuncSetAttribute(zpass4_kernel<__half2, A1, A2>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zpass4_smem<A1, A2>());
+    cudaFuncSetAttribute(zpass4_kernel<float2, A1, A2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)zpass4_smem<A1, A2, float2>());
+    cudaFuncSetAttribute(zpass4_kernel<__half2, A1, A2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)zpass4_smem<A1, A2, __half2>());
   }));
 }
 
