@@ -58,6 +58,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--small", action="store_true", help="128x128x64 / 24^3 quick check")
+    ap.add_argument("--profile-case", default=None, metavar="N0,N1,N2",
+                    help="run --groups launch groups of the fused scan on a target of this "
+                         "shape and exit (a small case for ncu captures; no timing, no JSON)")
+    ap.add_argument("--groups", type=int, default=2)
     return ap.parse_args()
 
 
@@ -73,6 +77,13 @@ def make_inputs(small=False):
     target, _, _ = syn.make_tomogram(shape, tmpl, 20 if small else 300, rng, snr=0.05, mask=mask)
     rots = syn.rotations_for_angle(ANGLE)
     return target, tmpl, mask, rots
+
+
+# DRAM bytes (read + write) of one x-pass launch of the benchmark configuration
+# (512x512x200, 48^3 template, mixed precision, 32 rotations per group), from the ncu
+# capture summarised in profiles/xpass_flcsm_512x512x48_t48_b8.md, scaled from the
+# captured 512x512x48 / 8-rotation launch by columns and rotations.
+NCU_TRAFFIC = {("xpass", "mixed", 32): 3.91e9}
 
 
 def measured_peaks():
@@ -331,7 +342,9 @@ def run_ours(args):
             "voxel_rotations_per_s": value * float(np.prod(fast)),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "alg_bytes_per_launch": alg,
+                         "traffic": NCU_TRAFFIC.get((dom, args.precision, args.batch))
+                         if not args.small else None,
+                         "alg_bytes_per_launch": alg,
                          "avg_launch_ms": avg_ms},
             "stages": stages,
             "plain": {"value": plain_rate, "unit": "rotations/s", "rotations": args.plain_rotations,
@@ -381,8 +394,41 @@ def run_ours(args):
     return 0
 
 
+def run_profile_case(args):
+    """A fixed amount of fused-scan work for profilers: FLCSphericalMask with a 48^3
+    blob template on an N(0,1) target of the given shape, --groups groups of --batch
+    rotations."""
+    import torch
+
+    from pytme_b200 import synthetic as syn
+    from pytme_b200.matching import rigid_transform_matrices
+    from pytme_b200.scores import ScanPlan
+
+    shape = tuple(int(x) for x in args.profile_case.split(","))
+    t = TSIZE
+    rng = np.random.default_rng(0)
+    tmpl = syn.blob_template(t, rng, sigma=1.5 * t / 16, radius=5.0 * t / 16)
+    mask = syn.spherical_mask((t,) * 3, t / 2, center=((t - 1) / 2,) * 3)
+    target = rng.normal(size=shape).astype(np.float32)
+    plan = ScanPlan("FLCSphericalMask", shape, (t,) * 3, precision=args.precision,
+                    batch=args.batch)
+    plan.set_template(tmpl[::-1, ::-1, ::-1].copy(), mask[::-1, ::-1, ::-1].copy())
+    plan.set_target(torch.as_tensor(target, device="cuda"))
+    rots = syn.super_fibonacci_rotations(args.batch * args.groups)
+    m = torch.as_tensor(rigid_transform_matrices(rots, ((t - 1) / 2,) * 3), device="cuda")
+    smax = torch.zeros(shape, device="cuda")
+    sarg = torch.full(shape, -1, dtype=torch.int32, device="cuda")
+    for g in range(args.groups):
+        plan.run(m[g * args.batch:(g + 1) * args.batch], g * args.batch, smax, sarg)
+    torch.cuda.synchronize()
+    print("profile case done", shape, float(smax.max()))
+    return 0
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        return run_profile_case(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
