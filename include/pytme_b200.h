@@ -155,6 +155,13 @@ int tm_scan_run(tm_scan* plan, const float* matrices, int n, int32_t first_index
 #define TM_STAGE_ZPASS 4    /* axis-2 c2r, score scaling, max/argmax update */
 #define TM_NUM_STAGES 5
 int tm_scan_set_timing(tm_scan* plan, int enable); /* also resets the counters */
+
+/* Replay full launch groups of the fused path from one captured CUDA graph (the
+ * template preparation and the four passes). The first full group of tm_scan_run
+ * captures it for the given max_scores/argmax buffers (a different pair recaptures);
+ * later groups copy their matrices and first index into the plan and replay it,
+ * ordered on the caller's stream. Ignored by the plain path and while timing. */
+int tm_scan_set_graph(tm_scan* plan, int enable);
 int tm_scan_get_timing(const tm_scan* plan, double* ms, int64_t* launches); /* TM_NUM_STAGES each */
 /* Algorithmic HBM bytes of one launch of `stage` for a group of nb rotations. */
 int64_t tm_scan_stage_bytes(const tm_scan* plan, int stage, int nb);

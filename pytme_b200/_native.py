@@ -36,7 +36,8 @@ EXPORTED = (
     "tm_normalize_template", "tm_norm_scores", "tm_max_score_over_rotations",
     "tm_fft_plan_create", "tm_fft_plan_destroy", "tm_fft_r2c", "tm_fft_c2r",
     "tm_scan_create", "tm_scan_destroy", "tm_scan_device_bytes", "tm_scan_set_template",
-    "tm_scan_set_target", "tm_scan_run", "tm_scan_set_timing", "tm_scan_get_timing",
+    "tm_scan_set_target", "tm_scan_run", "tm_scan_set_timing", "tm_scan_set_graph",
+    "tm_scan_get_timing",
     "tm_scan_stage_bytes", "tm_max_filter_peaks",
     "tm_find_candidate_indices_workspace", "tm_find_candidate_indices",
     "tm_find_candidate_indices_noalloc", "tm_line_fft_test",
@@ -86,6 +87,7 @@ def _load():
         "tm_scan_set_target": (c_int, [vp, f32p, vp]),
         "tm_scan_run": (c_int, [vp, f32p, c_int, c_int32, f32p, i32p, vp]),
         "tm_scan_set_timing": (c_int, [vp, c_int]),
+        "tm_scan_set_graph": (c_int, [vp, c_int]),
         "tm_scan_get_timing": (c_int, [vp, vp, vp]),
         "tm_scan_stage_bytes": (c_int64, [vp, c_int, c_int]),
         "tm_max_filter_peaks": (c_int, [f32p, c_int, c_int, c_int, c_int, f32p, f32p, vp, vp]),

@@ -1,0 +1,170 @@
+"""Many (tomogram, template) jobs of different sizes, and the rotation-batch autotuner.
+
+``scan_batch`` runs a list of jobs, each a target with its own template, mask,
+filters and rotation set. Jobs that share a score, transform shape and template shape
+reuse one ``ScanPlan`` (its spectra, scratch and cuFFT plans); each job only uploads
+its target and template. Full launch groups replay one captured CUDA graph per plan.
+Results come back per job in the reference's ``MaxScoreOverRotations.result``
+layout.
+
+``autotune_batch`` times candidate rotations-per-launch-group values on the real
+target and caches the fastest per (GPU, score, shapes, precision) in a JSON file
+(``$PYTME_B200_CACHE`` or ``~/.cache/pytme_b200/autotune.json``).
+"""
+from __future__ import annotations
+
+import json
+import os
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from .matching import apply_convolution_mode, fourier_padding, rigid_transform_matrices
+from .scores import ScanPlan, _prepare_target
+
+__all__ = ["MatchJob", "scan_batch", "autotune_batch"]
+
+
+@dataclass
+class MatchJob:
+    """One exhaustive search: target, template (as given, not reversed), optional
+    mask, rotations (n, 3, 3) and optional filters (arrays at the template's and the
+    transform's rfft shapes)."""
+
+    target: np.ndarray
+    template: np.ndarray
+    rotations: np.ndarray
+    mask: Optional[np.ndarray] = None
+    score: str = "FLCSphericalMask"
+    template_filter: Optional[np.ndarray] = None
+    target_filter: Optional[np.ndarray] = None
+    score_threshold: float = 0.0
+    meta: Dict = field(default_factory=dict)
+
+
+def _cache_path() -> str:
+    return os.environ.get("PYTME_B200_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "pytme_b200",
+                                       "autotune.json"))
+
+
+def _cache_load() -> Dict:
+    try:
+        with open(_cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _cache_store(data: Dict) -> None:
+    path = _cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        with open(path, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+    except OSError:
+        pass
+
+
+def _key(score, fast, tshape, precision) -> str:
+    name = torch.cuda.get_device_name(torch.cuda.current_device())
+    return f"{name}|{score}|{'x'.join(map(str, fast))}|{'x'.join(map(str, tshape))}|{precision}"
+
+
+def autotune_batch(job: MatchJob, precision: str = "mixed",
+                   candidates: Sequence[int] = (8, 16, 32, 64), groups: int = 2,
+                   use_cache: bool = True) -> int:
+    """Fastest rotations-per-launch-group for this job's shapes (device-timed)."""
+    conv, fast, fast_ft, shift = fourier_padding(job.target.shape, job.template.shape)
+    key = _key(job.score, fast, job.template.shape, precision)
+    cache = _cache_load() if use_cache else {}
+    if key in cache:
+        return int(cache[key])
+    t_rev = np.ascontiguousarray(job.template[::-1, ::-1, ::-1], dtype=np.float32)
+    m_rev = None if job.mask is None else np.ascontiguousarray(job.mask[::-1, ::-1, ::-1],
+                                                                   dtype=np.float32)
+    target = _prepare_target(job.target, tuple(fast), job.target_filter)
+    center = np.divide(np.asarray(job.template.shape) - 1, 2)
+    dev = target.device
+    best, best_rate = None, -1.0
+    for b in candidates:
+        try:
+            plan = ScanPlan(job.score, fast, job.template.shape, precision=precision, batch=b)
+        except MemoryError:
+            continue
+        if plan.plain:
+            plan.close()
+            return int(candidates[0])
+        plan.set_template(t_rev, m_rev, job.template_filter)
+        plan.set_target(target)
+        n = b * (groups + 1)
+        rots = np.resize(np.asarray(job.rotations, dtype=np.float32).reshape(-1, 3, 3), (n, 3, 3))
+        mats = torch.as_tensor(rigid_transform_matrices(rots, center), device=dev)
+        smax = torch.zeros(tuple(fast), dtype=torch.float32, device=dev)
+        sarg = torch.full(tuple(fast), -1, dtype=torch.int32, device=dev)
+        plan.run(mats[:b], 0, smax, sarg)  # warm-up group
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        plan.run(mats[b:], b, smax, sarg)
+        e1.record()
+        torch.cuda.synchronize()
+        rate = (n - b) / (e0.elapsed_time(e1) / 1000.0)
+        plan.close()
+        del smax, sarg
+        if rate > best_rate:
+            best, best_rate = b, rate
+    best = int(best if best is not None else candidates[0])
+    if use_cache:
+        cache = _cache_load()
+        cache[key] = best
+        _cache_store(cache)
+    return best
+
+
+def scan_batch(jobs: List[MatchJob], precision: str = "mixed", rotation_batch="auto",
+               use_graph: bool = True) -> List[Tuple[np.ndarray, np.ndarray]]:
+    """Run every job; returns [(scores, rotation_index)] in the reference's ``result``
+    layout (rolled by the Fourier shift and cropped to the target, "same" mode)."""
+    plans: Dict[Tuple, ScanPlan] = {}
+    out = []
+    try:
+        for job in jobs:
+            tmpl = np.asarray(job.template, dtype=np.float32)
+            conv, fast, fast_ft, shift = fourier_padding(job.target.shape, tmpl.shape)
+            has_filter = job.template_filter is not None
+            key = (job.score, tuple(fast), tmpl.shape, has_filter)
+            plan = plans.get(key)
+            if plan is None:
+                b = rotation_batch
+                if b == "auto":
+                    b = autotune_batch(job, precision=precision)
+                plan = ScanPlan(job.score, fast, tmpl.shape, precision=precision, batch=int(b))
+                if use_graph:
+                    plan.set_graph(True)
+                plans[key] = plan
+            t_rev = np.ascontiguousarray(tmpl[::-1, ::-1, ::-1])
+            m_rev = None if job.mask is None else np.ascontiguousarray(
+                np.asarray(job.mask, dtype=np.float32)[::-1, ::-1, ::-1])
+            plan.set_template(t_rev, m_rev, job.template_filter)
+            target = _prepare_target(job.target, tuple(fast), job.target_filter)
+            plan.set_target(target)
+            dev = target.device
+            smax = torch.full(tuple(fast), float(job.score_threshold), dtype=torch.float32,
+                              device=dev)
+            sarg = torch.full(tuple(fast), -1, dtype=torch.int32, device=dev)
+            center = np.divide(np.asarray(tmpl.shape) - 1, 2)
+            mats = torch.as_tensor(rigid_transform_matrices(job.rotations, center), device=dev)
+            plan.run(mats, 0, smax, sarg)
+            axis = tuple(range(3))
+            s = torch.roll(smax, shifts=shift, dims=axis)
+            r = torch.roll(sarg, shifts=shift, dims=axis)
+            s = apply_convolution_mode(s, "same", job.target.shape, tmpl.shape, conv)
+            r = apply_convolution_mode(r, "same", job.target.shape, tmpl.shape, conv)
+            out.append((s.contiguous().cpu().numpy(), r.contiguous().cpu().numpy()))
+    finally:
+        for p in plans.values():
+            p.close()
+    return out

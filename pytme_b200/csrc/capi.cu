@@ -186,6 +186,11 @@ int tm_scan_set_timing(tm_scan* plan, int enable) {
   return tmb::scan_set_timing(plan->impl, enable);
 }
 
+int tm_scan_set_graph(tm_scan* plan, int enable) {
+  TM_REQUIRE(plan, "tm_scan_set_graph: null plan");
+  return tmb::scan_set_graph(plan->impl, enable);
+}
+
 int tm_scan_get_timing(const tm_scan* plan, double* ms, int64_t* launches) {
   TM_REQUIRE(plan, "tm_scan_get_timing: null plan");
   return tmb::scan_get_timing(plan->impl, ms, launches);

@@ -591,7 +591,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 zpass_kernel(const HT* __restrict__ H, int B, int64_t rows, int n2, int h2, int R, LinePlan pm,
              const float2* __restrict__ tw2_g, float scale, const float* __restrict__ inv_den,
              int32_t first_index, float* __restrict__ state_max, int32_t* __restrict__ state_rot,
-             int64_t S) {
+             int64_t S, const int32_t* __restrict__ first_dev) {
+  if (first_dev) first_index = *first_dev;
   extern __shared__ float4 smem_raw[];
   const int m = n2 / 2;
   float2* tw2 = reinterpret_cast<float2*>(smem_raw);
@@ -688,7 +689,9 @@ zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
                  const float2* __restrict__ Hm2, int B, int64_t rows, int n2, int h2, int R,
                  LinePlan pm, const float2* __restrict__ tw2_g, float scale_t, float scale_m,
                  const double* __restrict__ stats, double eps, int32_t first_index,
-                 float* __restrict__ state_max, int32_t* __restrict__ state_rot, int64_t S) {
+                 float* __restrict__ state_max, int32_t* __restrict__ state_rot, int64_t S,
+                 const int32_t* __restrict__ first_dev) {
+  if (first_dev) first_index = *first_dev;
   extern __shared__ float4 smem_raw[];
   const int m = n2 / 2;
   float2* tw2 = reinterpret_cast<float2*>(smem_raw);
@@ -774,7 +777,8 @@ __global__ void __launch_bounds__(M1 * (256 / M1), 2)
 zpass4_kernel(const HT* __restrict__ H, int B, int64_t rows, int h2,
               const float2* __restrict__ tw2_g, float scale, const float* __restrict__ inv_den,
               int32_t first_index, float* __restrict__ state_max,
-              int32_t* __restrict__ state_rot, int64_t S) {
+              int32_t* __restrict__ state_rot, int64_t S, const int32_t* __restrict__ first_dev) {
+  if (first_dev) first_index = *first_dev;
   constexpr int M = M1 * M2;
   constexpr int N2 = 2 * M;
   constexpr int C = M2 / M1;
@@ -965,6 +969,20 @@ __global__ void inv_den_kernel(const double* __restrict__ cc1, const double* __r
   }
 }
 
+// The dynamic shared-memory limit is a property of each kernel function, shared by every
+// plan, so it is raised once to the device's opt-in maximum (launches still request only
+// their own tile size).
+static int smem_optin_max() {
+  static int v = -1;
+  if (v < 0) {
+    int dev = 0, val = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&val, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    v = val > 0 ? val : 48 * 1024;
+  }
+  return v;
+}
+
 static unsigned grid_for(int64_t n, int threads = 256, int64_t cap = 148 * 16) {
   int64_t b = ceil_div(n, threads);
   if (b < 1) b = 1;
@@ -1016,6 +1034,15 @@ struct Scan {
   size_t smem1 = 0, smem2 = 0, smem3 = 0, smem4 = 0;
   cufftHandle fwd = 0, inv = 0, tfwd = 0, tinv = 0;
   bool have_fwd = false, have_tfwd = false;
+  // CUDA-graph replay of a full launch group (see scan_set_graph)
+  bool use_graph = false;
+  cudaGraphExec_t gexec = nullptr;
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t gev_in = nullptr, gev_out = nullptr;
+  float* gkey_max = nullptr;
+  int32_t* gkey_rot = nullptr;
+  int32_t* first_dev = nullptr;     // group's first rotation index, read by the z pass
+  int32_t* graph_first = nullptr;   // == first_dev while capturing/replaying, else null
   // optional per-stage timing with CUDA events on the launching stream
   bool timing = false;
   double stage_ms[TM_NUM_STAGES] = {0};
@@ -1062,18 +1089,19 @@ static void launch_zpass_flc(Scan* s, dim3 g4, HT* H, int nb, int64_t rows, floa
   TM_DISPATCH_M(s->n2 / 2, (zpass_flc_kernel<HT, MM><<<g4, kThreads, s->smem4, st>>>(
                                H, s->Hm, s->Hm2, nb, rows, s->n2, s->h2, s->R4, s->pm, s->tw2,
                                out_scale, out_scale, stats, 1.1920928955078125e-07, first,
-                               state_max, state_rot, s->S)));
+                               state_max, state_rot, s->S, s->graph_first)));
 }
 
 static void set_zpass_attrs(int m, int smem) {
+  (void)smem;
   TM_DISPATCH_M(m, (cudaFuncSetAttribute(zpass_flc_kernel<float2, MM>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max()),
                     cudaFuncSetAttribute(zpass_flc_kernel<__half2, MM>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem)));
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max())));
   TM_DISPATCH_M(m, (cudaFuncSetAttribute(zpass_kernel<float2, MM>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max()),
                     cudaFuncSetAttribute(zpass_kernel<__half2, MM>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem)));
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max())));
 }
 
 #define TM_DISPATCH_4STEP(m, CALL)                                  \
@@ -1101,16 +1129,15 @@ static void launch_zpass4(Scan* s, HT* H, int nb, int64_t rows, float out_scale,
     constexpr int RW = 256 / A1;
     dim3 g(ceil_div(rows, RW));
     zpass4_kernel<HT, A1, A2><<<g, A1 * RW, zpass4_smem<A1, A2, HT>(), st>>>(
-        H, nb, rows, s->h2, s->tw2, out_scale, s->inv_den, first, state_max, state_rot, s->S);
+        H, nb, rows, s->h2, s->tw2, out_scale, s->inv_den, first, state_max, state_rot, s->S,
+        s->graph_first);
   }));
 }
 
 static void set_zpass4_attrs(int m) {
   TM_DISPATCH_4STEP(m, ({
-    cudaFuncSetAttribute(zpass4_kernel<float2, A1, A2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)zpass4_smem<A1, A2, float2>());
-    cudaFuncSetAttribute(zpass4_kernel<__half2, A1, A2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)zpass4_smem<A1, A2, __half2>());
+    cudaFuncSetAttribute(zpass4_kernel<float2, A1, A2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
+    cudaFuncSetAttribute(zpass4_kernel<__half2, A1, A2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
   }));
 }
 
@@ -1123,7 +1150,7 @@ static void launch_zpass(Scan* s, dim3 g4, HT* H, int nb, int64_t rows, float ou
   }
   TM_DISPATCH_M(s->n2 / 2, (zpass_kernel<HT, MM><<<g4, kThreads, s->smem4, st>>>(
                                H, nb, rows, s->n2, s->h2, s->R4, s->pm, s->tw2, out_scale,
-                               s->inv_den, first, state_max, state_rot, s->S)));
+                               s->inv_den, first, state_max, state_rot, s->S, s->graph_first)));
 }
 
 // ---- launch helpers for the register-resident kernels
@@ -1131,13 +1158,13 @@ template <int N>
 static void set_reg_attrs(size_t zy_smem) {
   constexpr int W = reg_lines<N>();
   const int sm = (int)reg_smem_bytes<N>(0, 0, 0, false);
-  cudaFuncSetAttribute(xpass_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(xpass_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(ypass_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ypass_smem_bytes<N, float2>());
-  cudaFuncSetAttribute(ypass_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ypass_smem_bytes<N, __half2>());
-  cudaFuncSetAttribute(tmpl_zy_reg_kernel<N, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zy_smem);
-  cudaFuncSetAttribute(xpass_flc_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  cudaFuncSetAttribute(xpass_flc_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaFuncSetAttribute(xpass_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
+  cudaFuncSetAttribute(xpass_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
+  cudaFuncSetAttribute(ypass_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
+  cudaFuncSetAttribute(ypass_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
+  cudaFuncSetAttribute(tmpl_zy_reg_kernel<N, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
+  cudaFuncSetAttribute(xpass_flc_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
+  cudaFuncSetAttribute(xpass_flc_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
 }
 
 static void set_reg_attrs_n(int n, size_t zy_smem) {
@@ -1246,6 +1273,10 @@ static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 static void destroy(Scan* s) {
   if (!s) return;
+  if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  if (s->gstream) cudaStreamDestroy(s->gstream);
+  if (s->gev_in) cudaEventDestroy(s->gev_in);
+  if (s->gev_out) cudaEventDestroy(s->gev_out);
   if (s->have_events)
     for (auto& e : s->ev) cudaEventDestroy(e);
   if (s->have_fwd) { cufftDestroy(s->fwd); cufftDestroy(s->inv); }
@@ -1314,6 +1345,7 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
   size_t o_mk = take(sizeof(float) * s->T);
   size_t o_tf = take(sizeof(float) * s->TS);
   size_t o_mat = take(sizeof(float) * 16 * B);
+  size_t o_first = take(sizeof(int32_t) * 4);
   size_t o_rt = take(sizeof(float) * s->T * B);
   size_t o_rm = take(sizeof(float) * s->T * B);
   size_t o_st = take(stats_workspace_bytes(B));
@@ -1356,6 +1388,7 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
   s->mask = reinterpret_cast<float*>(b8 + o_mk);
   s->tfilter = reinterpret_cast<float*>(b8 + o_tf);
   s->mat = reinterpret_cast<float*>(b8 + o_mat);
+  s->first_dev = reinterpret_cast<int32_t*>(b8 + o_first);
   s->rot_t = reinterpret_cast<float*>(b8 + o_rt);
   s->rot_m = reinterpret_cast<float*>(b8 + o_rm);
   s->stats_ws = reinterpret_cast<double*>(b8 + o_st);
@@ -1402,11 +1435,11 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
       destroy(s);
       return TM_E_UNSUPPORTED;
     }
-    cudaFuncSetAttribute(tmpl_zy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem1);
-    cudaFuncSetAttribute(xpass_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem2);
-    cudaFuncSetAttribute(xpass_kernel<__half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem2);
-    cudaFuncSetAttribute(ypass_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem3);
-    cudaFuncSetAttribute(ypass_kernel<__half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem3);
+    cudaFuncSetAttribute(tmpl_zy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
+    cudaFuncSetAttribute(xpass_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
+    cudaFuncSetAttribute(xpass_kernel<__half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
+    cudaFuncSetAttribute(ypass_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
+    cudaFuncSetAttribute(ypass_kernel<__half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
     set_zpass_attrs(s->n2 / 2, (int)s->smem4);
     set_zpass4_attrs(s->n2 / 2);
     s->reg0 = reg_supported(s->n0) && !getenv("PYTME_B200_GENERIC_FFT");
@@ -1614,11 +1647,86 @@ static int run_plain(Scan* s, int n, int32_t first_index, float* state_max, int3
   return TM_OK;
 }
 
+__global__ void set_first_kernel(int32_t* p, int32_t v) { *p = v; }
+
+// One launch group: template preparation and the four passes for nb rotations whose
+// matrices are already in s->mat.
+static int launch_group(Scan* s, int nb, double hs, float out_scale, int32_t first,
+                        float* state_max, int32_t* state_rot, cudaStream_t stream) {
+  StageTimer tmr(s, stream);
+  tmr.begin();
+  TM_TRY(prepare_templates(s, nb, stream));
+  tmr.end(TM_STAGE_PREPARE);
+  const int64_t rows = (int64_t)s->n0 * s->n1;
+  dim3 g4(ceil_div(rows, s->R4));
+  if (s->half) {
+    __half2* H = static_cast<__half2*>(s->H);
+    TM_TRY(launch_template_x_y<__half2>(s, nb, (float)hs, H, tmr, stream));
+    tmr.begin();
+    if (s->d.score == TM_SCORE_FLC)
+      launch_zpass_flc<__half2>(s, g4, H, nb, rows, out_scale, first, state_max, state_rot, stream);
+    else
+      launch_zpass<__half2>(s, g4, H, nb, rows, out_scale, first, state_max, state_rot, stream);
+    TM_TRY(check_launch("z pass"));
+    tmr.end(TM_STAGE_ZPASS);
+  } else {
+    float2* H = static_cast<float2*>(s->H);
+    TM_TRY(launch_template_x_y<float2>(s, nb, (float)hs, H, tmr, stream));
+    tmr.begin();
+    if (s->d.score == TM_SCORE_FLC)
+      launch_zpass_flc<float2>(s, g4, H, nb, rows, out_scale, first, state_max, state_rot, stream);
+    else
+      launch_zpass<float2>(s, g4, H, nb, rows, out_scale, first, state_max, state_rot, stream);
+    TM_TRY(check_launch("z pass"));
+    tmr.end(TM_STAGE_ZPASS);
+  }
+  return TM_OK;
+}
+
+// Full groups replay one captured graph: the group's matrices are copied into s->mat
+// and its first rotation index into s->first_dev before each replay, on the caller's
+// stream; the graph runs on a plan-owned stream ordered after and before the caller's.
+static int replay_group(Scan* s, double hs, float out_scale, int32_t first, float* state_max,
+                        int32_t* state_rot, cudaStream_t stream) {
+  set_first_kernel<<<1, 1, 0, stream>>>(s->first_dev, first);
+  TM_TRY(check_launch("set_first_kernel"));
+  if (!s->gstream) {
+    TM_TRY(cuda_status(cudaStreamCreateWithFlags(&s->gstream, cudaStreamNonBlocking), "graph stream"));
+    TM_TRY(cuda_status(cudaEventCreateWithFlags(&s->gev_in, cudaEventDisableTiming), "graph event"));
+    TM_TRY(cuda_status(cudaEventCreateWithFlags(&s->gev_out, cudaEventDisableTiming), "graph event"));
+  }
+  TM_TRY(cuda_status(cudaEventRecord(s->gev_in, stream), "graph event"));
+  TM_TRY(cuda_status(cudaStreamWaitEvent(s->gstream, s->gev_in, 0), "graph wait"));
+  if (!s->gexec || s->gkey_max != state_max || s->gkey_rot != state_rot) {
+    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    cudaGraph_t graph = nullptr;
+    s->graph_first = s->first_dev;
+    const bool timing = s->timing;
+    s->timing = false;
+    TM_TRY(cuda_status(cudaStreamBeginCapture(s->gstream, cudaStreamCaptureModeThreadLocal),
+                       "begin capture"));
+    int st = launch_group(s, s->B, hs, out_scale, first, state_max, state_rot, s->gstream);
+    cudaError_t e = cudaStreamEndCapture(s->gstream, &graph);
+    s->timing = timing;
+    s->graph_first = nullptr;
+    if (st != TM_OK) { if (graph) cudaGraphDestroy(graph); return st; }
+    TM_TRY(cuda_status(e, "end capture"));
+    e = cudaGraphInstantiate(&s->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    TM_TRY(cuda_status(e, "graph instantiate"));
+    s->gkey_max = state_max;
+    s->gkey_rot = state_rot;
+  }
+  TM_TRY(cuda_status(cudaGraphLaunch(s->gexec, s->gstream), "graph launch"));
+  TM_TRY(cuda_status(cudaEventRecord(s->gev_out, s->gstream), "graph event"));
+  return cuda_status(cudaStreamWaitEvent(stream, s->gev_out, 0), "graph wait");
+}
+
 static int run_fused(Scan* s, int n, int32_t first_index, float* state_max, int32_t* state_rot,
                      const float* matrices, cudaStream_t stream) {
   const double Nd = (double)s->N;
   // H holds the product after two inverse passes scaled by hs; the z pass divides by
-  // N * hs. hs keeps half2 storage in range (see the precision note in the header).
+  // N * hs. hs keeps half2 storage in range.
   double hs = 1.0;
   if (s->half) hs = 1.0 / (sqrt(Nd) * sqrt((double)s->n0) * sqrt(std::max(1.0, s->mask_sum)));
   const float out_scale = (float)(1.0 / (Nd * hs));
@@ -1626,34 +1734,20 @@ static int run_fused(Scan* s, int n, int32_t first_index, float* state_max, int3
     const int nb = std::min(s->B, n - g0);
     cudaMemcpyAsync(s->mat, matrices + (int64_t)g0 * 16, sizeof(float) * 16 * nb,
                     cudaMemcpyDeviceToDevice, stream);
-    StageTimer tmr(s, stream);
-    tmr.begin();
-    TM_TRY(prepare_templates(s, nb, stream));
-    tmr.end(TM_STAGE_PREPARE);
-    const int64_t rows = (int64_t)s->n0 * s->n1;
-    dim3 g4(ceil_div(rows, s->R4));
-    if (s->half) {
-      __half2* H = static_cast<__half2*>(s->H);
-      TM_TRY(launch_template_x_y<__half2>(s, nb, (float)hs, H, tmr, stream));
-      tmr.begin();
-      if (s->d.score == TM_SCORE_FLC)
-        launch_zpass_flc<__half2>(s, g4, H, nb, rows, out_scale, first_index + g0, state_max, state_rot, stream);
-      else
-        launch_zpass<__half2>(s, g4, H, nb, rows, out_scale, first_index + g0, state_max, state_rot, stream);
-      TM_TRY(check_launch("zpass_kernel"));
-      tmr.end(TM_STAGE_ZPASS);
+    if (s->use_graph && nb == s->B && !s->timing) {
+      TM_TRY(replay_group(s, hs, out_scale, first_index + g0, state_max, state_rot, stream));
     } else {
-      float2* H = static_cast<float2*>(s->H);
-      TM_TRY(launch_template_x_y<float2>(s, nb, (float)hs, H, tmr, stream));
-      tmr.begin();
-      if (s->d.score == TM_SCORE_FLC)
-        launch_zpass_flc<float2>(s, g4, H, nb, rows, out_scale, first_index + g0, state_max, state_rot, stream);
-      else
-        launch_zpass<float2>(s, g4, H, nb, rows, out_scale, first_index + g0, state_max, state_rot, stream);
-      TM_TRY(check_launch("zpass_kernel"));
-      tmr.end(TM_STAGE_ZPASS);
+      TM_TRY(launch_group(s, nb, hs, out_scale, first_index + g0, state_max, state_rot, stream));
     }
   }
+  return TM_OK;
+}
+
+int scan_set_graph(Scan* s, int enable) {
+  TM_REQUIRE(s, "scan_set_graph: null plan");
+  if (!s->fused) enable = 0;  // the plain path is one rotation at a time by design
+  s->use_graph = enable != 0;
+  if (!s->use_graph && s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
   return TM_OK;
 }
 
@@ -1733,7 +1827,7 @@ int line_fft_test(const void* x, void* y, int n, int lines, int dir, cudaStream_
   TM_TRY(cuda_status(cudaMalloc(&tw, sizeof(float2) * n), "line_fft_test: alloc"));
   cudaMemcpy(tw, tv.data(), sizeof(float2) * n, cudaMemcpyHostToDevice);
   size_t smem = sizeof(float2) * (n + (size_t)n * lines);
-  cudaFuncSetAttribute(line_fft_test_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(line_fft_test_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
   line_fft_test_kernel<<<1, kThreads, smem, stream>>>((const float2*)x, (float2*)y, n, lines, p, tw, dir);
   int st = check_launch("line_fft_test_kernel");
   cudaStreamSynchronize(stream);

@@ -21,6 +21,7 @@ int scan_set_target(Scan* s, const float* target, cudaStream_t stream);
 int scan_run(Scan* s, const float* matrices, int n, int32_t first_index, float* state_max,
              int32_t* state_rot, cudaStream_t stream);
 int scan_set_timing(Scan* s, int enable);
+int scan_set_graph(Scan* s, int enable);
 int scan_get_timing(const Scan* s, double* ms, int64_t* launches);
 int64_t scan_stage_bytes(const Scan* s, int stage, int nb);
 int line_fft_test(const void* x, void* y, int n, int lines, int dir, cudaStream_t stream);

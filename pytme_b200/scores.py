@@ -124,6 +124,10 @@ class ScanPlan:
                                   N.ptr(max_scores), N.ptr(argmax), N.stream_ptr(stream)),
                 "tm_scan_run")
 
+    def set_graph(self, enable: bool = True):
+        """Replay full launch groups from one captured CUDA graph."""
+        N.check(N.lib.tm_scan_set_graph(self._h, int(bool(enable))), "tm_scan_set_graph")
+
     def set_timing(self, enable: bool = True):
         """Bracket each fused-path stage with CUDA events (resets the counters)."""
         N.check(N.lib.tm_scan_set_timing(self._h, int(bool(enable))), "tm_scan_set_timing")

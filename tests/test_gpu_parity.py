@@ -340,3 +340,35 @@ def test_xy_lengths(torch_cuda, shape):
     r = _scan("FLCSphericalMask", target, tmpl, mask, rots, precision="fp32", batch=3)
     ref = O.scan(target, tmpl, rots, "FLCSphericalMask", template_mask=mask)
     assert np.abs(r[0] - ref["scores"]).max() <= TOL
+
+
+def test_scan_batch_uneven_jobs_and_graph_replay(torch_cuda, tmp_path, monkeypatch):
+    """Uneven (tomogram, template) jobs through scan_batch with per-job CTF x wedge
+    filters, autotuned batch and CUDA-graph replay, against per-job oracle scans; graph
+    replay must give bit-identical maps to direct launches."""
+    from pytme_b200 import synthetic as syn
+    from pytme_b200.batch import MatchJob, scan_batch
+    from pytme_b200.filters import Compose, CTFReconstructed, WedgeReconstructed
+
+    monkeypatch.setenv("PYTME_B200_CACHE", str(tmp_path / "autotune.json"))
+    rng = np.random.default_rng(31)
+    jobs = []
+    for shape, t, defocus, wedge in (((64, 64, 48), 12, 15000, 50), ((32, 64, 40), 8, 30000, 60),
+                                     ((64, 64, 48), 12, 45000, 65)):
+        tmpl = syn.blob_template(t, rng, radius=t / 4, sigma=1.2)
+        mask = syn.spherical_mask((t,) * 3, t / 2, center=((t - 1) / 2,) * 3)
+        target, _, _ = syn.make_tomogram(shape, tmpl, 3, rng, scale=0.5)
+        w = WedgeReconstructed(angles=(wedge, wedge), opening_axis=2, tilt_axis=0)
+        ctf = CTFReconstructed(defocus_x=defocus, sampling_rate=6.8)
+        tf = Compose([w, ctf])(shape=tmpl.shape, return_real_fourier=True)["data"]
+        jobs.append(MatchJob(target=target, template=tmpl, mask=mask,
+                             rotations=syn.random_rotation_matrices(20, rng),
+                             template_filter=tf))
+    res = scan_batch(jobs, precision="fp32", rotation_batch="auto", use_graph=True)
+    direct = scan_batch(jobs, precision="fp32", rotation_batch=8, use_graph=False)
+    graph8 = scan_batch(jobs, precision="fp32", rotation_batch=8, use_graph=True)
+    for job, (s, r), (s2, r2), (s3, r3) in zip(jobs, res, direct, graph8):
+        ref = O.scan(job.target, job.template, job.rotations, "FLCSphericalMask",
+                     template_mask=job.mask, template_filter=job.template_filter)
+        assert np.abs(s - ref["scores"]).max() <= TOL
+        assert np.array_equal(s2, s3) and np.array_equal(r2, r3)
