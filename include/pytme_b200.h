@@ -98,6 +98,13 @@ int tm_fft_plan_create(int ndim, const int* shape, int batch, int double_precisi
 int tm_fft_plan_destroy(tm_fft_plan* plan);
 int tm_fft_r2c(tm_fft_plan* plan, const void* in, void* out, void* stream);
 int tm_fft_c2r(tm_fft_plan* plan, void* in, void* out, double scale, void* stream);
+/* Template filter at template shape (_apply_filter_subset of _create_filter_func,
+ * tme/matching_scores.py:90-135): x = irfftn(rfftn(x) * filter) in place for every
+ * batch item of a single-precision plan. `filter` holds one real value per rfft
+ * element of one item and is shared by all items; `spectrum` holds the plan's
+ * complex output (batch x rfft elements). */
+int tm_fft_filter(tm_fft_plan* plan, float* x, void* spectrum, const float* filter,
+                  void* stream);
 
 /* ---- rotation scan: the per-rotation loops of corr_scoring
  * (tme/matching_scores.py:491-626) and flc_scoring (:629-759) with the
@@ -203,6 +210,57 @@ int tm_find_candidate_indices(const int64_t* coords, int n, int64_t min_distance
 #define TM_NOALLOC_MAX_POINTS 65536
 int tm_find_candidate_indices_noalloc(const int64_t* coords, int n, int64_t min_distance,
                                       int32_t* out_idx, int32_t* out_count, void* stream);
+
+/* ---- local refinement of candidate peaks: the FLC of flc_scoring
+ * (tme/matching_scores.py:629-759) at one pose per peak and its adjoint. This
+ * replaces the derivative-free score of tme/matching_optimization.py:54-277 and
+ * 488-548, whose optimize_match (:1143-1312) drives scipy.optimize.
+ *
+ * Peak p: box corner corners[3p..] (target voxel of template voxel 0), rotation
+ * rot[9p..] (row-major R, the matrix of the scan's rotation set) about the template
+ * centre (t-1)/2, shift shifts[3p..] in voxels in the target frame. Template voxel o
+ * samples the template and mask at R^T (o - c - s) + c (order 1, zero unless every
+ * coordinate is inside [0, t-1]). The score is computed from the filtered template
+ * when tmpl_filtered (n_peaks x t^3, from tm_refine_rotate + tm_fft_filter) is
+ * given, else from the rotated template directly; eps is norm_scores' epsilon
+ * (tme/backends/npfftw_backend.py:537-587). Sums (n_peaks x 6 doubles: sum M,
+ * M T, M T^2, M T f, M f, M f^2) are what the backward pass needs. */
+typedef struct {
+  const float* tmpl;     /* t^3 template (not reversed) */
+  const float* mask;     /* t^3 mask */
+  int template_shape[3];
+  const float* target;   /* target volume (already filtered) */
+  int target_shape[3];
+  float target_outside;  /* value of the target outside its bounds (0 for the raw
+                            target; minus the subtracted mean for a centred one) */
+  const float* rot;      /* n_peaks x 9 */
+  const float* shifts;   /* n_peaks x 3 */
+  const int32_t* corners;/* n_peaks x 3 */
+  int n_peaks;
+  double eps;
+} tm_refine_desc;
+
+/* R = Rz(a2) Ry(a1) Rz(a0) from zyz angles in degrees (euler_to_rotationmatrix,
+ * tme/rotations.py:171-196, SciPy's extrinsic "zyz"), and when drot is not NULL
+ * dR/da_k per degree (n x 3 x 9). */
+int tm_euler_zyz(const float* angles, int n, float* rot, float* drot, void* stream);
+/* Rotated template for every peak (n_peaks x t^3), the input of tm_fft_filter. */
+int tm_refine_rotate(const tm_refine_desc* d, float* tmpl_rot, void* stream);
+int tm_refine_forward(const tm_refine_desc* d, const float* tmpl_filtered, double* sums,
+                      float* scores, void* stream);
+/* Filtered path, first half of the backward: dS/d(filtered template), n_peaks x t^3.
+ * tm_fft_filter of it (the filter is self-adjoint) gives grad_rotated below. */
+int tm_refine_grad_filtered(const tm_refine_desc* d, const float* tmpl_filtered,
+                            const double* sums, const float* grad_scores,
+                            float* grad_filtered, void* stream);
+/* Pose and template gradients of sum_p grad_scores[p] * S_p. tmpl_filtered and
+ * grad_rotated are both NULL (unfiltered) or both given. Outputs may be NULL:
+ * grad_rot n x 9, grad_shift n x 3, grad_angles n x 3 (needs drot), grad_tmpl t^3 is
+ * ACCUMULATED into (zero it first). */
+int tm_refine_backward(const tm_refine_desc* d, const float* tmpl_filtered,
+                       const float* grad_rotated, const double* sums, const float* grad_scores,
+                       const float* drot, double* grad_rot, double* grad_shift,
+                       double* grad_angles, float* grad_tmpl, void* stream);
 
 /* Diagnostic: `lines` complex FFTs of length n (dir -1 forward, +1 unnormalised
  * inverse) with the shared-memory line-FFT routine of the fused scan.

@@ -40,6 +40,9 @@ __all__ = [
     "find_candidate_indices",
     "topk_indices",
     "peak_caller_maximum_filter",
+    "euler_zyz_to_matrix",
+    "score_box_corner",
+    "refine_flc_score",
 ]
 
 
@@ -466,3 +469,71 @@ def peak_caller_maximum_filter(scores: np.ndarray, num_peaks: int = 1000,
     top, *_ = topk_indices(s, top_n)
     final = order[top]
     return positions[final], all_scores[final]
+
+
+# --------------------------------------------------------------------------- refinement
+def euler_zyz_to_matrix(angles) -> np.ndarray:
+    """``euler_to_rotationmatrix`` (tme/rotations.py:171-196): SciPy's extrinsic "zyz"
+    sequence in degrees, R = Rz(angles[2]) . Ry(angles[1]) . Rz(angles[0]); float64
+    here (the reference casts to float32)."""
+    from scipy.spatial.transform import Rotation
+
+    return Rotation.from_euler("zyz", np.asarray(angles, dtype=np.float64),
+                               degrees=True).as_matrix()
+
+
+def score_box_corner(position, target_shape, template_shape) -> np.ndarray:
+    """Target voxel of template voxel 0 for the score-map voxel ``position`` of a
+    "same"-mode ``MaxScoreOverRotations.result`` (target at least as large as the
+    template on every axis): the scan correlates with the reversed template, so the
+    box starts t - 1 before the raw correlation index, and ``result`` rolls by
+    ``1 - t//2 - t%2`` (tme/matching_data.py:510-512) and crops from
+    (min(conv, fast) - T) // 2 (tme/matching_utils.py:469-524)."""
+    conv, fast, _, _ = fourier_padding(target_shape, template_shape)
+    start = [(min(c, f) - n) // 2 for c, f, n in zip(conv, fast, target_shape)]
+    return (np.asarray(position, dtype=np.int64) + np.asarray(start)
+            - np.asarray(template_shape) // 2)
+
+
+def refine_flc_score(target, template, mask, corner, rotation, shift=(0.0, 0.0, 0.0),
+                     template_filter=None, dtype=np.float64) -> float:
+    """The FLC score of ``flc_scoring`` (tme/matching_scores.py:629-759) at one pose,
+    written in real space. The template and mask are rotated by ``rotation`` about the
+    template centre (t - 1)/2 with order-1 constant-mode interpolation
+    (``_rigid_transform``, tme/backends/npfftw_backend.py:357-388) and moved by the
+    sub-voxel ``shift`` in the target frame, so template voxel o samples
+    R^T (o - c - shift) + c. The template filter is applied at template shape
+    (``_apply_filter_subset``, tme/matching_scores.py:131-135), the filtered template is
+    normalised under the rotated mask (tme/matching_utils.py:61-99), correlated with the
+    target box starting at ``corner`` (zero outside the target) and divided by the
+    masked local standard deviation times n_obs (``norm_scores``,
+    tme/backends/npfftw_backend.py:537-587, eps = float32 eps). At shift 0 this is the
+    exhaustive FLC map value at the score-map voxel whose ``score_box_corner`` is
+    ``corner``, because correlating with the reversed, rotated template equals
+    correlating the rotated template in real space."""
+    template = np.asarray(template, dtype=dtype)
+    mask = np.asarray(mask, dtype=dtype)
+    t = np.asarray(template.shape)
+    c = (t - 1) / 2.0
+    rt = np.asarray(rotation, dtype=np.float64).T
+    offset = c - rt @ (c + np.asarray(shift, dtype=np.float64))
+    tr = affine_transform(template, rt, offset=offset, order=1, mode="constant",
+                          prefilter=False)
+    mr = affine_transform(mask, rt, offset=offset, order=1, mode="constant", prefilter=False)
+    if template_filter is not None:
+        tr = apply_template_filter(tr, np.asarray(template_filter, dtype=dtype))
+    box = np.zeros(template.shape, dtype=dtype)
+    corner = np.asarray(corner, dtype=np.int64)
+    src = tuple(slice(max(k, 0), min(k + n, m)) for k, n, m in zip(corner, t, target.shape))
+    dst = tuple(slice(s.start - k, s.stop - k) for s, k in zip(src, corner))
+    if all(s.stop > s.start for s in src):
+        box[dst] = np.asarray(target, dtype=dtype)[src]
+    n_obs = np.sum(mr)
+    tn = normalize_template(tr, mr, n_obs)
+    numerator = np.sum(tn * box)
+    exp_sq = np.sum(box * box * mr)
+    sq_exp = np.sum(box * mr)
+    eps = np.finfo(np.float32).eps
+    out = norm_scores(np.asarray([numerator]), np.asarray([exp_sq]), np.asarray([sq_exp]),
+                      n_obs, eps, np.zeros(1, dtype=dtype))
+    return float(out[0])

@@ -40,7 +40,9 @@ EXPORTED = (
     "tm_scan_get_timing",
     "tm_scan_stage_bytes", "tm_max_filter_peaks",
     "tm_find_candidate_indices_workspace", "tm_find_candidate_indices",
-    "tm_find_candidate_indices_noalloc", "tm_line_fft_test",
+    "tm_find_candidate_indices_noalloc", "tm_line_fft_test", "tm_fft_filter",
+    "tm_euler_zyz", "tm_refine_rotate", "tm_refine_forward", "tm_refine_grad_filtered",
+    "tm_refine_backward",
 )
 
 
@@ -53,6 +55,22 @@ class ScanDesc(Structure):
         ("batch", c_int),
         ("plain", c_int),
         ("has_template_filter", c_int),
+    ]
+
+
+class RefineDesc(Structure):
+    _fields_ = [
+        ("tmpl", c_void_p),
+        ("mask", c_void_p),
+        ("template_shape", c_int * 3),
+        ("target", c_void_p),
+        ("target_shape", c_int * 3),
+        ("target_outside", c_float),
+        ("rot", c_void_p),
+        ("shifts", c_void_p),
+        ("corners", c_void_p),
+        ("n_peaks", c_int),
+        ("eps", c_double),
     ]
 
 
@@ -95,6 +113,13 @@ def _load():
         "tm_find_candidate_indices": (c_int, [vp, c_int, c_int64, i32p, i32p, vp, vp]),
         "tm_find_candidate_indices_noalloc": (c_int, [vp, c_int, c_int64, i32p, i32p, vp]),
         "tm_line_fft_test": (c_int, [vp, vp, c_int, c_int, c_int, vp]),
+        "tm_fft_filter": (c_int, [vp, f32p, vp, f32p, vp]),
+        "tm_euler_zyz": (c_int, [f32p, c_int, f32p, f32p, vp]),
+        "tm_refine_rotate": (c_int, [POINTER(RefineDesc), f32p, vp]),
+        "tm_refine_forward": (c_int, [POINTER(RefineDesc), f32p, vp, f32p, vp]),
+        "tm_refine_grad_filtered": (c_int, [POINTER(RefineDesc), f32p, vp, f32p, f32p, vp]),
+        "tm_refine_backward": (c_int, [POINTER(RefineDesc), f32p, f32p, vp, f32p, f32p, vp, vp,
+                                       vp, f32p, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

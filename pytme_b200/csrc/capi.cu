@@ -3,6 +3,7 @@
 #include "common.cuh"
 #include "ops.cuh"
 #include "peaks.cuh"
+#include "refine.cuh"
 #include "scan.cuh"
 
 #include <cufft.h>
@@ -13,6 +14,9 @@ struct tm_fft_plan {
   cufftHandle fwd = 0, inv = 0;
   bool dbl = false;
   int64_t n_real = 0;   // elements per real array (all batches)
+  int64_t n_item = 0;   // real elements per batch item
+  int64_t n_ft = 0;     // complex elements per batch item
+  int batch = 1;
 };
 
 struct tm_scan {
@@ -20,6 +24,24 @@ struct tm_scan {
 };
 
 static cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
+
+static tmb::RefineArgs refine_args(const tm_refine_desc* d) {
+  tmb::RefineArgs a;
+  a.tmpl = d->tmpl;
+  a.mask = d->mask;
+  a.rot = d->rot;
+  a.shifts = d->shifts;
+  a.corners = d->corners;
+  a.P = d->n_peaks;
+  a.target = d->target;
+  a.eps = d->eps;
+  a.outside = d->target_outside;
+  for (int i = 0; i < 3; ++i) {
+    a.t[i] = d->template_shape[i];
+    a.n[i] = d->target_shape[i];
+  }
+  return a;
+}
 
 extern "C" {
 
@@ -88,6 +110,9 @@ int tm_fft_plan_create(int ndim, const int* shape, int batch, int double_precisi
   tm_fft_plan* p = new tm_fft_plan();
   p->dbl = double_precision != 0;
   p->n_real = nr * batch;
+  p->n_item = nr;
+  p->n_ft = nr / n[ndim - 1] * (n[ndim - 1] / 2 + 1);
+  p->batch = batch;
   cufftResult r = cufftPlanMany(&p->fwd, ndim, n, nullptr, 1, 0, nullptr, 1, 0,
                                 p->dbl ? CUFFT_D2Z : CUFFT_R2C, batch);
   if (r == CUFFT_SUCCESS)
@@ -216,6 +241,49 @@ int tm_find_candidate_indices(const int64_t* coords, int n, int64_t min_distance
 int tm_line_fft_test(const void* x, void* y, int n, int lines, int dir, void* stream) {
   TM_REQUIRE(x && y, "tm_line_fft_test: null pointer");
   return tmb::line_fft_test(x, y, n, lines, dir, S(stream));
+}
+
+
+// ------------------------------------------------------------------ FFT filter
+int tm_fft_filter(tm_fft_plan* p, float* x, void* spectrum, const float* filter, void* stream) {
+  TM_REQUIRE(p && x && spectrum && filter, "tm_fft_filter: null pointer");
+  TM_REQUIRE(!p->dbl, "tm_fft_filter: single-precision plans only");
+  TM_TRY(tm_fft_r2c(p, x, spectrum, stream));
+  TM_TRY(tmb::apply_real_filter(spectrum, filter, p->n_ft, p->batch, S(stream)));
+  return tm_fft_c2r(p, spectrum, x, 1.0 / (double)p->n_item, stream);
+}
+
+// ------------------------------------------------------------------ refinement
+int tm_euler_zyz(const float* angles, int n, float* rot, float* drot, void* stream) {
+  return tmb::euler_zyz(angles, n, rot, drot, S(stream));
+}
+
+int tm_refine_rotate(const tm_refine_desc* d, float* tmpl_rot, void* stream) {
+  TM_REQUIRE(d, "tm_refine_rotate: null descriptor");
+  return tmb::refine_rotate(refine_args(d), tmpl_rot, S(stream));
+}
+
+int tm_refine_forward(const tm_refine_desc* d, const float* tmpl_filtered, double* sums,
+                      float* scores, void* stream) {
+  TM_REQUIRE(d, "tm_refine_forward: null descriptor");
+  return tmb::refine_forward(refine_args(d), tmpl_filtered, sums, scores, S(stream));
+}
+
+int tm_refine_grad_filtered(const tm_refine_desc* d, const float* tmpl_filtered,
+                            const double* sums, const float* grad_scores, float* grad_filtered,
+                            void* stream) {
+  TM_REQUIRE(d, "tm_refine_grad_filtered: null descriptor");
+  return tmb::refine_grad_filtered(refine_args(d), tmpl_filtered, sums, grad_scores,
+                                   grad_filtered, S(stream));
+}
+
+int tm_refine_backward(const tm_refine_desc* d, const float* tmpl_filtered,
+                       const float* grad_rotated, const double* sums, const float* grad_scores,
+                       const float* drot, double* grad_rot, double* grad_shift,
+                       double* grad_angles, float* grad_tmpl, void* stream) {
+  TM_REQUIRE(d, "tm_refine_backward: null descriptor");
+  return tmb::refine_backward(refine_args(d), tmpl_filtered, grad_rotated, sums, grad_scores,
+                              drot, grad_rot, grad_shift, grad_angles, grad_tmpl, S(stream));
 }
 
 }  // extern "C"

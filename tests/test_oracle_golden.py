@@ -88,3 +88,28 @@ def test_kat_box_case_fp32(golden):
         m = r["scores"]
         assert tuple(np.unravel_index(np.argmax(m), m.shape)) == tuple(g[f"{score}_0_argmax"])
         assert abs(float(m.max()) - float(g[f"{score}_0_max"])) < 1e-5
+
+
+def test_refine_score_matches_reference_flc_map(golden):
+    """The real-space refinement score at the scan's own pose reproduces the reference's
+    FP64 FLC map (filtered, arbitrary mask) at interior score-map voxels."""
+    g = golden("flc_filt.npz")
+    tgt, tmpl, mask = g["target"], g["template"], g["mask"]
+    _, fast, _, _ = O.fourier_padding(tgt.shape, tmpl.shape)
+    tg = O.apply_target_filter(tgt.astype(np.float64), fast,
+                               g["target_filter"].astype(np.float64))
+    t = np.asarray(tmpl.shape)
+    rng = np.random.default_rng(0)
+    checked = 0
+    for _ in range(40):
+        x = np.array([rng.integers(t[i] // 2 + 1, tgt.shape[i] - t[i] // 2 - 1)
+                      for i in range(3)])
+        r = int(g["rot64"][tuple(x)])
+        if r < 0:
+            continue
+        k = O.score_box_corner(x, tgt.shape, tmpl.shape)
+        s = O.refine_flc_score(tg, tmpl, mask, k, g["rotations"][r].astype(np.float64),
+                               template_filter=g["template_filter"])
+        assert abs(s - float(g["scores64"][tuple(x)])) < 1e-6
+        checked += 1
+    assert checked >= 20
