@@ -52,15 +52,35 @@ __device__ __forceinline__ Box make_box(int t0, int t1, int t2) {
   return b;
 }
 
-// d = o - c - s and u = R^T d + c for template voxel v; R row-major.
-__device__ __forceinline__ void pose_coords(const Box& b, const float* R, const float* s, int v,
-                                            int o[3], float d[3], float u[3]) {
-  o[2] = v % b.t2;
-  o[1] = (v / b.t2) % b.t1;
-  o[0] = v / (b.t1 * b.t2);
-  d[0] = (float)o[0] - b.c0 - s[0];
-  d[1] = (float)o[1] - b.c1 - s[1];
-  d[2] = (float)o[2] - b.c2 - s[2];
+// Template voxel (o0, o1, o2) of v = start, start + stride, ...: one division set at
+// the start, then carries instead of a division per voxel.
+struct Walker {
+  int o0, o1, o2, d0, d1, d2;
+  __device__ __forceinline__ void init(const Box& b, int v, int stride) {
+    o2 = v % b.t2;
+    o1 = (v / b.t2) % b.t1;
+    o0 = v / (b.t1 * b.t2);
+    d2 = stride % b.t2;
+    d1 = (stride / b.t2) % b.t1;
+    d0 = stride / (b.t1 * b.t2);
+  }
+  __device__ __forceinline__ void next(const Box& b) {
+    o2 += d2;
+    int c = o2 >= b.t2 ? 1 : 0;
+    o2 -= c * b.t2;
+    o1 += d1 + c;
+    c = o1 >= b.t1 ? 1 : 0;
+    o1 -= c * b.t1;
+    o0 += d0 + c;
+  }
+};
+
+// d = o - c - s and u = R^T d + c; R row-major.
+__device__ __forceinline__ void pose_coords(const Box& b, const float* R, const float* s,
+                                            const Walker& w, float d[3], float u[3]) {
+  d[0] = (float)w.o0 - b.c0 - s[0];
+  d[1] = (float)w.o1 - b.c1 - s[1];
+  d[2] = (float)w.o2 - b.c2 - s[2];
   u[0] = fmaf(R[0], d[0], fmaf(R[3], d[1], fmaf(R[6], d[2], b.c0)));
   u[1] = fmaf(R[1], d[0], fmaf(R[4], d[1], fmaf(R[7], d[2], b.c1)));
   u[2] = fmaf(R[2], d[0], fmaf(R[5], d[1], fmaf(R[8], d[2], b.c2)));
@@ -92,20 +112,48 @@ __device__ __forceinline__ bool stencil(const Box& b, const float u[3], Stencil&
   return true;
 }
 
-__device__ __forceinline__ int corner_index(const Stencil& st, int q) {
-  return st.base + ((q & 4) ? st.s0 : 0) + ((q & 2) ? st.s1 : 0) + ((q & 1) ? st.s2 : 0);
+// Corner values c[4*b0 + 2*b1 + b2] (b_a = 1: upper neighbour on axis a).
+__device__ __forceinline__ void corners8(const float* __restrict__ a, const Stencil& st,
+                                         float c[8]) {
+  const float* p = a + st.base;
+  const int s12 = st.s1 + st.s2;
+  c[0] = __ldg(p);
+  c[1] = __ldg(p + st.s2);
+  c[2] = __ldg(p + st.s1);
+  c[3] = __ldg(p + s12);
+  p += st.s0;
+  c[4] = __ldg(p);
+  c[5] = __ldg(p + st.s2);
+  c[6] = __ldg(p + st.s1);
+  c[7] = __ldg(p + s12);
 }
 
-__device__ __forceinline__ float corner_weight(const Stencil& st, int q) {
-  const float w0 = (q & 4) ? st.f0 : 1.f - st.f0;
-  const float w1 = (q & 2) ? st.f1 : 1.f - st.f1;
-  const float w2 = (q & 1) ? st.f2 : 1.f - st.f2;
-  return w0 * w1 * w2;
+// Trilinear value as nested linear interpolations (axis 2, then 1, then 0).
+__device__ __forceinline__ float lerp8(const float c[8], const Stencil& st) {
+  const float l00 = fmaf(st.f2, c[1] - c[0], c[0]);
+  const float l01 = fmaf(st.f2, c[3] - c[2], c[2]);
+  const float l10 = fmaf(st.f2, c[5] - c[4], c[4]);
+  const float l11 = fmaf(st.f2, c[7] - c[6], c[6]);
+  const float l0 = fmaf(st.f1, l01 - l00, l00);
+  const float l1 = fmaf(st.f1, l11 - l10, l10);
+  return fmaf(st.f0, l1 - l0, l0);
+}
+
+// Gradient of lerp8 with respect to the fractions (= the sample coordinates).
+__device__ __forceinline__ void lerp8_grad(const float e[8], const Stencil& st, float du[3]) {
+  const float a00 = e[1] - e[0], a01 = e[3] - e[2], a10 = e[5] - e[4], a11 = e[7] - e[6];
+  const float l00 = fmaf(st.f2, a00, e[0]), l01 = fmaf(st.f2, a01, e[2]);
+  const float l10 = fmaf(st.f2, a10, e[4]), l11 = fmaf(st.f2, a11, e[6]);
+  const float b0 = fmaf(st.f1, a01 - a00, a00), b1 = fmaf(st.f1, a11 - a10, a10);
+  du[2] = fmaf(st.f0, b1 - b0, b0);
+  const float c0 = l01 - l00, c1 = l11 - l10;
+  du[1] = fmaf(st.f0, c1 - c0, c0);
+  du[0] = fmaf(st.f1, l11 - l10, l10) - fmaf(st.f1, l01 - l00, l00);
 }
 
 __device__ __forceinline__ float target_at(const float* __restrict__ tg, int n0, int n1, int n2,
-                                           float outside, const int k[3], const int o[3]) {
-  const int x = k[0] + o[0], y = k[1] + o[1], z = k[2] + o[2];
+                                           float outside, const int k[3], const Walker& w) {
+  const int x = k[0] + w.o0, y = k[1] + w.o1, z = k[2] + w.o2;
   if (x < 0 || y < 0 || z < 0 || x >= n0 || y >= n1 || z >= n2) return outside;
   return __ldg(tg + ((int64_t)x * n1 + y) * n2 + z);
 }
@@ -223,15 +271,18 @@ refine_rotate_kernel(const float* __restrict__ T, int t0, int t1, int t2,
   if (threadIdx.x < 3) ss[threadIdx.x] = shifts[p * 3 + threadIdx.x];
   __syncthreads();
   const Box b = make_box(t0, t1, t2);
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < b.nv; v += gridDim.x * blockDim.x) {
-    int o[3];
+  const int start = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  Walker w;
+  w.init(b, start, stride);
+  for (int v = start; v < b.nv; v += stride, w.next(b)) {
     float d[3], u[3];
-    pose_coords(b, Rs, ss, v, o, d, u);
+    pose_coords(b, Rs, ss, w, d, u);
     Stencil st;
     float a = 0.f;
     if (stencil(b, u, st)) {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) a += corner_weight(st, q) * __ldg(T + corner_index(st, q));
+      float c[8];
+      corners8(T, st, c);
+      a = lerp8(c, st);
     }
     Tr[(int64_t)p * b.nv + v] = a;
   }
@@ -259,24 +310,26 @@ refine_forward_kernel(const float* __restrict__ T, const float* __restrict__ M, 
     }
     __syncthreads();
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int v = threadIdx.x; v < b.nv; v += blockDim.x) {
-      int o[3];
+    Walker w;
+    w.init(b, threadIdx.x, blockDim.x);
+    for (int v = threadIdx.x; v < b.nv; v += blockDim.x, w.next(b)) {
       float d[3], u[3];
-      pose_coords(b, Rs, ss, v, o, d, u);
+      pose_coords(b, Rs, ss, w, d, u);
       Stencil st;
       if (!stencil(b, u, st)) continue;
-      float mr = 0.f, tr = 0.f;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int i = corner_index(st, q);
-        const float w = corner_weight(st, q);
-        mr += w * __ldg(M + i);
-        if (!FILTERED) tr += w * __ldg(T + i);
-      }
+      float c[8];
+      corners8(M, st, c);
+      const float mr = lerp8(c, st);
       if (mr == 0.f) continue;
-      const double m = mr;
-      const double tf = FILTERED ? (double)__ldg(Tf + (int64_t)p * b.nv + v) : (double)tr;
-      const double f = target_at(tg, n0, n1, n2, outside, ks, o);
+      float tr;
+      if (FILTERED) {
+        tr = __ldg(Tf + (int64_t)p * b.nv + v);
+      } else {
+        corners8(T, st, c);
+        tr = lerp8(c, st);
+      }
+      const double m = mr, tf = tr;
+      const double f = target_at(tg, n0, n1, n2, outside, ks, w);
       const double mt = m * tf, mf = m * f;
       acc[0] += m;
       acc[1] += mt;
@@ -309,20 +362,22 @@ refine_grad_filtered_kernel(const float* __restrict__ M, int t0, int t1, int t2,
   __syncthreads();
   const ScoreGrad sg = score_grad(sums + 6 * p, eps, (double)gout[p]);
   const Box b = make_box(t0, t1, t2);
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < b.nv; v += gridDim.x * blockDim.x) {
+  const int start = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  Walker w;
+  w.init(b, start, stride);
+  for (int v = start; v < b.nv; v += stride, w.next(b)) {
     float g = 0.f;
     if (sg.valid) {
-      int o[3];
       float d[3], u[3];
-      pose_coords(b, Rs, ss, v, o, d, u);
+      pose_coords(b, Rs, ss, w, d, u);
       Stencil st;
       if (stencil(b, u, st)) {
-        float mr = 0.f;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) mr += corner_weight(st, q) * __ldg(M + corner_index(st, q));
+        float c[8];
+        corners8(M, st, c);
+        const float mr = lerp8(c, st);
         if (mr != 0.f) {
           const double tf = __ldg(Tf + (int64_t)p * b.nv + v);
-          const double f = target_at(tg, n0, n1, n2, outside, ks, o);
+          const double f = target_at(tg, n0, n1, n2, outside, ks, w);
           g = (float)((double)mr * (sg.gB + 2.0 * sg.gC * tf + sg.gD * f));
         }
       }
@@ -361,66 +416,61 @@ refine_backward_kernel(const float* __restrict__ T, const float* __restrict__ M,
     }
     __syncthreads();
     const ScoreGrad sg = score_grad(sums + 6 * p, eps, (double)gout[p]);
-    double acc[12];
+    // per-voxel gradient terms in float; the coefficients come from the double sums
+    const float gA = (float)sg.gA, gB = (float)sg.gB, gC = (float)sg.gC, gD = (float)sg.gD,
+                gE = (float)sg.gE, gF = (float)sg.gF;
+    // per-thread partial sums in float (a few hundred terms each), combined in double
+    float accf[12];
 #pragma unroll
-    for (int k = 0; k < 12; ++k) acc[k] = 0.0;
+    for (int k = 0; k < 12; ++k) accf[k] = 0.f;
     if (sg.valid) {
-      for (int v = threadIdx.x; v < b.nv; v += blockDim.x) {
-        int o[3];
+      Walker w;
+      w.init(b, threadIdx.x, blockDim.x);
+      for (int v = threadIdx.x; v < b.nv; v += blockDim.x, w.next(b)) {
         float d[3], u[3];
-        pose_coords(b, Rs, ss, v, o, d, u);
+        pose_coords(b, Rs, ss, w, d, u);
         Stencil st;
         if (!stencil(b, u, st)) continue;
         float tq[8], mq[8];
-        float mr = 0.f, tr = 0.f;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int i = corner_index(st, q);
-          const float w = corner_weight(st, q);
-          tq[q] = __ldg(T + i);
-          mq[q] = __ldg(M + i);
-          mr += w * mq[q];
-          tr += w * tq[q];
-        }
-        const double tf = FILTERED ? (double)__ldg(Tf + (int64_t)p * b.nv + v) : (double)tr;
-        const double f = target_at(tg, n0, n1, n2, outside, ks, o);
-        const float gm = (float)(sg.gA + tf * (sg.gB + sg.gC * tf + sg.gD * f) +
-                                 f * (sg.gE + sg.gF * f));
-        const float gt = FILTERED
-                             ? __ldg(gTr_in + (int64_t)p * b.nv + v)
-                             : (float)((double)mr * (sg.gB + 2.0 * sg.gC * tf + sg.gD * f));
-        // dS/du through the corner weights; fractional derivative signs per axis
+        corners8(T, st, tq);
+        corners8(M, st, mq);
+        const float mr = lerp8(mq, st);
+        const float tf = FILTERED ? __ldg(Tf + (int64_t)p * b.nv + v) : lerp8(tq, st);
+        const float f = target_at(tg, n0, n1, n2, outside, ks, w);
+        const float gm = fmaf(tf, fmaf(gC, tf, fmaf(gD, f, gB)), fmaf(f, fmaf(gF, f, gE), gA));
+        const float gt = FILTERED ? __ldg(gTr_in + (int64_t)p * b.nv + v)
+                                  : mr * fmaf(2.f * gC, tf, fmaf(gD, f, gB));
+        // dS/du through the trilinear weights of T and M
         float e[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) e[q] = gt * tq[q] + gm * mq[q];
-        const float f0 = st.f0, f1 = st.f1, f2 = st.f2;
-        // differences along axis 2, then bilinear weights on the other two
-        const float a00 = e[1] - e[0], a01 = e[3] - e[2], a10 = e[5] - e[4], a11 = e[7] - e[6];
-        const float du2 = (1.f - f0) * ((1.f - f1) * a00 + f1 * a01) +
-                          f0 * ((1.f - f1) * a10 + f1 * a11);
-        const float l00 = e[0] + f2 * (e[1] - e[0]), l01 = e[2] + f2 * (e[3] - e[2]);
-        const float l10 = e[4] + f2 * (e[5] - e[4]), l11 = e[6] + f2 * (e[7] - e[6]);
-        const float du1 = (1.f - f0) * (l01 - l00) + f0 * (l11 - l10);
-        const float du0 = ((1.f - f1) * l10 + f1 * l11) - ((1.f - f1) * l00 + f1 * l01);
+        for (int q = 0; q < 8; ++q) e[q] = fmaf(gt, tq[q], gm * mq[q]);
+        float du[3];
+        lerp8_grad(e, st, du);
         if (gT != nullptr && gt != 0.f) {
+          const float wx[2] = {1.f - st.f0, st.f0}, wy[2] = {1.f - st.f1, st.f1};
+          const float wz[2] = {(1.f - st.f2) * gt, st.f2 * gt};
 #pragma unroll
           for (int q = 0; q < 8; ++q) {
-            const float w = corner_weight(st, q) * gt;
-            if (SMEM_GT) atomicAdd(gts + corner_index(st, q), w);
-            else atomicAdd(gT + corner_index(st, q), w);
+            const int i = st.base + ((q & 4) ? st.s0 : 0) + ((q & 2) ? st.s1 : 0) +
+                          ((q & 1) ? st.s2 : 0);
+            const float wq = wx[q >> 2] * wy[(q >> 1) & 1] * wz[q & 1];
+            if (SMEM_GT) atomicAdd(gts + i, wq);
+            else atomicAdd(gT + i, wq);
           }
         }
         // u_i = sum_j R[j][i] d_j + c_i: dS/dR[j][i] += du_i d_j; dS/ds_j = -sum_i R[j][i] du_i
-        const float du[3] = {du0, du1, du2};
 #pragma unroll
         for (int j = 0; j < 3; ++j)
 #pragma unroll
-          for (int i = 0; i < 3; ++i) acc[j * 3 + i] += (double)(du[i] * d[j]);
-        acc[9] += du0;
-        acc[10] += du1;
-        acc[11] += du2;
+          for (int i = 0; i < 3; ++i) accf[j * 3 + i] = fmaf(du[i], d[j], accf[j * 3 + i]);
+        accf[9] += du[0];
+        accf[10] += du[1];
+        accf[11] += du[2];
       }
     }
+    double acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = accf[k];
     block_sums<12>(acc, red);
     if (threadIdx.x == 0) {
       if (grad_rot)
