@@ -367,7 +367,8 @@ def run_ours(args):
             md.rotations = rots[:n_e2e]
             res = P.scan_subsets(md, matching_score=scoring, matching_setup=setup,
                                  callback_class=P.MaxScoreOverRotations,
-                                 callback_class_args={"score_threshold": 0})
+                                 callback_class_args={"score_threshold": 0},
+                                 interpolation_order=1)
             return res
 
         e2e()

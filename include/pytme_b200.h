@@ -62,6 +62,20 @@ int tm_rigid_transform(const float* data, const float* mask, int d0, int d1, int
                        const float* matrices, int n_mat, float* out, float* out_mask, int o0,
                        int o1, int o2, void* stream);
 
+/* Order-3 path of the same method: SciPy's spline_filter (order 3, mirror boundary),
+ * which affine_transform(prefilter=True) applies to the data
+ * (tme/backends/npfftw_backend.py:381-388), writing `batch` coefficient volumes of
+ * d0 x d1 x d2 doubles. */
+int tm_spline_prefilter(const float* in, double* coef, int d0, int d1, int d2, int batch,
+                        void* stream);
+/* Order-3 rigid transform from coefficient volumes: `coef` from tm_spline_prefilter for
+ * the data, `mask_coef` the mask itself as doubles (the reference does not prefilter
+ * masks, :434-447). Otherwise as tm_rigid_transform (SciPy constant mode, mirrored
+ * coefficients inside the support at the edges). */
+int tm_rigid_transform_cubic(const double* coef, const double* mask_coef, int d0, int d1,
+                             int d2, const float* matrices, int n_mat, float* out,
+                             float* out_mask, int o0, int o1, int o2, void* stream);
+
 /* In-place masked standardisation of `batch` volumes of n elements:
  * x = (x - mean) / std * mask with mean/std over mask weights, the reference's
  * normalize_template (tme/matching_utils.py:61-99). n_obs > 0 is used as the
@@ -143,6 +157,12 @@ int tm_scan_set_template(tm_scan* plan, const float* template_rev, const float* 
  * tme/matching_scores.py:390-450). Call after tm_scan_set_template.
  * Synchronises the stream. */
 int tm_scan_set_target(tm_scan* plan, const float* target, void* stream);
+/* interpolation_order of corr_scoring / flc_scoring (tme/matching_scores.py:600-608,
+ * 731-740) as rigid_transform applies it (tme/backends/npfftw_backend.py:390-449):
+ * 1 = trilinear (the default), 3 = cubic B-spline with the template prefiltered and
+ * the rotated mask not. Other orders return TM_E_UNSUPPORTED. Synchronous with respect
+ * to `stream` only when the template is already set (it then builds the coefficients). */
+int tm_scan_set_interpolation(tm_scan* plan, int order, void* stream);
 
 /* Scores n rotations given as row-major 4x4 float32 pull matrices on the device
  * (NumpyFFTWBackend._rigid_transform_matrix of each rotation about the template

@@ -29,6 +29,7 @@ __all__ = [
     "fourier_padding",
     "rigid_transform_matrix",
     "rotate_order1",
+    "rotate",
     "normalize_template",
     "norm_scores",
     "apply_template_filter",
@@ -113,9 +114,16 @@ def rotate_order1(data: np.ndarray, matrix: np.ndarray, output: np.ndarray) -> n
     """``_rigid_transform`` (tme/backends/npfftw_backend.py:357-388): order-1
     ``affine_transform`` in constant mode into the top-left ``data.shape`` box of
     ``output``."""
+    return rotate(data, matrix, output, order=1, prefilter=True)
+
+
+def rotate(data: np.ndarray, matrix: np.ndarray, output: np.ndarray, order: int = 1,
+           prefilter: bool = True) -> np.ndarray:
+    """``_rigid_transform`` (tme/backends/npfftw_backend.py:357-388) at any spline order:
+    ``rigid_transform`` (:390-449) prefilters the data and not the mask."""
     out_slice = tuple(slice(0, s) for s in data.shape)
     affine_transform(input=data, matrix=matrix, mode="constant", output=output[out_slice],
-                     order=1, prefilter=True)
+                     order=order, prefilter=prefilter)
     return output
 
 
@@ -212,7 +220,7 @@ def _setup(score, target, template_rev, mask_rev, fast, dtype, cdtype):
 
 
 def _loop(score, setup, template_rev, mask_rev, rotations, fast, dtype, cdtype,
-          template_filter, first_index, max_scores, argmax):
+          template_filter, first_index, max_scores, argmax, order=1):
     """Per-rotation loops ``corr_scoring`` (tme/matching_scores.py:600-624) and
     ``flc_scoring`` (tme/matching_scores.py:727-757) with ``MaxScoreOverRotations``
     state updates (tme/analyzer/aggregation.py:142-189)."""
@@ -227,8 +235,8 @@ def _loop(score, setup, template_rev, mask_rev, rotations, fast, dtype, cdtype,
             matrix = rigid_transform_matrix(rotations[i], center, dtype)
             arr.fill(0)
             temp.fill(0)
-            rotate_order1(template_rev, matrix, arr)
-            rotate_order1(mask_rev, matrix, temp)
+            rotate(template_rev, matrix, arr, order, prefilter=True)
+            rotate(mask_rev, matrix, temp, order, prefilter=False)
             n_obs = np.sum(temp)
             apply_template_filter(arr[unpadded], template_filter)
             normalize_template(arr, temp, n_obs)
@@ -247,7 +255,7 @@ def _loop(score, setup, template_rev, mask_rev, rotations, fast, dtype, cdtype,
         mask_sum = np.sum(mask_rev)
     for i in range(rotations.shape[0]):
         matrix = rigid_transform_matrix(rotations[i], center, dtype)
-        rotate_order1(template_rev, matrix, template_rot)
+        rotate(template_rev, matrix, template_rot, order, prefilter=True)
         apply_template_filter(template_rot, template_filter)
         if mask_sum is not None:
             normalize_template(template_rot, mask_rev, mask_sum)
@@ -284,7 +292,7 @@ def scan(target: np.ndarray, template: np.ndarray, rotations: np.ndarray,
          score: str = "FLCSphericalMask", template_mask: Optional[np.ndarray] = None,
          template_filter: Optional[np.ndarray] = None,
          target_filter: Optional[np.ndarray] = None, pad_target_edges: bool = False,
-         dtype=np.float32, score_threshold: float = 0.0) -> Dict:
+         dtype=np.float32, score_threshold: float = 0.0, interpolation_order: int = 1) -> Dict:
     """One split of ``scan`` (tme/matching_exhaustive.py:144-295) with
     ``MaxScoreOverRotations`` and ``job_schedule=(1, 1)``; returns the raw state and the
     post-processed ``result`` maps (tme/analyzer/aggregation.py:207-277)."""
@@ -302,7 +310,7 @@ def scan(target: np.ndarray, template: np.ndarray, rotations: np.ndarray,
     argmax = np.full(fast, -1, dtype=np.int32)
     tf = None if template_filter is None else np.asarray(template_filter, dtype=dtype)
     _loop(score, setup, t_rev, m_rev, rotations, fast, dtype, cdtype, tf, 0, max_scores,
-          argmax)
+          argmax, order=interpolation_order)
     scores, rot = result_map(max_scores, argmax, shift, conv, tgt.shape, t_rev.shape,
                              "valid" if pad_target_edges else "same")
     return {"scores": scores, "rotations": rot, "fast_shape": fast, "fourier_shift": shift,

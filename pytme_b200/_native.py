@@ -42,7 +42,8 @@ EXPORTED = (
     "tm_find_candidate_indices_workspace", "tm_find_candidate_indices",
     "tm_find_candidate_indices_noalloc", "tm_line_fft_test", "tm_fft_filter",
     "tm_euler_zyz", "tm_refine_rotate", "tm_refine_forward", "tm_refine_grad_filtered",
-    "tm_refine_backward",
+    "tm_refine_backward", "tm_spline_prefilter", "tm_rigid_transform_cubic",
+    "tm_scan_set_interpolation",
 )
 
 
@@ -114,6 +115,10 @@ def _load():
         "tm_find_candidate_indices_noalloc": (c_int, [vp, c_int, c_int64, i32p, i32p, vp]),
         "tm_line_fft_test": (c_int, [vp, vp, c_int, c_int, c_int, vp]),
         "tm_fft_filter": (c_int, [vp, f32p, vp, f32p, vp]),
+        "tm_spline_prefilter": (c_int, [f32p, vp, c_int, c_int, c_int, c_int, vp]),
+        "tm_rigid_transform_cubic": (c_int, [vp, vp, c_int, c_int, c_int, f32p, c_int, f32p,
+                                             f32p, c_int, c_int, c_int, vp]),
+        "tm_scan_set_interpolation": (c_int, [vp, c_int, vp]),
         "tm_euler_zyz": (c_int, [f32p, c_int, f32p, f32p, vp]),
         "tm_refine_rotate": (c_int, [POINTER(RefineDesc), f32p, vp]),
         "tm_refine_forward": (c_int, [POINTER(RefineDesc), f32p, vp, f32p, vp]),

@@ -382,11 +382,14 @@ class B200Backend:
     def rigid_transform(self, arr, rotation_matrix, arr_mask=None, translation=None,
                         use_geometric_center: bool = False, out=None, out_mask=None,
                         order: int = 3, cache: bool = False, batched: bool = False):
-        """Order-1 rigid transform on the device (tm_rigid_transform); the reference's
-        NumpyFFTWBackend.rigid_transform (tme/backends/npfftw_backend.py:390-449) with
-        SciPy's constant mode. Only order 1 and the geometric centre are supported."""
-        if int(order) != 1:
-            raise NotImplementedError("only order=1 (trilinear) rigid transforms are supported")
+        """Rigid transform on the device; the reference's NumpyFFTWBackend.rigid_transform
+        (tme/backends/npfftw_backend.py:390-449) with SciPy's constant mode. Order 1 is
+        trilinear (tm_rigid_transform); order 3 is the cubic B-spline with the data
+        prefiltered and the mask not (tm_spline_prefilter + tm_rigid_transform_cubic).
+        Only the geometric centre is supported."""
+        if int(order) not in (1, 3):
+            raise NotImplementedError("only order 1 (trilinear) and 3 (cubic B-spline) rigid "
+                                      "transforms are supported")
         if batched:
             raise NotImplementedError("batched rigid transforms are not supported")
         arr = self.to_backend_array(arr).to(torch.float32).contiguous()
@@ -405,6 +408,16 @@ class B200Backend:
             if out_mask is None:
                 out_mask = torch.zeros_like(mask)
         o = out.shape
+        if int(order) == 3:
+            coef = torch.empty(arr.shape, dtype=torch.float64, device=arr.device)
+            N.check(N.lib.tm_spline_prefilter(N.ptr(arr), N.ptr(coef), *arr.shape, 1,
+                                              N.stream_ptr()), "tm_spline_prefilter")
+            mcoef = None if mask is None else mask.to(torch.float64).contiguous()
+            N.check(N.lib.tm_rigid_transform_cubic(
+                N.ptr(coef), N.ptr(mcoef), *arr.shape, N.ptr(matrix), 1, N.ptr(out),
+                N.ptr(out_mask) if mask is not None else None, *o, N.stream_ptr()),
+                "tm_rigid_transform_cubic")
+            return out, out_mask
         N.check(N.lib.tm_rigid_transform(N.ptr(arr), N.ptr(mask), *arr.shape, N.ptr(matrix), 1,
                                          N.ptr(out), N.ptr(out_mask) if mask is not None else None,
                                          *o, N.stream_ptr()), "tm_rigid_transform")

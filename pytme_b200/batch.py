@@ -30,8 +30,9 @@ __all__ = ["MatchJob", "scan_batch", "autotune_batch"]
 @dataclass
 class MatchJob:
     """One exhaustive search: target, template (as given, not reversed), optional
-    mask, rotations (n, 3, 3) and optional filters (arrays at the template's and the
-    transform's rfft shapes)."""
+    mask, rotations (n, 3, 3), optional filters (arrays at the template's and the
+    transform's rfft shapes) and the template rotation order (3, the reference's
+    default, or 1)."""
 
     target: np.ndarray
     template: np.ndarray
@@ -41,6 +42,7 @@ class MatchJob:
     template_filter: Optional[np.ndarray] = None
     target_filter: Optional[np.ndarray] = None
     score_threshold: float = 0.0
+    interpolation_order: int = 3
     meta: Dict = field(default_factory=dict)
 
 
@@ -98,6 +100,7 @@ def autotune_batch(job: MatchJob, precision: str = "mixed",
             plan.close()
             return int(candidates[0])
         plan.set_template(t_rev, m_rev, job.template_filter)
+        plan.set_interpolation(job.interpolation_order)
         plan.set_target(target)
         n = b * (groups + 1)
         rots = np.resize(np.asarray(job.rotations, dtype=np.float32).reshape(-1, 3, 3), (n, 3, 3))
@@ -149,6 +152,7 @@ def scan_batch(jobs: List[MatchJob], precision: str = "mixed", rotation_batch="a
             m_rev = None if job.mask is None else np.ascontiguousarray(
                 np.asarray(job.mask, dtype=np.float32)[::-1, ::-1, ::-1])
             plan.set_template(t_rev, m_rev, job.template_filter)
+            plan.set_interpolation(job.interpolation_order)
             target = _prepare_target(job.target, tuple(fast), job.target_filter)
             plan.set_target(target)
             dev = target.device

@@ -65,6 +65,19 @@ int tm_rigid_transform(const float* data, const float* mask, int d0, int d1, int
                              S(stream));
 }
 
+int tm_spline_prefilter(const float* in, double* coef, int d0, int d1, int d2, int batch,
+                        void* stream) {
+  TM_REQUIRE(in, "tm_spline_prefilter: null input");
+  return tmb::spline_prefilter(in, coef, d0, d1, d2, batch, S(stream));
+}
+
+int tm_rigid_transform_cubic(const double* coef, const double* mask_coef, int d0, int d1,
+                             int d2, const float* matrices, int n_mat, float* out,
+                             float* out_mask, int o0, int o1, int o2, void* stream) {
+  return tmb::rigid_transform_cubic(coef, mask_coef, d0, d1, d2, matrices, n_mat, out, out_mask,
+                                   o0, o1, o2, S(stream));
+}
+
 int64_t tm_normalize_template_workspace(int batch) {
   return batch > 0 ? tmb::stats_workspace_bytes(batch) : 0;
 }
@@ -198,6 +211,11 @@ int tm_scan_set_template(tm_scan* plan, const float* template_rev, const float* 
 int tm_scan_set_target(tm_scan* plan, const float* target, void* stream) {
   TM_REQUIRE(plan, "tm_scan_set_target: null plan");
   return tmb::scan_set_target(plan->impl, target, S(stream));
+}
+
+int tm_scan_set_interpolation(tm_scan* plan, int order, void* stream) {
+  TM_REQUIRE(plan, "tm_scan_set_interpolation: null plan");
+  return tmb::scan_set_interpolation(plan->impl, order, S(stream));
 }
 
 int tm_scan_run(tm_scan* plan, const float* matrices, int n, int32_t first_index,

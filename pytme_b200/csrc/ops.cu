@@ -5,6 +5,7 @@
 #include "common.cuh"
 #include "ops.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -126,6 +127,175 @@ int rigid_transform(const float* data, const float* mask, int d0, int d1, int d2
                                                        out_mask, o1, o2,
                                                        (int64_t)o0 * o1 * o2);
   return check_launch("rigid_transform_kernel");
+}
+
+// --------------------------------------------------------------- cubic B-spline (order 3)
+// SciPy's order-3 path (affine_transform with prefilter=True calls spline_filter, then
+// evaluates the spline): interpolation coefficients by the recursive filter of Unser,
+// Aldroubi and Eden ("B-spline signal processing", IEEE Trans. Signal Process. 41, 1993)
+// with the single pole z = sqrt(3) - 2, gain (1 - z)(1 - 1/z) = 6, and mirror-symmetric
+// boundaries (x[-k] = x[k], x[n-1+k] = x[n-1-k]): exact causal initialisation over the
+// mirrored period 2n - 2 and the closed-form anticausal start
+// c[n-1] = z/(z^2 - 1) * (c+[n-1] + z c+[n-2]) (Thevenaz, Blu and Unser, "Interpolation
+// revisited", IEEE Trans. Med. Imaging 19, 2000). Axes are filtered 0, 1, 2 in double.
+__global__ void spline_prefilter_kernel(const float* __restrict__ in, double* __restrict__ c,
+                                        int d0, int d1, int d2, int axis, int batch) {
+  const int n = axis == 0 ? d0 : (axis == 1 ? d1 : d2);
+  const int64_t stride = axis == 0 ? (int64_t)d1 * d2 : (axis == 1 ? d2 : 1);
+  const int64_t lines_per_item = (int64_t)d0 * d1 * d2 / n;
+  const int64_t nvox = (int64_t)d0 * d1 * d2;
+  for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < lines_per_item * batch;
+       l += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = l / lines_per_item, r = l % lines_per_item;
+    int64_t start;
+    if (axis == 0) start = r;                               // r = i1 * d2 + i2
+    else if (axis == 1) start = (r / d2) * d1 * d2 + r % d2;  // r = i0 * d2 + i2
+    else start = r * d2;                                    // r = i0 * d1 + i1
+    double* x = c + b * nvox + start;
+    const float* xi = in ? in + b * nvox + start : nullptr;
+    if (xi)
+      for (int i = 0; i < n; ++i) x[i * stride] = (double)xi[i * stride];
+    if (n == 1) continue;
+    const double z = sqrt(3.0) - 2.0, gain = (1.0 - z) * (1.0 - 1.0 / z);
+    for (int i = 0; i < n; ++i) x[i * stride] *= gain;
+    // causal initialisation over the mirrored signal
+    double zn = 1.0;
+    for (int i = 0; i < n - 1; ++i) zn *= z;  // z^(n-1)
+    double acc = x[0] + zn * x[(n - 1) * stride];
+    double zi = z;
+    for (int i = 1; i < n - 1; ++i) {
+      acc += zi * (x[i * stride] + zn * x[(n - 1 - i) * stride]);
+      zi *= z;
+    }
+    x[0] = acc / (1.0 - zn * zn);
+    for (int i = 1; i < n; ++i) x[i * stride] += z * x[(i - 1) * stride];
+    x[(n - 1) * stride] = z / (z * z - 1.0) * (z * x[(n - 2) * stride] + x[(n - 1) * stride]);
+    for (int i = n - 2; i >= 0; --i) x[i * stride] = z * (x[(i + 1) * stride] - x[i * stride]);
+  }
+}
+
+int spline_prefilter(const float* in, double* coef, int d0, int d1, int d2, int batch,
+                     cudaStream_t stream) {
+  TM_REQUIRE(coef, "spline_prefilter: null output");
+  TM_REQUIRE(d0 > 0 && d1 > 0 && d2 > 0 && batch > 0, "spline_prefilter: empty input");
+  const int dims[3] = {d0, d1, d2};
+  for (int axis = 0; axis < 3; ++axis) {
+    const int64_t lines = (int64_t)d0 * d1 * d2 / dims[axis] * batch;
+    const int64_t blocks = std::min<int64_t>(ceil_div(lines, 128), 148 * 8);
+    spline_prefilter_kernel<<<(unsigned)blocks, 128, 0, stream>>>(axis == 0 ? in : nullptr,
+                                                                 coef, d0, d1, d2, axis, batch);
+    TM_TRY(check_launch("spline_prefilter_kernel"));
+  }
+  return TM_OK;
+}
+
+__global__ void to_double_kernel(const float* __restrict__ in, double* __restrict__ out,
+                                 int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+
+int to_double(const float* in, double* out, int64_t n, cudaStream_t stream) {
+  if (n <= 0) return TM_OK;
+  const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148 * 8);
+  to_double_kernel<<<(unsigned)blocks, 256, 0, stream>>>(in, out, n);
+  return check_launch("to_double_kernel");
+}
+
+// Cubic B-spline basis values at the four samples floor(x) - 1 .. floor(x) + 2 for the
+// fractional part t of x.
+__device__ __forceinline__ void bspline3_weights(double t, double w[4]) {
+  const double t2 = t * t, t3 = t2 * t, s = 1.0 - t;
+  w[0] = s * s * s / 6.0;
+  w[1] = (3.0 * t3 - 6.0 * t2 + 4.0) / 6.0;
+  w[2] = (-3.0 * t3 + 3.0 * t2 + 3.0 * t + 1.0) / 6.0;
+  w[3] = t3 / 6.0;
+}
+
+// Whole-sample mirror of an index into [0, n-1] (period 2n - 2).
+__device__ __forceinline__ int mirror_index(int i, int n) {
+  if (n == 1) return 0;
+  const int p = 2 * n - 2;
+  i = abs(i) % p;
+  return i < n ? i : p - i;
+}
+
+// Order-3 pull interpolation from coefficient arrays with SciPy's constant mode: a
+// sample whose coordinate is below 0 or above n-1 on any axis is 0; otherwise the
+// 4 x 4 x 4 spline support reads mirrored coefficients at the edges. Coordinates in
+// double from the float32 matrix, exactly as the order-1 kernel forms them.
+__global__ void rigid_transform_cubic_kernel(const double* __restrict__ coef,
+                                             const double* __restrict__ mcoef, int d0, int d1,
+                                             int d2, const float* __restrict__ matrices,
+                                             float* __restrict__ out, float* __restrict__ out_mask,
+                                             int o1, int o2, int64_t out_stride) {
+  __shared__ float m[16];
+  const int b = blockIdx.y;
+  if (threadIdx.x < 16) m[threadIdx.x] = matrices[b * 16 + threadIdx.x];
+  __syncthreads();
+  const int64_t nvox = (int64_t)d0 * d1 * d2;
+  const int n[3] = {d0, d1, d2};
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nvox;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const int i2 = (int)(v % d2);
+    const int64_t r = v / d2;
+    const int i1 = (int)(r % d1);
+    const int i0 = (int)(r / d1);
+    const double c[3] = {coord(m, 0, i0, i1, i2), coord(m, 1, i0, i1, i2),
+                         coord(m, 2, i0, i1, i2)};
+    bool inside = true;
+    double w[3][4];
+    int idx[3][4];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (!(c[a] >= 0.0) || c[a] > (double)(n[a] - 1)) inside = false;
+      const double fl = floor(c[a]);
+      bspline3_weights(c[a] - fl, w[a]);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) idx[a][k] = mirror_index((int)fl - 1 + k, n[a]);
+    }
+    const int64_t oi = b * out_stride + ((int64_t)i0 * o1 + i1) * o2 + i2;
+    double acc = 0.0, accm = 0.0;
+    if (inside) {
+      for (int i = 0; i < 4; ++i) {
+        double ai = 0.0, am = 0.0;
+        for (int j = 0; j < 4; ++j) {
+          const int64_t row = ((int64_t)idx[0][i] * d1 + idx[1][j]) * d2;
+          double aj = 0.0, amj = 0.0;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            aj += w[2][k] * __ldg(coef + row + idx[2][k]);
+            if (mcoef) amj += w[2][k] * __ldg(mcoef + row + idx[2][k]);
+          }
+          ai += w[1][j] * aj;
+          am += w[1][j] * amj;
+        }
+        acc += w[0][i] * ai;
+        accm += w[0][i] * am;
+      }
+    }
+    out[oi] = (float)acc;
+    if (out_mask) out_mask[oi] = (float)accm;
+  }
+}
+
+int rigid_transform_cubic(const double* coef, const double* mcoef, int d0, int d1, int d2,
+                          const float* matrices, int n_mat, float* out, float* out_mask, int o0,
+                          int o1, int o2, cudaStream_t stream) {
+  TM_REQUIRE(coef && matrices && out, "rigid_transform_cubic: null pointer");
+  TM_REQUIRE(!out_mask || mcoef, "rigid_transform_cubic: out_mask given without mask");
+  TM_REQUIRE(d0 > 0 && d1 > 0 && d2 > 0 && n_mat > 0, "rigid_transform_cubic: empty input");
+  TM_REQUIRE(o0 >= d0 && o1 >= d1 && o2 >= d2,
+             "rigid_transform_cubic: output box (%d,%d,%d) smaller than input (%d,%d,%d)", o0,
+             o1, o2, d0, d1, d2);
+  const int64_t nvox = (int64_t)d0 * d1 * d2;
+  int64_t blocks = std::min<int64_t>(ceil_div(nvox, 256), 4096);
+  dim3 grid((unsigned)blocks, (unsigned)n_mat);
+  rigid_transform_cubic_kernel<<<grid, 256, 0, stream>>>(coef, out_mask ? mcoef : nullptr, d0,
+                                                         d1, d2, matrices, out, out_mask, o1,
+                                                         o2, (int64_t)o0 * o1 * o2);
+  return check_launch("rigid_transform_cubic_kernel");
 }
 
 // --------------------------------------------------------------- template statistics

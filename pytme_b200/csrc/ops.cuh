@@ -14,6 +14,15 @@ int rigid_transform(const float* data, const float* mask, int d0, int d1, int d2
                     const float* matrices, int n_mat, float* out, float* out_mask, int o0,
                     int o1, int o2, cudaStream_t stream);
 
+// Order 3: interpolation coefficients (SciPy spline_filter, mirror boundary) and the
+// pull interpolation from coefficient arrays.
+int spline_prefilter(const float* in, double* coef, int d0, int d1, int d2, int batch,
+                     cudaStream_t stream);
+int to_double(const float* in, double* out, int64_t n, cudaStream_t stream);
+int rigid_transform_cubic(const double* coef, const double* mcoef, int d0, int d1, int d2,
+                          const float* matrices, int n_mat, float* out, float* out_mask, int o0,
+                          int o1, int o2, cudaStream_t stream);
+
 int64_t stats_workspace_bytes(int batch);
 // stats layout per item: {mean, std, n_obs, 0} (double) after the partial sums
 int template_stats(const float* x, const float* m, int64_t m_item_stride, int e0, int e1, int e2,

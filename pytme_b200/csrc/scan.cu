@@ -1009,6 +1009,11 @@ struct Scan {
   float* mask = nullptr;
   float* tfilter = nullptr;
   float* mat = nullptr;  // B x 16 matrices for the current group (device copy)
+  // interpolation order of the template rotation (1 trilinear, 3 cubic B-spline); for
+  // order 3 the template's spline coefficients and the mask in double
+  int order = 1;
+  double* coef = nullptr;
+  double* mcoef = nullptr;
   // per-group scratch
   float* rot_t = nullptr;
   float* rot_m = nullptr;
@@ -1282,6 +1287,8 @@ static void destroy(Scan* s) {
   if (s->have_fwd) { cufftDestroy(s->fwd); cufftDestroy(s->inv); }
   if (s->have_tfwd) { cufftDestroy(s->tfwd); cufftDestroy(s->tinv); }
   if (s->base) cudaFree(s->base);
+  if (s->coef) cudaFree(s->coef);
+  if (s->mcoef) cudaFree(s->mcoef);
   delete s;
 }
 
@@ -1563,6 +1570,12 @@ int scan_set_target(Scan* s, const float* target, cudaStream_t stream) {
   return check_launch("scan_set_target");
 }
 
+static int make_coefficients(Scan* s, cudaStream_t stream) {
+  TM_TRY(spline_prefilter(s->tmpl, s->coef, s->t0, s->t1, s->t2, 1, stream));
+  if (s->d.score == TM_SCORE_FLC) TM_TRY(to_double(s->mask, s->mcoef, s->T, stream));
+  return TM_OK;
+}
+
 // template/mask: reversed (t0,t1,t2) float32 device arrays; filter: (t0,t1,t2//2+1) or null.
 int scan_set_template(Scan* s, const float* tmpl, const float* mask, const float* filt,
                       cudaStream_t stream) {
@@ -1587,14 +1600,45 @@ int scan_set_template(Scan* s, const float* tmpl, const float* mask, const float
     s->mask_sum = tot;
   }
   s->template_ready = true;
+  if (s->order == 3) TM_TRY(make_coefficients(s, stream));
   return check_launch("scan_set_template");
+}
+
+// interpolation_order of corr_scoring / flc_scoring (tme/matching_scores.py:600-608,
+// 731-740), passed on to rigid_transform (tme/backends/npfftw_backend.py:390-449): the
+// template is prefiltered, the mask is not. A captured launch-group graph is dropped
+// because it holds the other rotation kernel.
+int scan_set_interpolation(Scan* s, int order, cudaStream_t stream) {
+  TM_REQUIRE(s, "scan_set_interpolation: null plan");
+  if (order == 0) order = 1;
+  if (order != 1 && order != 3) {
+    set_error("scan_set_interpolation: interpolation order %d is not supported (1 and 3 are)",
+              order);
+    return TM_E_UNSUPPORTED;
+  }
+  if (order == s->order) return TM_OK;
+  if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+  s->order = order;
+  if (order == 3) {
+    if (!s->coef) {
+      TM_TRY(cuda_status(cudaMalloc((void**)&s->coef, sizeof(double) * s->T), "coefficients"));
+      TM_TRY(cuda_status(cudaMalloc((void**)&s->mcoef, sizeof(double) * s->T), "coefficients"));
+    }
+    if (s->template_ready) TM_TRY(make_coefficients(s, stream));
+  }
+  return TM_OK;
 }
 
 // rotate, filter and normalise B templates of the current group into rot_t (and rot_m for FLC)
 static int prepare_templates(Scan* s, int nb, cudaStream_t stream) {
   const bool flc = s->d.score == TM_SCORE_FLC;
-  TM_TRY(rigid_transform(s->tmpl, flc ? s->mask : nullptr, s->t0, s->t1, s->t2, s->mat, nb,
-                         s->rot_t, flc ? s->rot_m : nullptr, s->t0, s->t1, s->t2, stream));
+  if (s->order == 3)
+    TM_TRY(rigid_transform_cubic(s->coef, flc ? s->mcoef : nullptr, s->t0, s->t1, s->t2, s->mat,
+                                 nb, s->rot_t, flc ? s->rot_m : nullptr, s->t0, s->t1, s->t2,
+                                 stream));
+  else
+    TM_TRY(rigid_transform(s->tmpl, flc ? s->mask : nullptr, s->t0, s->t1, s->t2, s->mat, nb,
+                           s->rot_t, flc ? s->rot_m : nullptr, s->t0, s->t1, s->t2, stream));
   if (s->d.has_template_filter) {
     // _apply_filter_subset (tme/matching_scores.py:125-135): rfftn -> * filter -> irfftn
     cufftSetStream(s->tfwd, stream);

@@ -280,7 +280,7 @@ def _evaluate_filter(filt, shape, data_rfft=None, **kwargs):
 def scan(matching_data: MatchingData, matching_setup: Callable, matching_score: Callable,
          n_jobs: int = 1, callback_class=None, callback_class_args: Optional[Dict] = None,
          pad_target: bool = True, pad_template_filter: bool = False,
-         interpolation_order: int = 1, jobs_per_callback_class: int = 8, target_slice=None,
+         interpolation_order: int = 3, jobs_per_callback_class: int = 8, target_slice=None,
          template_slice=None, **kwargs):
     """One split of the search (tme/matching_exhaustive.py:144-295). Rotations are
     scored in one process on the current GPU; ``n_jobs`` only shapes the rotation
@@ -333,7 +333,7 @@ def scan_subsets(matching_data: MatchingData, matching_score: Callable,
                  callback_class_args: Optional[Dict] = None, job_schedule=(1, 1),
                  target_splits: Optional[Dict] = None, template_splits: Optional[Dict] = None,
                  pad_target_edges: bool = False, pad_template_filter: bool = False,
-                 interpolation_order: int = 1, jobs_per_callback_class: int = 8,
+                 interpolation_order: int = 3, jobs_per_callback_class: int = 8,
                  backend_name: str = None, backend_args: Optional[Dict] = None,
                  verbose: bool = False, **kwargs):
     """tme/matching_exhaustive.py:298-465. Splits run one after another on the

@@ -104,6 +104,16 @@ class ScanPlan:
         N.check(N.lib.tm_scan_set_template(self._h, N.ptr(t), N.ptr(m), N.ptr(f),
                                            N.stream_ptr(stream)), "tm_scan_set_template")
 
+    def set_interpolation(self, order: int, stream=None):
+        """Template rotation order: 1 trilinear, 3 cubic B-spline (SciPy's prefiltered
+        spline for the template, unfiltered for the FLC mask)."""
+        order = int(order)
+        if order == getattr(self, "_order", 1):
+            return
+        N.check(N.lib.tm_scan_set_interpolation(self._h, order, N.stream_ptr(stream)),
+                "tm_scan_set_interpolation")
+        self._order = order
+
     def set_target(self, target_fast, stream=None):
         t = _to_device(target_fast)
         if tuple(t.shape) != self.fast_shape:
@@ -264,8 +274,7 @@ def _matrices(rotations, template_shape) -> Tuple[torch.Tensor, np.ndarray]:
 
 
 def _score_chunk(plan: "ScanPlan", rotations, callback, interpolation_order: int):
-    if int(interpolation_order) != 1:
-        raise NotImplementedError("only interpolation_order=1 (trilinear) is implemented")
+    plan.set_interpolation(interpolation_order)
     mats, rot = _matrices(rotations, plan.template_shape)
     n = rot.shape[0]
     if n == 0:
@@ -288,13 +297,13 @@ def _score_chunk(plan: "ScanPlan", rotations, callback, interpolation_order: int
     return callback
 
 
-def corr_scoring(plan: "ScanPlan", rotations, callback, interpolation_order: int = 1,
+def corr_scoring(plan: "ScanPlan", rotations, callback, interpolation_order: int = 3,
                  template_filter=None, **kwargs):
     """corr_scoring (tme/matching_scores.py:491-626) for CC and FLCSphericalMask."""
     return _score_chunk(plan, rotations, callback, interpolation_order)
 
 
-def flc_scoring(plan: "ScanPlan", rotations, callback, interpolation_order: int = 1,
+def flc_scoring(plan: "ScanPlan", rotations, callback, interpolation_order: int = 3,
                 template_filter=None, **kwargs):
     """flc_scoring (tme/matching_scores.py:629-759): rotated mask, per-rotation local
     statistics."""

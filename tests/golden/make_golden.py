@@ -20,6 +20,8 @@ mrcfile; scikit-image stubs). Its own public API then produces:
                      for every score and both ``pad_target_edges`` settings.
 * ``rigid.npz``      order-1 rigid transforms of random data (both matrix forms).
 * ``candidates.npz`` ``find_candidate_indices`` on random integer coordinates.
+* ``cubic.npz``      FLCSphericalMask, FLC and CC scans with ``interpolation_order=3``
+                     (FP32 and FP64), and one order-3 rigid transform of data and mask.
 
 Inputs are stored next to the outputs so the tests never need the reference.
 """
@@ -58,7 +60,7 @@ def _import_reference(ref: str):
 
 def _scan(be, score, target, template, mask, rotations, dtype64=False,
           template_filter=None, target_filter=None, pad_edges=False, splits=None,
-          callback=None, callback_args=None, job_schedule=(1, 1)):
+          callback=None, callback_args=None, job_schedule=(1, 1), order=1):
     from tme.matching_data import MatchingData
     from tme.matching_exhaustive import scan_subsets, MATCHING_EXHAUSTIVE_REGISTER
     from tme.analyzer import MaxScoreOverRotations
@@ -81,15 +83,48 @@ def _scan(be, score, target, template, mask, rotations, dtype64=False,
         md, matching_score=scoring, matching_setup=setup,
         callback_class=callback or MaxScoreOverRotations,
         callback_class_args=callback_args or {"score_threshold": 0},
-        job_schedule=job_schedule, interpolation_order=1, pad_target_edges=pad_edges,
+        job_schedule=job_schedule, interpolation_order=order, pad_target_edges=pad_edges,
         pad_template_filter=False, target_splits=splits or {},
         backend_name="numpyfftw", backend_args=kw)
+
+
+def _cubic(be, create_mask, syn):
+    """Scans and one rigid transform with interpolation_order=3."""
+    rng = np.random.default_rng(6)
+    tmpl = syn.blob_template(12, rng, radius=3.5, sigma=1.2)
+    target, _, _ = syn.make_tomogram((36, 32, 30), tmpl, 3, rng, scale=1.0)
+    mask = syn.dilated_threshold_mask(tmpl, 0.1, 1)
+    smask = create_mask("ellipse", shape=(12, 12, 12), radius=6,
+                        center=(5.5, 5.5, 5.5)).astype(np.float32)
+    rotations = syn.random_rotation_matrices(12, rng)
+    cubic = {"target": target, "template": tmpl, "mask": mask, "smask": smask,
+             "rotations": rotations}
+    for score, m in (("FLCSphericalMask", smask), ("FLC", mask), ("CC", None)):
+        r32 = _scan(be, score, target, tmpl, m, rotations, order=3)
+        r64 = _scan(be, score, target, tmpl, m, rotations, dtype64=True, order=3)
+        cubic[f"{score}_scores32"] = np.asarray(r32[0], np.float32)
+        cubic[f"{score}_rot32"] = np.asarray(r32[2]).astype(np.int16)
+        cubic[f"{score}_scores64"] = np.asarray(r64[0]).astype(np.float32)
+        cubic[f"{score}_rot64"] = np.asarray(r64[2]).astype(np.int16)
+    be.change_backend("numpyfftw")
+    data = rng.normal(size=(13, 11, 9)).astype(np.float32)
+    dmask = (rng.uniform(size=data.shape) > 0.3).astype(np.float32)
+    big = np.zeros((16, 16, 16), np.float32)
+    bigm = np.zeros((16, 16, 16), np.float32)
+    o3, om3 = be.rigid_transform(arr=data, arr_mask=dmask, rotation_matrix=rotations[0],
+                                 out=big, out_mask=bigm, use_geometric_center=True, order=3)
+    cubic.update(rigid_data=data, rigid_mask=dmask, rigid_out=np.asarray(o3),
+                 rigid_out_mask=np.asarray(om3))
+    np.savez_compressed(os.path.join(HERE, "cubic.npz"), **cubic)
+
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("PYTME_REFERENCE",
                                                           "/root/reference"))
+    ap.add_argument("--only", default=None,
+                    help="write only this fixture (e.g. cubic) and leave the others")
     args = ap.parse_args()
     warnings.simplefilter("ignore")
     _import_reference(args.reference)
@@ -102,6 +137,11 @@ def main():
     from tme.filters import Compose, CTFReconstructed, WedgeReconstructed
     from tme.extensions import find_candidate_indices
     from pytme_b200 import synthetic as syn
+
+    if args.only == "cubic":
+        _cubic(be, create_mask, syn)
+        print("golden vectors written to", HERE)
+        return
 
     # ---- config 1: 64^3 target, 16^3 blob template, spherical mask r=8, 30 deg set
     rng = np.random.default_rng(0)
@@ -208,6 +248,8 @@ def main():
                                                                             m.shape))
             kat[f"{score}_{int(pad)}_max"] = m.max()
     np.savez_compressed(os.path.join(HERE, "kat_exhaustive.npz"), **kat)
+
+    _cubic(be, create_mask, syn)
 
     # ---- rigid transforms (order 1, constant mode), both matrix forms
     be.change_backend("numpyfftw")

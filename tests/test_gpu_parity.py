@@ -33,7 +33,7 @@ def torch_cuda():
 
 def _scan(score, target, template, mask, rotations, precision="fp32", plain=False, batch=16,
           template_filter=None, target_filter=None, pad=False, splits=None, callback=None,
-          callback_args=None):
+          callback_args=None, order=1):
     import pytme_b200 as P
     from pytme_b200.analyzer import MaxScoreOverRotations
 
@@ -48,7 +48,7 @@ def _scan(score, target, template, mask, rotations, precision="fp32", plain=Fals
     return P.scan_subsets(md, matching_score=scoring, matching_setup=setup,
                           callback_class=callback or MaxScoreOverRotations,
                           callback_class_args=callback_args or {"score_threshold": 0},
-                          job_schedule=(1, 1), interpolation_order=1,
+                          job_schedule=(1, 1), interpolation_order=order,
                           pad_target_edges=pad, target_splits=splits or {})
 
 
@@ -369,6 +369,43 @@ def test_scan_batch_uneven_jobs_and_graph_replay(torch_cuda, tmp_path, monkeypat
     graph8 = scan_batch(jobs, precision="fp32", rotation_batch=8, use_graph=True)
     for job, (s, r), (s2, r2), (s3, r3) in zip(jobs, res, direct, graph8):
         ref = O.scan(job.target, job.template, job.rotations, "FLCSphericalMask",
-                     template_mask=job.mask, template_filter=job.template_filter)
+                     template_mask=job.mask, template_filter=job.template_filter,
+                     interpolation_order=job.interpolation_order)
         assert np.abs(s - ref["scores"]).max() <= TOL
         assert np.array_equal(s2, s3) and np.array_equal(r2, r3)
+
+
+def test_cubic_rigid_transform_matches_reference(torch_cuda, golden):
+    """Backend rigid_transform with order 3 (prefiltered data, unfiltered mask) against
+    the reference's own output."""
+    import pytme_b200 as P
+
+    g = golden("cubic.npz")
+    be = P.backend
+    be.change_backend("b200")
+    out = torch_cuda.zeros((16, 16, 16), device="cuda")
+    outm = torch_cuda.zeros((16, 16, 16), device="cuda")
+    o, om = be.rigid_transform(arr=g["rigid_data"], arr_mask=g["rigid_mask"],
+                               rotation_matrix=g["rotations"][0], out=out, out_mask=outm,
+                               use_geometric_center=True, order=3)
+    assert np.abs(o.cpu().numpy() - g["rigid_out"]).max() < 1e-5
+    assert np.abs(om.cpu().numpy() - g["rigid_out_mask"]).max() < 1e-5
+
+
+@pytest.mark.parametrize("score", ["FLCSphericalMask", "FLC", "CC"])
+@pytest.mark.parametrize("precision,plain", [("fp32", True), ("fp32", False), ("mixed", False)])
+def test_cubic_scan_matches_reference(torch_cuda, golden, score, precision, plain):
+    """interpolation_order=3, the reference's default, through scan_subsets."""
+    g = golden("cubic.npz")
+    mask = {"FLCSphericalMask": g["smask"], "FLC": g["mask"], "CC": None}[score]
+    res = _scan(score, g["target"], g["template"], mask, g["rotations"], precision=precision,
+                plain=plain, batch=8, order=3)
+    scores, rot = np.asarray(res[0]), np.asarray(res[2])
+    ref32, ref64 = g[f"{score}_scores32"], g[f"{score}_scores64"]
+    # CC maps are not normalised: the bound is relative to the map's scale there
+    scale = max(1.0, float(np.abs(ref64).max())) if score == "CC" else 1.0
+    tol = TOL * scale if precision == "fp32" else max(TOL * scale, mixed_tol(ref32))
+    assert np.abs(scores - ref32).max() <= tol
+    assert np.abs(scores - ref64).max() <= tol
+    mism = np.argwhere(rot != g[f"{score}_rot32"].astype(np.int32))
+    assert len(mism) <= max(1, int(1e-3 * rot.size))

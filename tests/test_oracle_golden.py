@@ -113,3 +113,32 @@ def test_refine_score_matches_reference_flc_map(golden):
         assert abs(s - float(g["scores64"][tuple(x)])) < 1e-6
         checked += 1
     assert checked >= 20
+
+
+@pytest.mark.parametrize("score", ["FLCSphericalMask", "FLC", "CC"])
+def test_cubic_scan(golden, score):
+    """interpolation_order=3 (the reference's default): prefiltered cubic B-spline
+    rotation of the template, unprefiltered of the mask."""
+    g = golden("cubic.npz")
+    mask = {"FLCSphericalMask": g["smask"], "FLC": g["mask"], "CC": None}[score]
+    r = O.scan(g["target"], g["template"], g["rotations"], score, template_mask=mask,
+               interpolation_order=3)
+    assert np.array_equal(r["scores"], g[f"{score}_scores32"])
+    assert np.array_equal(r["rotations"], g[f"{score}_rot32"].astype(np.int32))
+    r = O.scan(g["target"], g["template"], g["rotations"], score, template_mask=mask,
+               interpolation_order=3, dtype=np.float64)
+    # the fixture stores the FP64 map rounded to float32 (CC maps are not normalised)
+    ref64 = g[f"{score}_scores64"]
+    assert np.abs(r["scores"] - ref64).max() < 1e-7 * max(1.0, float(np.abs(ref64).max()))
+
+
+def test_cubic_rigid_transform(golden):
+    g = golden("cubic.npz")
+    data, mask = g["rigid_data"], g["rigid_mask"]
+    m = O.rigid_transform_matrix(g["rotations"][0], (np.asarray(data.shape) - 1) / 2)
+    out = np.zeros((16, 16, 16), np.float32)
+    outm = np.zeros((16, 16, 16), np.float32)
+    O.rotate(data, m, out, order=3, prefilter=True)
+    O.rotate(mask, m, outm, order=3, prefilter=False)
+    assert np.array_equal(out, g["rigid_out"])
+    assert np.array_equal(outm, g["rigid_out_mask"])
