@@ -231,6 +231,26 @@ int tm_find_candidate_indices(const int64_t* coords, int n, int64_t min_distance
 int tm_find_candidate_indices_noalloc(const int64_t* coords, int n, int64_t min_distance,
                                       int32_t* out_idx, int32_t* out_count, void* stream);
 
+/* ---- filters built on the device: CTFReconstructed (tme/filters/ctf.py:260-336, 528-655)
+ * and WedgeReconstructed with create_continuous_wedge=True (tme/filters/wedge.py:282-374),
+ * multiplied in the given order like Compose (tme/filters/compose.py:36-59), written
+ * as float32 with the DC term at index 0, in rfft layout (last axis n2//2 + 1) when
+ * `rfft` is non-zero. Component parameters are the float64 scalars the reference
+ * derives from the filter's arguments:
+ *   CTF:   p[0] defocus_x, p[1] 0.5 * aberration, p[2] pi * wavelength, p[3] phase shift,
+ *          p[4] atan(A / sqrt(1 - A^2)), p[5] frequency cutoff, p[6] flip phase (0/1);
+ *   WEDGE: p[0] start, p[1] stop, p[2] ratio at opening index 0, p[3] opening axis,
+ *          p[4] tilt axis, p[5] frequency cutoff (negative: none). */
+#define TM_FILTER_CTF 1
+#define TM_FILTER_WEDGE 2
+#define TM_FILTER_MAX_COMPONENTS 4
+typedef struct {
+  int kind;
+  double p[8];
+} tm_filter_component;
+int tm_build_filter(const tm_filter_component* components, int n_components,
+                    const int* shape, int rfft, float* out, void* stream);
+
 /* ---- local refinement of candidate peaks: the FLC of flc_scoring
  * (tme/matching_scores.py:629-759) at one pose per peak and its adjoint. This
  * replaces the derivative-free score of tme/matching_optimization.py:54-277 and

@@ -43,7 +43,7 @@ EXPORTED = (
     "tm_find_candidate_indices_noalloc", "tm_line_fft_test", "tm_fft_filter",
     "tm_euler_zyz", "tm_refine_rotate", "tm_refine_forward", "tm_refine_grad_filtered",
     "tm_refine_backward", "tm_spline_prefilter", "tm_rigid_transform_cubic",
-    "tm_scan_set_interpolation",
+    "tm_scan_set_interpolation", "tm_build_filter",
 )
 
 
@@ -57,6 +57,15 @@ class ScanDesc(Structure):
         ("plain", c_int),
         ("has_template_filter", c_int),
     ]
+
+
+TM_FILTER_CTF = 1
+TM_FILTER_WEDGE = 2
+TM_FILTER_MAX_COMPONENTS = 4
+
+
+class FilterComponent(Structure):
+    _fields_ = [("kind", c_int), ("p", c_double * 8)]
 
 
 class RefineDesc(Structure):
@@ -119,6 +128,7 @@ def _load():
         "tm_rigid_transform_cubic": (c_int, [vp, vp, c_int, c_int, c_int, f32p, c_int, f32p,
                                              f32p, c_int, c_int, c_int, vp]),
         "tm_scan_set_interpolation": (c_int, [vp, c_int, vp]),
+        "tm_build_filter": (c_int, [vp, c_int, POINTER(c_int), c_int, f32p, vp]),
         "tm_euler_zyz": (c_int, [f32p, c_int, f32p, f32p, vp]),
         "tm_refine_rotate": (c_int, [POINTER(RefineDesc), f32p, vp]),
         "tm_refine_forward": (c_int, [POINTER(RefineDesc), f32p, vp, f32p, vp]),

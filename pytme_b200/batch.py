@@ -21,7 +21,8 @@ from typing import Dict, List, Optional, Sequence, Tuple
 import numpy as np
 import torch
 
-from .matching import apply_convolution_mode, fourier_padding, rigid_transform_matrices
+from .matching import (_evaluate_filter, apply_convolution_mode, fourier_padding,
+                       rigid_transform_matrices)
 from .scores import ScanPlan, _prepare_target
 
 __all__ = ["MatchJob", "scan_batch", "autotune_batch"]
@@ -31,16 +32,17 @@ __all__ = ["MatchJob", "scan_batch", "autotune_batch"]
 class MatchJob:
     """One exhaustive search: target, template (as given, not reversed), optional
     mask, rotations (n, 3, 3), optional filters (arrays at the template's and the
-    transform's rfft shapes) and the template rotation order (3, the reference's
-    default, or 1)."""
+    transform's rfft shapes, or filter objects; CTFs and continuous wedges are then
+    built on the GPU) and the template rotation order (3, the reference's default, or
+    1)."""
 
     target: np.ndarray
     template: np.ndarray
     rotations: np.ndarray
     mask: Optional[np.ndarray] = None
     score: str = "FLCSphericalMask"
-    template_filter: Optional[np.ndarray] = None
-    target_filter: Optional[np.ndarray] = None
+    template_filter: Optional[object] = None
+    target_filter: Optional[object] = None
     score_threshold: float = 0.0
     interpolation_order: int = 3
     meta: Dict = field(default_factory=dict)
@@ -87,7 +89,9 @@ def autotune_batch(job: MatchJob, precision: str = "mixed",
     t_rev = np.ascontiguousarray(job.template[::-1, ::-1, ::-1], dtype=np.float32)
     m_rev = None if job.mask is None else np.ascontiguousarray(job.mask[::-1, ::-1, ::-1],
                                                                    dtype=np.float32)
-    target = _prepare_target(job.target, tuple(fast), job.target_filter)
+    tf = _evaluate_filter(job.template_filter, job.template.shape)
+    gf = _evaluate_filter(job.target_filter, tuple(fast), weight_type=None)
+    target = _prepare_target(job.target, tuple(fast), gf)
     center = np.divide(np.asarray(job.template.shape) - 1, 2)
     dev = target.device
     best, best_rate = None, -1.0
@@ -99,7 +103,7 @@ def autotune_batch(job: MatchJob, precision: str = "mixed",
         if plan.plain:
             plan.close()
             return int(candidates[0])
-        plan.set_template(t_rev, m_rev, job.template_filter)
+        plan.set_template(t_rev, m_rev, tf)
         plan.set_interpolation(job.interpolation_order)
         plan.set_target(target)
         n = b * (groups + 1)
@@ -151,9 +155,10 @@ def scan_batch(jobs: List[MatchJob], precision: str = "mixed", rotation_batch="a
             t_rev = np.ascontiguousarray(tmpl[::-1, ::-1, ::-1])
             m_rev = None if job.mask is None else np.ascontiguousarray(
                 np.asarray(job.mask, dtype=np.float32)[::-1, ::-1, ::-1])
-            plan.set_template(t_rev, m_rev, job.template_filter)
+            plan.set_template(t_rev, m_rev, _evaluate_filter(job.template_filter, tmpl.shape))
             plan.set_interpolation(job.interpolation_order)
-            target = _prepare_target(job.target, tuple(fast), job.target_filter)
+            gf = _evaluate_filter(job.target_filter, tuple(fast), weight_type=None)
+            target = _prepare_target(job.target, tuple(fast), gf)
             plan.set_target(target)
             dev = target.device
             smax = torch.full(tuple(fast), float(job.score_threshold), dtype=torch.float32,

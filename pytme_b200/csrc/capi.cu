@@ -272,6 +272,11 @@ int tm_fft_filter(tm_fft_plan* p, float* x, void* spectrum, const float* filter,
 }
 
 // ------------------------------------------------------------------ refinement
+int tm_build_filter(const tm_filter_component* components, int n_components, const int* shape,
+                    int rfft, float* out, void* stream) {
+  return tmb::build_filter(components, n_components, shape, rfft, out, S(stream));
+}
+
 int tm_euler_zyz(const float* angles, int n, float* rot, float* drot, void* stream) {
   return tmb::euler_zyz(angles, n, rot, drot, S(stream));
 }

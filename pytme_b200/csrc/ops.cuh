@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "pytme_b200.h"
+
 namespace tmb {
 
 const char* last_error();
@@ -22,6 +24,9 @@ int to_double(const float* in, double* out, int64_t n, cudaStream_t stream);
 int rigid_transform_cubic(const double* coef, const double* mcoef, int d0, int d1, int d2,
                           const float* matrices, int n_mat, float* out, float* out_mask, int o0,
                           int o1, int o2, cudaStream_t stream);
+
+int build_filter(const tm_filter_component* comps, int n_comp, const int* shape, int rfft,
+                 float* out, cudaStream_t stream);
 
 int64_t stats_workspace_bytes(int batch);
 // stats layout per item: {mean, std, n_obs, 0} (double) after the partial sums

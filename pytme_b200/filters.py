@@ -12,7 +12,9 @@ casts), the filters a scan multiplies into template and target spectra:
 
 Each filter is called like the reference's (``f(shape=..., return_real_fourier=True,
 ...)``) and returns a dict whose ``data`` is a float32 NumPy array in rfft layout
-(DC at index 0). The scan multiplies these arrays on the device.
+(DC at index 0). ``device_filter`` builds CTFs, continuous wedges and their Compose
+directly on the GPU (``csrc/filters.cu``) with the same per-voxel arithmetic; the scan
+path uses it whenever a filter is one of those.
 """
 from __future__ import annotations
 
@@ -22,7 +24,8 @@ from typing import Dict, Tuple
 import numpy as np
 
 __all__ = ["fftfreqn", "shift_fourier", "crop_real_fourier", "create_ctf",
-           "CTFReconstructed", "WedgeReconstructed", "LinearWhiteningFilter", "Compose"]
+           "CTFReconstructed", "WedgeReconstructed", "LinearWhiteningFilter", "Compose",
+           "device_filter"]
 
 
 def fftfreqn(shape, sampling_rate, compute_euclidean_norm=False, shape_is_real_fourier=False):
@@ -300,3 +303,78 @@ class Compose:
                 ret["merge"] = None
             meta = ret
         return meta
+
+
+# ----------------------------------------------------------------------------- device
+def _ctf_component(f: "CTFReconstructed", kwargs: Dict):
+    """Float64 scalars of ``create_ctf`` for one CTF (the per-voxel part runs on the
+    device)."""
+    args = dict(vars(f))
+    args.update(kwargs)
+    if args.get("defocus_y") is not None or np.ndim(args["defocus_x"]) != 0:
+        raise NotImplementedError("astigmatic or per-tilt CTFs are built on the host")
+    sampling_rate = np.max(args.get("sampling_rate", 1))
+    lam = _electron_wavelength(f.acceleration_voltage)
+    lam /= sampling_rate
+    aberration = (args.get("spherical_aberration", 2.7e3) / sampling_rate) * lam ** 2
+    amp = args.get("amplitude_contrast", 0.07)
+    amp_phase = np.arctan(np.divide(amp, np.sqrt(1 - np.square(amp))))
+    return (1, [float(args["defocus_x"]), float(0.5 * aberration), float(np.pi * lam),
+                float(args.get("phase_shift", 0)), float(amp_phase),
+                float(args.get("cutoff_frequency", 0.5)),
+                1.0 if args.get("flip_phase", True) else 0.0])
+
+
+def _wedge_component(f: "WedgeReconstructed", shape, kwargs: Dict):
+    """Float64 bounds of ``continuous_wedge`` for one wedge."""
+    args = dict(vars(f))
+    args.update(kwargs)
+    oa, ta = int(args["opening_axis"]), int(args["tilt_axis"])
+    angles = np.abs(np.asarray(args["angles"]))
+    aspect = shape[oa] / shape[ta]
+    angles = np.degrees(np.arctan(np.tan(np.radians(angles)) * aspect))
+    start = np.tan(np.radians(90 - angles[0]))
+    stop = np.tan(np.radians(-1 * (90 - angles[1])))
+    at_zero = np.tan(np.radians(90)) + 1
+    cutoff = args.get("frequency_cutoff", None)
+    return (2, [float(start), float(stop), float(at_zero), float(oa), float(ta),
+                -1.0 if cutoff is None else float(cutoff)])
+
+
+def device_filter(filt, shape, return_real_fourier: bool = True, **kwargs):
+    """Build ``CTFReconstructed``, ``WedgeReconstructed`` or a ``Compose`` of them on the
+    current GPU (``tm_build_filter``) and return it as a float32 torch tensor with the
+    DC term at index 0, equal to ``filt(shape=shape, return_real_fourier=...)["data"]``.
+    Raises ``NotImplementedError`` for filters it does not cover (astigmatic CTFs,
+    weighted or per-angle wedges, whitening, other classes)."""
+    import torch
+
+    from . import _native as N
+
+    shape = tuple(int(x) for x in shape)
+    if len(shape) != 3:
+        raise NotImplementedError("device filters are built for 3D shapes")
+    if not torch.cuda.is_available():
+        raise NotImplementedError("no CUDA device: filters are built on the host")
+    items = filt.transforms if isinstance(filt, Compose) else [filt]
+    comps = []
+    for f in items:
+        if type(f) is CTFReconstructed:
+            comps.append(_ctf_component(f, kwargs))
+        elif type(f) is WedgeReconstructed:
+            comps.append(_wedge_component(f, shape, kwargs))
+        else:
+            raise NotImplementedError(f"{type(f).__name__} is built on the host")
+    if not 1 <= len(comps) <= N.TM_FILTER_MAX_COMPONENTS:
+        raise NotImplementedError("1 to 4 filter components are built on the device")
+    arr = (N.FilterComponent * len(comps))()
+    for i, (kind, p) in enumerate(comps):
+        arr[i].kind = kind
+        for j, v in enumerate(p):
+            arr[i].p[j] = v
+    out_shape = shape[:-1] + ((shape[-1] // 2 + 1) if return_real_fourier else shape[-1],)
+    out = torch.empty(out_shape, dtype=torch.float32, device=torch.device("cuda"))
+    dims = (N.c_int * 3)(*shape)
+    N.check(N.lib.tm_build_filter(arr, len(comps), dims, int(bool(return_real_fourier)),
+                                  N.ptr(out), N.stream_ptr()), "tm_build_filter")
+    return out

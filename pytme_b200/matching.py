@@ -15,6 +15,7 @@ from itertools import product
 from typing import Callable, Dict, Optional, Tuple
 
 import numpy as np
+import torch
 
 __all__ = [
     "next_fast_len",
@@ -271,9 +272,18 @@ def _evaluate_filter(filt, shape, data_rfft=None, **kwargs):
     if filt is None:
         return None
     if callable(filt):
+        from .filters import device_filter
+
+        try:
+            # CTFs, continuous wedges and their Compose are built on the GPU
+            return device_filter(filt, shape, return_real_fourier=True)
+        except NotImplementedError:
+            pass
         ret = filt(shape=shape, return_real_fourier=True, shape_is_real_fourier=False,
                    data_rfft=data_rfft, batch_dimension=None, **kwargs)
         return np.asarray(ret["data"], dtype=np.float32)
+    if isinstance(filt, torch.Tensor):
+        return filt.to(torch.float32)
     return np.asarray(filt, dtype=np.float32)
 
 

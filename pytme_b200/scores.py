@@ -213,13 +213,19 @@ def _setup(score: str, matching_data, fast_shape, template_filter=None, target_f
     plan = ScanPlan(score, fast_shape, tmpl.shape, precision=opts["precision"],
                     batch=opts["rotation_batch"], plain=opts["plain"])
     tf = None
-    if template_filter is not None and np.asarray(_host(template_filter)).size > 1:
-        tf = np.asarray(_host(template_filter), dtype=np.float32)
+    if template_filter is not None:
+        tf = template_filter if isinstance(template_filter, torch.Tensor) else \
+            np.asarray(_host(template_filter), dtype=np.float32)
+        n_tf = tf.numel() if isinstance(tf, torch.Tensor) else tf.size
+        if n_tf <= 1:
+            tf = None
+    if tf is not None:
         expect = (tmpl.shape[0], tmpl.shape[1], tmpl.shape[2] // 2 + 1)
-        if tf.size != int(np.prod(expect)):
+        n_tf = tf.numel() if isinstance(tf, torch.Tensor) else tf.size
+        if n_tf != int(np.prod(expect)):
             raise NotImplementedError(
-                f"template filter of shape {tf.shape} is not at the template's rfft shape "
-                f"{expect}; only pad_template_filter=False filters are supported")
+                f"template filter of shape {tuple(tf.shape)} is not at the template's rfft "
+                f"shape {expect}; only pad_template_filter=False filters are supported")
         tf = tf.reshape(expect)
     plan.set_template(tmpl, mask, tf)
     target = _prepare_target(_host(matching_data.target), tuple(fast_shape), target_filter)

@@ -20,6 +20,7 @@ mrcfile; scikit-image stubs). Its own public API then produces:
                      for every score and both ``pad_target_edges`` settings.
 * ``rigid.npz``      order-1 rigid transforms of random data (both matrix forms).
 * ``candidates.npz`` ``find_candidate_indices`` on random integer coordinates.
+* ``filters.npz``    CTF, continuous wedge and Compose arrays for ``FILTER_CASES``.
 * ``cubic.npz``      FLCSphericalMask, FLC and CC scans with ``interpolation_order=3``
                      (FP32 and FP64), and one order-3 rigid transform of data and mask.
 
@@ -119,6 +120,18 @@ def _cubic(be, create_mask, syn):
 
 
 
+def _filters():
+    """CTF / wedge / Compose arrays of FILTER_CASES from the reference."""
+    from tme.filters import Compose, CTFReconstructed, WedgeReconstructed
+    from filter_cases import FILTER_CASES, build_filter_case
+
+    out = {}
+    for i, case in enumerate(FILTER_CASES):
+        out[f"case{i}"] = np.asarray(build_filter_case(case, CTFReconstructed,
+                                                       WedgeReconstructed, Compose))
+    np.savez_compressed(os.path.join(HERE, "filters.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("PYTME_REFERENCE",
@@ -140,6 +153,10 @@ def main():
 
     if args.only == "cubic":
         _cubic(be, create_mask, syn)
+        print("golden vectors written to", HERE)
+        return
+    if args.only == "filters":
+        _filters()
         print("golden vectors written to", HERE)
         return
 
@@ -250,6 +267,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "kat_exhaustive.npz"), **kat)
 
     _cubic(be, create_mask, syn)
+    _filters()
 
     # ---- rigid transforms (order 1, constant mode), both matrix forms
     be.change_backend("numpyfftw")
