@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--step-rotations", type=int, default=1024)
     ap.add_argument("--precision", choices=("fp32", "mixed"), default="mixed")
     ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--xpass", choices=("tensor", "fft"), default="fft",
+                    help="x pass on the tensor cores or as CUDA-core FFTs")
     ap.add_argument("--plain-rotations", type=int, default=12)
     ap.add_argument("--e2e-rotations", type=int, default=0,
                     help="rotations per end-to-end call (0: the whole set)")
@@ -83,7 +85,7 @@ def make_inputs(small=False):
 # (512x512x200, 48^3 template, mixed precision, 32 rotations per group), from the ncu
 # capture summarised in profiles/xpass_flcsm_512x512x48_t48_b8.md, scaled from the
 # captured 512x512x48 / 8-rotation launch by columns and rotations.
-NCU_TRAFFIC = {("xpass", "mixed", 32): 3.91e9}
+NCU_TRAFFIC = {("xpass", "mixed", 32, "fft"): 3.91e9}
 
 
 def measured_peaks():
@@ -248,6 +250,7 @@ def run_ours(args):
 
     plan = ScanPlan("FLCSphericalMask", fast, tmpl.shape, precision=args.precision,
                     batch=args.batch)
+    plan.set_xpass(args.xpass)
     plan.set_template(t_rev, m_rev)
     tpad = torch.zeros(fast, dtype=torch.float32, device=dev)
     tpad[tuple(slice(0, s) for s in target.shape)] = torch.as_tensor(target, device=dev)
@@ -278,6 +281,7 @@ def run_ours(args):
             merge_max_argmax(smax, sarg)
         e1.record(stream)
         torch.cuda.synchronize()
+    plan.check()
     if world > 1:
         dist.barrier()
     ms = e0.elapsed_time(e1)
@@ -336,13 +340,13 @@ def run_ours(args):
             "data": "synthetic",
             "config": {"workload": WORKLOAD + ("" if not args.small else " [small]"),
                        "step_rotations": R, "rotation_batch": args.batch,
-                       "precision": args.precision,
+                       "precision": args.precision, "xpass": args.xpass,
                        "l2": "inputs larger than L2 (target spectrum 212 MB, state 420 MB)",
                        "fast_shape": list(fast), "template": [TSIZE] * 3},
             "voxel_rotations_per_s": value * float(np.prod(fast)),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": NCU_TRAFFIC.get((dom, args.precision, args.batch))
+                         "traffic": NCU_TRAFFIC.get((dom, args.precision, args.batch, args.xpass))
                          if not args.small else None,
                          "alg_bytes_per_launch": alg,
                          "avg_launch_ms": avg_ms},
@@ -413,6 +417,7 @@ def run_profile_case(args):
     target = rng.normal(size=shape).astype(np.float32)
     plan = ScanPlan("FLCSphericalMask", shape, (t,) * 3, precision=args.precision,
                     batch=args.batch)
+    plan.set_xpass(args.xpass)
     plan.set_template(tmpl[::-1, ::-1, ::-1].copy(), mask[::-1, ::-1, ::-1].copy())
     plan.set_target(torch.as_tensor(target, device="cuda"))
     rots = syn.super_fibonacci_rotations(args.batch * args.groups)

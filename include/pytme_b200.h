@@ -163,6 +163,15 @@ int tm_scan_set_target(tm_scan* plan, const float* target, void* stream);
  * the rotated mask not. Other orders return TM_E_UNSUPPORTED. Synchronous with respect
  * to `stream` only when the template is already set (it then builds the coefficients). */
 int tm_scan_set_interpolation(tm_scan* plan, int order, void* stream);
+/* x pass of the fused CC / FLCSphericalMask scan (the axis-0 transforms and the product
+ * with the target spectrum of corr_scoring, tme/matching_scores.py:610-618): mode 0 runs
+ * it on the tensor cores as a per-column circular correlation, mode 1 (the default) as
+ * forward and inverse FFTs on the CUDA cores.
+ * TM_E_UNSUPPORTED when mode 0 is not available for this plan. */
+int tm_scan_set_xpass(tm_scan* plan, int mode);
+/* Synchronise `stream`; TM_E_TIMEOUT if a bounded wait inside a tensor-core kernel of
+ * this plan gave up since the last check (the results of that run are invalid). */
+int tm_scan_check(tm_scan* plan, void* stream);
 
 /* Scores n rotations given as row-major 4x4 float32 pull matrices on the device
  * (NumpyFFTWBackend._rigid_transform_matrix of each rotation about the template
@@ -301,6 +310,12 @@ int tm_refine_backward(const tm_refine_desc* d, const float* tmpl_filtered,
                        const float* grad_rotated, const double* sums, const float* grad_scores,
                        const float* drot, double* grad_rot, double* grad_shift,
                        double* grad_angles, float* grad_tmpl, void* stream);
+
+/* Diagnostic: the tensor-core x pass alone (complex64 G [nb][t0][n1][h2] and C
+ * [n0][n1][h2] in, H [nb][n0][n1][h2] complex64 or half2 out):
+ * H[b][x'] = sum_{x<t0} scale * C[(x'-x) mod n0] * G[b][x] per column. Synchronises. */
+int tm_xcorr_tc_test(const void* G, const void* C, int nb, int t0, int n0, int n1, int h2,
+                     float scale, void* H, int half, void* stream);
 
 /* Diagnostic: `lines` complex FFTs of length n (dir -1 forward, +1 unnormalised
  * inverse) with the shared-memory line-FFT routine of the fused scan.

@@ -5,6 +5,7 @@
 #include "peaks.cuh"
 #include "refine.cuh"
 #include "scan.cuh"
+#include "xcorr_tc.cuh"
 
 #include <cufft.h>
 
@@ -218,6 +219,16 @@ int tm_scan_set_interpolation(tm_scan* plan, int order, void* stream) {
   return tmb::scan_set_interpolation(plan->impl, order, S(stream));
 }
 
+int tm_scan_set_xpass(tm_scan* plan, int mode) {
+  TM_REQUIRE(plan, "tm_scan_set_xpass: null plan");
+  return tmb::scan_set_xpass(plan->impl, mode);
+}
+
+int tm_scan_check(tm_scan* plan, void* stream) {
+  TM_REQUIRE(plan, "tm_scan_check: null plan");
+  return tmb::scan_check(plan->impl, S(stream));
+}
+
 int tm_scan_run(tm_scan* plan, const float* matrices, int n, int32_t first_index,
                 float* max_scores, int32_t* argmax, void* stream) {
   TM_REQUIRE(plan, "tm_scan_run: null plan");
@@ -254,6 +265,33 @@ int tm_find_candidate_indices(const int64_t* coords, int n, int64_t min_distance
                               int32_t* out_idx, int32_t* out_count, void* workspace,
                               void* stream) {
   return tmb::greedy_nms(coords, n, min_distance, out_idx, out_count, workspace, S(stream));
+}
+
+int tm_xcorr_tc_test(const void* G, const void* C, int nb, int t0, int n0, int n1, int h2,
+                     float scale, void* H, int half, void* stream) {
+  TM_REQUIRE(G && C && H, "tm_xcorr_tc_test: null pointer");
+  tmb::XcorrTcConfig cfg;
+  TM_TRY(tmb::xcorr_tc_config(n0, t0, nb, &cfg));
+  if (!cfg.ok) {
+    tmb::set_error("tm_xcorr_tc_test: configuration n0=%d t0=%d nb=%d not supported", n0, t0, nb);
+    return TM_E_UNSUPPORTED;
+  }
+  int* err = nullptr;
+  TM_TRY(tmb::cuda_status(cudaMalloc((void**)&err, sizeof(int)), "tm_xcorr_tc_test: alloc"));
+  cudaMemsetAsync(err, 0, sizeof(int), S(stream));
+  int st = tmb::xcorr_tc_run(cfg, (const float2*)G, (const float2*)C, nb, t0, n0, n1, h2, scale,
+                             H, half != 0, err, S(stream));
+  int herr = 0;
+  if (st == TM_OK) {
+    cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, S(stream));
+    st = tmb::cuda_status(cudaStreamSynchronize(S(stream)), "tm_xcorr_tc_test");
+  }
+  cudaFree(err);
+  if (st == TM_OK && herr) {
+    tmb::set_error("tm_xcorr_tc_test: tensor-core wait timed out");
+    st = TM_E_TIMEOUT;
+  }
+  return st;
 }
 
 int tm_line_fft_test(const void* x, void* y, int n, int lines, int dir, void* stream) {

@@ -32,6 +32,9 @@
 #include "fft_smem.cuh"
 #include "ops.cuh"
 #include "scan.cuh"
+#include "xcorr_tc.cuh"
+
+#include <type_traits>
 
 #include <cuda_fp16.h>
 #include <cufft.h>
@@ -1014,6 +1017,12 @@ struct Scan {
   int order = 1;
   double* coef = nullptr;
   double* mcoef = nullptr;
+  // tensor-core x pass (CC / FLCSphericalMask): per-column correlation kernels of the
+  // target, the launch configuration and a device error flag for its bounded waits
+  bool xtc_avail = false, xtc = false;
+  XcorrTcConfig xcfg{};
+  float2* ctarget = nullptr;
+  int* tc_err = nullptr;
   // per-group scratch
   float* rot_t = nullptr;
   float* rot_m = nullptr;
@@ -1248,6 +1257,9 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
   tmr.begin();
   if (flc) {
     TM_DISPATCH_N(s->n0, (launch_xpass_flc_reg<NN, HT>(s, nb, hs, H, stream)));
+  } else if (s->xtc) {
+    TM_TRY(xcorr_tc_run(s->xcfg, s->G, s->ctarget, nb, s->t0, s->n0, s->n1, s->h2, hs, H,
+                        std::is_same<HT, __half2>::value, s->tc_err, stream));
   } else if (s->reg0) {
     TM_DISPATCH_N(s->n0, (launch_xpass_reg<NN, HT>(s, nb, hs, H, stream)));
   } else {
@@ -1380,6 +1392,16 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     o_tw1 = take(sizeof(float2) * s->n1);
     o_tw2 = take(sizeof(float2) * s->n2);
   }
+  size_t o_ct = 0, o_err = 0;
+  if (s->fused && d.score != TM_SCORE_FLC) {
+    TM_TRY(xcorr_tc_config(s->n0, s->t0, B, &s->xcfg));
+    s->xtc_avail = s->xcfg.ok;
+    s->xtc = false;  // FFT x pass by default; tm_scan_set_xpass(plan, 0) selects this one
+  }
+  if (s->xtc_avail) {
+    o_ct = take(sizeof(float2) * s->S);
+    o_err = take(sizeof(int) * 4);
+  }
   s->bytes = off;
   cudaError_t e = cudaMalloc(&s->base, s->bytes);
   if (e != cudaSuccess) {
@@ -1418,6 +1440,11 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
       s->Hm2 = reinterpret_cast<float2*>(b8 + o_Hm2);
     }
     s->tw0 = reinterpret_cast<float2*>(b8 + o_tw0);
+    if (s->xtc_avail) {
+      s->ctarget = reinterpret_cast<float2*>(b8 + o_ct);
+      s->tc_err = reinterpret_cast<int*>(b8 + o_err);
+      cudaMemset(s->tc_err, 0, sizeof(int));
+    }
     s->tw1 = reinterpret_cast<float2*>(b8 + o_tw1);
     s->tw2 = reinterpret_cast<float2*>(b8 + o_tw2);
     auto t0v = twiddle_table(s->n0), t1v = twiddle_table(s->n1), t2v = twiddle_table(s->n2);
@@ -1492,6 +1519,8 @@ int scan_set_target(Scan* s, const float* target, cudaStream_t stream) {
     int r = cufftExecR2C(s->fwd, tmp, (cufftComplex*)s->ft_target);
     cudaFreeAsync(tmp, stream);
     TM_TRY(cufft_status((cufftResult)r, "scan_set_target: r2c"));
+    if (s->xtc_avail)
+      TM_TRY(xcorr_tc_prepare(s->ft_target, s->ctarget, s->n0, s->n1, s->h2, stream));
     s->target_ready = true;
     return check_launch("scan_set_target");
   }
@@ -1566,8 +1595,40 @@ int scan_set_target(Scan* s, const float* target, cudaStream_t stream) {
   cudaFreeAsync(centred, stream);
   cudaFreeAsync(partial, stream);
   TM_TRY(cufft_status((cufftResult)r, "scan_set_target: transforms"));
+  if (s->xtc_avail)
+    TM_TRY(xcorr_tc_prepare(s->ft_target, s->ctarget, s->n0, s->n1, s->h2, stream));
   s->target_ready = true;
   return check_launch("scan_set_target");
+}
+
+// x pass on the tensor cores (mode 0, the default where supported) or as FFTs on the
+// CUDA cores (mode 1). A captured launch-group graph is dropped.
+int scan_set_xpass(Scan* s, int mode) {
+  TM_REQUIRE(s, "scan_set_xpass: null plan");
+  TM_REQUIRE(mode == 0 || mode == 1, "scan_set_xpass: mode must be 0 (tensor cores) or 1 (FFT)");
+  const bool want = mode == 0;
+  if (want && !s->xtc_avail) {
+    set_error("scan_set_xpass: the tensor-core x pass does not support this plan");
+    return TM_E_UNSUPPORTED;
+  }
+  if (want != s->xtc && s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+  s->xtc = want;
+  return TM_OK;
+}
+
+// Synchronise `stream` and report a timed-out wait of the tensor-core x pass.
+int scan_check(Scan* s, cudaStream_t stream) {
+  TM_REQUIRE(s, "scan_check: null plan");
+  TM_TRY(cuda_status(cudaStreamSynchronize(stream), "scan_check"));
+  if (!s->tc_err) return TM_OK;
+  int h = 0;
+  TM_TRY(cuda_status(cudaMemcpy(&h, s->tc_err, sizeof(int), cudaMemcpyDeviceToHost), "scan_check"));
+  if (h) {
+    cudaMemset(s->tc_err, 0, sizeof(int));
+    set_error("scan_check: a tensor-core wait timed out");
+    return TM_E_TIMEOUT;
+  }
+  return TM_OK;
 }
 
 static int make_coefficients(Scan* s, cudaStream_t stream) {

@@ -1,0 +1,25 @@
+// Tensor-core x pass of the fused FLCSphericalMask / CC scan (xcorr_tc.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+namespace tmb {
+
+struct XcorrTcConfig {
+  bool ok;
+  int t0p, K, NB, W;
+  size_t smem;
+};
+
+// Whether the tensor-core x pass handles n0 / t0 / nb, with its launch shape.
+int xcorr_tc_config(int n0, int t0, int nb, XcorrTcConfig* cfg);
+// C = unnormalised inverse DFT along x (axis 0) of the target spectrum F [n0][n1][h2].
+int xcorr_tc_prepare(const float2* F, float2* C, int n0, int n1, int h2, cudaStream_t stream);
+// H[b][x'][k1][k2] = sum_{x<t0} scale * C[(x'-x) mod n0][k1][k2] * G[b][x][k1][k2].
+int xcorr_tc_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int nb, int t0,
+                 int n0, int n1, int h2, float scale, void* H, bool half, int* err,
+                 cudaStream_t stream);
+
+}  // namespace tmb

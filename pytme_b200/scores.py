@@ -134,6 +134,16 @@ class ScanPlan:
                                   N.ptr(max_scores), N.ptr(argmax), N.stream_ptr(stream)),
                 "tm_scan_run")
 
+    def set_xpass(self, mode: str = "tensor"):
+        """x pass on the tensor cores ("tensor") or as FFTs on the CUDA cores ("fft",
+        the default)."""
+        N.check(N.lib.tm_scan_set_xpass(self._h, 0 if mode == "tensor" else 1),
+                "tm_scan_set_xpass")
+
+    def check(self, stream=None):
+        """Synchronise and raise if a bounded wait of a tensor-core kernel gave up."""
+        N.check(N.lib.tm_scan_check(self._h, N.stream_ptr(stream)), "tm_scan_check")
+
     def set_graph(self, enable: bool = True):
         """Replay full launch groups from one captured CUDA graph."""
         N.check(N.lib.tm_scan_set_graph(self._h, int(bool(enable))), "tm_scan_set_graph")
