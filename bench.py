@@ -360,7 +360,8 @@ def run_ours(args):
     # end-to-end through the public API with host arrays (rank 0)
     if rank == 0 and not args.no_e2e:
         n_e2e = args.e2e_rotations or n_rot
-        P.backend.change_backend("b200", precision=args.precision, rotation_batch=args.batch)
+        P.backend.change_backend("b200", precision=args.precision, rotation_batch=args.batch,
+                                 xpass=args.xpass)
         setup, scoring = P.MATCHING_EXHAUSTIVE_REGISTER["FLCSphericalMask"]
         del plan, smax, sarg
         torch.cuda.empty_cache()

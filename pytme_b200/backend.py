@@ -25,7 +25,7 @@ from . import _native as N
 
 __all__ = ["B200Backend", "backend", "current_options", "fft_plan", "FFTPlan"]
 
-_DEFAULTS = {"precision": "fp32", "rotation_batch": 32, "plain": False}
+_DEFAULTS = {"precision": "fp32", "rotation_batch": 32, "plain": False, "xpass": "fft"}
 _OPTIONS = dict(_DEFAULTS)
 
 
@@ -34,11 +34,16 @@ def current_options() -> Dict:
 
 
 def _set_options(**kwargs):
+    """Options of a new backend instance: the defaults, updated by ``kwargs``."""
+    _OPTIONS.clear()
+    _OPTIONS.update(_DEFAULTS)
     for k, v in kwargs.items():
         if k in _DEFAULTS:
             _OPTIONS[k] = v
     if _OPTIONS["precision"] not in ("fp32", "mixed"):
         raise ValueError("precision must be 'fp32' or 'mixed'")
+    if _OPTIONS["xpass"] not in ("fft", "tensor"):
+        raise ValueError("xpass must be 'fft' or 'tensor'")
     _OPTIONS["rotation_batch"] = int(_OPTIONS["rotation_batch"])
     if not 1 <= _OPTIONS["rotation_batch"] <= 4096:
         raise ValueError("rotation_batch must be in [1, 4096]")

@@ -279,8 +279,8 @@ int tm_xcorr_tc_test(const void* G, const void* C, int nb, int t0, int n0, int n
   int* err = nullptr;
   TM_TRY(tmb::cuda_status(cudaMalloc((void**)&err, sizeof(int)), "tm_xcorr_tc_test: alloc"));
   cudaMemsetAsync(err, 0, sizeof(int), S(stream));
-  int st = tmb::xcorr_tc_run(cfg, (const float2*)G, (const float2*)C, nb, t0, n0, n1, h2, scale,
-                             H, half != 0, err, S(stream));
+  int st = tmb::xcorr_tc_run(cfg, (const float2*)G, (const float2*)C, nb, t0, n0, n1, h2, h2,
+                             scale, H, half != 0, err, S(stream));
   int herr = 0;
   if (st == TM_OK) {
     cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, S(stream));

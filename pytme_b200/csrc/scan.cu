@@ -174,7 +174,7 @@ template <typename HT>
 __global__ void __launch_bounds__(kThreads, 1)
 xpass_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, int B, int t0, int n0,
              int n1, int h2, int W, LinePlan p0, const float2* __restrict__ tw0_g, float scale,
-             HT* __restrict__ H) {
+             HT* __restrict__ H, int hp) {
   extern __shared__ float4 smem_raw[];
   float2* tw0 = reinterpret_cast<float2*>(smem_raw);
   float2* buf = tw0 + n0;
@@ -187,6 +187,7 @@ xpass_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, int B,
   const float2* ft_col = Ft + (int64_t)k1 * h2 + k2_0;
   const int64_t ft_row = (int64_t)n1 * h2;
   const int64_t S = (int64_t)n0 * n1 * h2;
+  const int64_t SH = (int64_t)n0 * n1 * hp;
   for (int b = 0; b < B; ++b) {
     const float2* g = G + (int64_t)b * t0 * n1 * h2;
     for (int e = tid; e < tile; e += kThreads) {
@@ -206,11 +207,11 @@ xpass_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, int B,
     }
     __syncthreads();
     fft::fft_lines<1, kMaxE, true>(buf, p0, W, 1, W, tw0, n0, tid, kThreads);
-    HT* h = H + (int64_t)b * S;
+    HT* h = H + (int64_t)b * SH;
     for (int e = tid; e < tile; e += kThreads) {
       int x = e / W, l = e % W;
       int k2 = k2_0 + l;
-      if (k2 < h2) Store<HT>::store(h + ((int64_t)x * n1 + k1) * h2 + k2, buf[e]);
+      if (k2 < h2) Store<HT>::store(h + ((int64_t)x * n1 + k1) * hp + k2, buf[e]);
     }
     __syncthreads();
   }
@@ -221,7 +222,7 @@ xpass_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, int B,
 template <typename HT>
 __global__ void __launch_bounds__(kThreads, 1)
 ypass_kernel(HT* __restrict__ H, int n0, int n1, int h2, int W, LinePlan p1,
-             const float2* __restrict__ tw1_g) {
+             const float2* __restrict__ tw1_g, int hp) {
   extern __shared__ float4 smem_raw[];
   float2* tw1 = reinterpret_cast<float2*>(smem_raw);
   float2* buf = tw1 + n1;
@@ -231,18 +232,18 @@ ypass_kernel(HT* __restrict__ H, int n0, int n1, int h2, int W, LinePlan p1,
   const int b = blockIdx.z;
   for (int i = tid; i < n1; i += kThreads) tw1[i] = tw1_g[i];
   const int tile = n1 * W;
-  HT* h = H + (int64_t)b * n0 * n1 * h2 + (int64_t)x * n1 * h2;
+  HT* h = H + (int64_t)b * n0 * n1 * hp + (int64_t)x * n1 * hp;
   for (int e = tid; e < tile; e += kThreads) {
     int y = e / W, l = e % W;
     int k2 = k2_0 + l;
-    buf[e] = (k2 < h2) ? Store<HT>::load(h + (int64_t)y * h2 + k2) : make_float2(0.f, 0.f);
+    buf[e] = (k2 < h2) ? Store<HT>::load(h + (int64_t)y * hp + k2) : make_float2(0.f, 0.f);
   }
   __syncthreads();
   fft::fft_lines<1, kMaxE, true>(buf, p1, W, 1, W, tw1, n1, tid, kThreads);
   for (int e = tid; e < tile; e += kThreads) {
     int y = e / W, l = e % W;
     int k2 = k2_0 + l;
-    if (k2 < h2) Store<HT>::store(h + (int64_t)y * h2 + k2, buf[e]);
+    if (k2 < h2) Store<HT>::store(h + (int64_t)y * hp + k2, buf[e]);
   }
 }
 
@@ -351,7 +352,7 @@ template <int N, int W, typename HT>
 __global__ void __launch_bounds__(N / 8 * W, 1024 / (N / 8 * W))
 xpass_reg_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, int B, int t0,
                  int n1, int h2, const float2* __restrict__ tw0_g, float scale,
-                 HT* __restrict__ H) {
+                 HT* __restrict__ H, int hp) {
   constexpr int T = N / 8;
   constexpr int NT = T * W;
   constexpr int R = colfft::stage_radix(N, colfft::num_stages(N) - 1);
@@ -369,7 +370,8 @@ xpass_reg_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, in
   const int64_t row = (int64_t)n1 * h2;
   const float2* fb = Ft + (int64_t)colfft::out_index<N>(t, 0, 0) * row + col;
   __syncthreads();
-  const int64_t S = (int64_t)N * n1 * h2;
+  const int64_t SH = (int64_t)N * n1 * hp, rowH = (int64_t)n1 * hp;
+  const int64_t colH = (int64_t)k1 * hp + k2;
   for (int b = 0; b < B; ++b) {
     const float2* g = G + (int64_t)b * t0 * row + col;
     float2 v[8];
@@ -393,9 +395,9 @@ xpass_reg_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, in
       }
     colfft::dif_adjoint<N, W>(v, sm, tw, l, t);
     if (valid) {
-      HT* h = H + (int64_t)b * S + col;
+      HT* h = H + (int64_t)b * SH + colH;
 #pragma unroll
-      for (int r = 0; r < 8; ++r) Store<HT>::store(h + (int64_t)(t + T * r) * row, v[r]);
+      for (int r = 0; r < 8; ++r) Store<HT>::store(h + (int64_t)(t + T * r) * rowH, v[r]);
     }
   }
 }
@@ -407,7 +409,7 @@ constexpr int kYPlanes = 4;
 
 template <int N, int W, typename HT>
 __global__ void __launch_bounds__(N / 8 * W, 1024 / (N / 8 * W))
-ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ tw1_g) {
+ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ tw1_g, int hp) {
   constexpr int T = N / 8;
   constexpr int NT = T * W;
   constexpr int R = colfft::stage_radix(N, colfft::num_stages(N) - 1);
@@ -421,12 +423,12 @@ ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ 
   const int nx = min(kYPlanes, n0 - x0);
   const bool valid = k2 < h2;
   for (int i = tid; i < N; i += NT) tw[i] = tw1_g[i];
-  HT* base = H + ((int64_t)b * n0 + x0) * N * h2 + k2;
-  const int64_t plane = (int64_t)N * h2;
+  HT* base = H + ((int64_t)b * n0 + x0) * N * hp + k2;
+  const int64_t plane = (int64_t)N * hp;
   if (valid) {
 #pragma unroll
     for (int r = 0; r < 8; ++r)
-      cp_async<sizeof(HT)>(stage + (t + T * r) * W + l, base + (int64_t)(t + T * r) * h2);
+      cp_async<sizeof(HT)>(stage + (t + T * r) * W + l, base + (int64_t)(t + T * r) * hp);
   }
   cp_async_commit();
   __syncthreads();
@@ -438,7 +440,7 @@ ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ 
         const HT* hn = base + (int64_t)(xi + 1) * plane;
 #pragma unroll
         for (int r = 0; r < 8; ++r)
-          cp_async<sizeof(HT)>(nb + (t + T * r) * W + l, hn + (int64_t)(t + T * r) * h2);
+          cp_async<sizeof(HT)>(nb + (t + T * r) * W + l, hn + (int64_t)(t + T * r) * hp);
       }
       cp_async_commit();
       cp_async_wait<1>();
@@ -458,7 +460,7 @@ ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ 
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int y = colfft::out_index<N>(t, i, r);
-          Store<HT>::store(h + (int64_t)y * h2, v[i * R + r]);
+          Store<HT>::store(h + (int64_t)y * hp, v[i * R + r]);
         }
     }
     __syncthreads();  // the next plane's stage-0 stores reuse the exchange buffer
@@ -475,7 +477,8 @@ __global__ void __launch_bounds__(N / 8 * W, 1)
 xpass_flc_reg_kernel(const float2* __restrict__ Gt, const float2* __restrict__ Gm,
                      const float2* __restrict__ Ft, const float2* __restrict__ Ft2, int B, int t0,
                      int n1, int h2, const float2* __restrict__ tw0_g, float scale,
-                     HT* __restrict__ Ht, float2* __restrict__ Hm, float2* __restrict__ Hm2) {
+                     HT* __restrict__ Ht, float2* __restrict__ Hm, float2* __restrict__ Hm2,
+                     int hp) {
   constexpr int T = N / 8;
   constexpr int NT = T * W;
   constexpr int R = colfft::stage_radix(N, colfft::num_stages(N) - 1);
@@ -496,9 +499,10 @@ xpass_flc_reg_kernel(const float2* __restrict__ Gt, const float2* __restrict__ G
       foff[i * R + r] = ((int64_t)k0 * n1 + k1) * h2 + k2;
     }
   __syncthreads();
-  const int64_t S = (int64_t)N * n1 * h2;
   const int64_t row = (int64_t)n1 * h2;
   const int64_t col = (int64_t)k1 * h2 + k2;
+  const int64_t S = (int64_t)N * n1 * hp, rowH = (int64_t)n1 * hp;
+  const int64_t colH = (int64_t)k1 * hp + k2;
   for (int b = 0; b < B; ++b) {
     // mask spectrum along axis 0
     float2 vm[8], v[8];
@@ -519,9 +523,9 @@ xpass_flc_reg_kernel(const float2* __restrict__ Gt, const float2* __restrict__ G
     }
     colfft::dif_adjoint<N, W>(v, sm, tw, l, t);
     if (valid) {
-      float2* h = Hm + (int64_t)b * S + col;
+      float2* h = Hm + (int64_t)b * S + colH;
 #pragma unroll
-      for (int r = 0; r < 8; ++r) h[(int64_t)(t + T * r) * row] = v[r];
+      for (int r = 0; r < 8; ++r) h[(int64_t)(t + T * r) * rowH] = v[r];
     }
     __syncthreads();
     // CC(f^2, m)
@@ -532,9 +536,9 @@ xpass_flc_reg_kernel(const float2* __restrict__ Gt, const float2* __restrict__ G
     }
     colfft::dif_adjoint<N, W>(v, sm, tw, l, t);
     if (valid) {
-      float2* h = Hm2 + (int64_t)b * S + col;
+      float2* h = Hm2 + (int64_t)b * S + colH;
 #pragma unroll
-      for (int r = 0; r < 8; ++r) h[(int64_t)(t + T * r) * row] = v[r];
+      for (int r = 0; r < 8; ++r) h[(int64_t)(t + T * r) * rowH] = v[r];
     }
     __syncthreads();
     // numerator CC(f, t)
@@ -554,9 +558,9 @@ xpass_flc_reg_kernel(const float2* __restrict__ Gt, const float2* __restrict__ G
     }
     colfft::dif_adjoint<N, W>(v, sm, tw, l, t);
     if (valid) {
-      HT* h = Ht + (int64_t)b * S + col;
+      HT* h = Ht + (int64_t)b * S + colH;
 #pragma unroll
-      for (int r = 0; r < 8; ++r) Store<HT>::store(h + (int64_t)(t + T * r) * row, v[r]);
+      for (int r = 0; r < 8; ++r) Store<HT>::store(h + (int64_t)(t + T * r) * rowH, v[r]);
     }
     __syncthreads();
   }
@@ -591,7 +595,7 @@ constexpr int kMaxV = 8;   // output voxels per thread
 
 template <typename HT, int M = 0>
 __global__ void __launch_bounds__(kThreads, 1)
-zpass_kernel(const HT* __restrict__ H, int B, int64_t rows, int n2, int h2, int R, LinePlan pm,
+zpass_kernel(const HT* __restrict__ H, int B, int64_t rows, int n2, int hp, int R, LinePlan pm,
              const float2* __restrict__ tw2_g, float scale, const float* __restrict__ inv_den,
              int32_t first_index, float* __restrict__ state_max, int32_t* __restrict__ state_rot,
              int64_t S, const int32_t* __restrict__ first_dev) {
@@ -600,7 +604,7 @@ zpass_kernel(const HT* __restrict__ H, int B, int64_t rows, int n2, int h2, int 
   const int m = n2 / 2;
   float2* tw2 = reinterpret_cast<float2*>(smem_raw);
   float2* raw = tw2 + n2;
-  float2* buf = raw + (int64_t)R * h2;
+  float2* buf = raw + (int64_t)R * hp;
   const int tid = threadIdx.x;
   const int64_t row0 = (int64_t)blockIdx.x * R;
   const int nrows = (int)min((int64_t)R, rows - row0);
@@ -617,12 +621,12 @@ zpass_kernel(const HT* __restrict__ H, int B, int64_t rows, int n2, int h2, int 
     arg[c] = -1;
   }
   for (int b = 0; b < B; ++b) {
-    const HT* src = H + (int64_t)b * S + row0 * h2;
-    for (int e = tid; e < nrows * h2; e += kThreads) raw[e] = Store<HT>::load(src + e);
+    const HT* src = H + (int64_t)b * S + row0 * hp;
+    for (int e = tid; e < nrows * hp; e += kThreads) raw[e] = Store<HT>::load(src + e);
     __syncthreads();
     for (int e = tid; e < nrows * m; e += kThreads) {
       int r = e / m, k = e % m;
-      const float2* xr = raw + (int64_t)r * h2;
+      const float2* xr = raw + (int64_t)r * hp;
       float2 a = xr[k], c = xr[m - k];
       if (k == 0) { a.y = 0.f; c.y = 0.f; }
       float2 cc = fft::cconj(c);
@@ -667,11 +671,11 @@ zpass_kernel(const HT* __restrict__ H, int B, int64_t rows, int n2, int h2, int 
 // rotation's own n_obs = sum(rotated mask), and the strict-> update.
 template <int M>
 __device__ __forceinline__ void c2r_rows(float2* raw, float2* buf, const float2* tw2, int nrows,
-                                         int n2, int h2, const LinePlan& pm, int tid) {
+                                         int n2, int hp, const LinePlan& pm, int tid) {
   const int m = n2 / 2;
   for (int e = tid; e < nrows * m; e += kThreads) {
     int r = e / m, k = e % m;
-    const float2* xr = raw + (int64_t)r * h2;
+    const float2* xr = raw + (int64_t)r * hp;
     float2 a = xr[k], c = xr[m - k];
     if (k == 0) { a.y = 0.f; c.y = 0.f; }
     float2 cc = fft::cconj(c);
@@ -689,7 +693,7 @@ __device__ __forceinline__ void c2r_rows(float2* raw, float2* buf, const float2*
 template <typename HT, int M = 0>
 __global__ void __launch_bounds__(kThreads, 1)
 zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
-                 const float2* __restrict__ Hm2, int B, int64_t rows, int n2, int h2, int R,
+                 const float2* __restrict__ Hm2, int B, int64_t rows, int n2, int hp, int R,
                  LinePlan pm, const float2* __restrict__ tw2_g, float scale_t, float scale_m,
                  const double* __restrict__ stats, double eps, int32_t first_index,
                  float* __restrict__ state_max, int32_t* __restrict__ state_rot, int64_t S,
@@ -699,7 +703,7 @@ zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
   const int m = n2 / 2;
   float2* tw2 = reinterpret_cast<float2*>(smem_raw);
   float2* raw = tw2 + n2;
-  float2* buf = raw + (int64_t)R * h2;
+  float2* buf = raw + (int64_t)R * hp;
   const int tid = threadIdx.x;
   const int64_t row0 = (int64_t)blockIdx.x * R;
   const int nrows = (int)min((int64_t)R, rows - row0);
@@ -715,10 +719,10 @@ zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
   for (int b = 0; b < B; ++b) {
     const double nobs = stats[b * 4 + 2];
     // local mean
-    const float2* src = Hm + (int64_t)b * S + row0 * h2;
-    for (int e = tid; e < nrows * h2; e += kThreads) raw[e] = src[e];
+    const float2* src = Hm + (int64_t)b * S + row0 * hp;
+    for (int e = tid; e < nrows * hp; e += kThreads) raw[e] = src[e];
     __syncthreads();
-    c2r_rows<M>(raw, buf, tw2, nrows, n2, h2, pm, tid);
+    c2r_rows<M>(raw, buf, tw2, nrows, n2, hp, pm, tid);
 #pragma unroll
     for (int c = 0; c < kMaxV; ++c) {
       int v = tid + c * kThreads;
@@ -726,10 +730,10 @@ zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
     }
     __syncthreads();
     // local mean square -> variance
-    src = Hm2 + (int64_t)b * S + row0 * h2;
-    for (int e = tid; e < nrows * h2; e += kThreads) raw[e] = src[e];
+    src = Hm2 + (int64_t)b * S + row0 * hp;
+    for (int e = tid; e < nrows * hp; e += kThreads) raw[e] = src[e];
     __syncthreads();
-    c2r_rows<M>(raw, buf, tw2, nrows, n2, h2, pm, tid);
+    c2r_rows<M>(raw, buf, tw2, nrows, n2, hp, pm, tid);
 #pragma unroll
     for (int c = 0; c < kMaxV; ++c) {
       int v = tid + c * kThreads;
@@ -743,10 +747,10 @@ zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
     }
     __syncthreads();
     // numerator
-    const HT* st = Ht + (int64_t)b * S + row0 * h2;
-    for (int e = tid; e < nrows * h2; e += kThreads) raw[e] = Store<HT>::load(st + e);
+    const HT* st = Ht + (int64_t)b * S + row0 * hp;
+    for (int e = tid; e < nrows * hp; e += kThreads) raw[e] = Store<HT>::load(st + e);
     __syncthreads();
-    c2r_rows<M>(raw, buf, tw2, nrows, n2, h2, pm, tid);
+    c2r_rows<M>(raw, buf, tw2, nrows, n2, hp, pm, tid);
 #pragma unroll
     for (int c = 0; c < kMaxV; ++c) {
       int v = tid + c * kThreads;
@@ -777,7 +781,7 @@ zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
 // threads are contiguous, so the state merge is coalesced.
 template <typename HT, int M1, int M2>
 __global__ void __launch_bounds__(M1 * (256 / M1), 2)
-zpass4_kernel(const HT* __restrict__ H, int B, int64_t rows, int h2,
+zpass4_kernel(const HT* __restrict__ H, int B, int64_t rows, int hp,
               const float2* __restrict__ tw2_g, float scale, const float* __restrict__ inv_den,
               int32_t first_index, float* __restrict__ state_max,
               int32_t* __restrict__ state_rot, int64_t S, const int32_t* __restrict__ first_dev) {
@@ -792,7 +796,7 @@ zpass4_kernel(const HT* __restrict__ H, int B, int64_t rows, int h2,
   extern __shared__ float4 smem_raw[];
   float2* tw = reinterpret_cast<float2*>(smem_raw);
   float2* sx = tw + N2;
-  HT* stage = reinterpret_cast<HT*>(sx + RW * PITCH);  // 2 x RW*h2 staged rows
+  HT* stage = reinterpret_cast<HT*>(sx + RW * PITCH);  // 2 x RW*hp staged rows
   const int tid = threadIdx.x;
   const int rho = tid / M1, j = tid % M1;
   for (int i = tid; i < N2; i += NT) tw[i] = tw2_g[i];
@@ -800,12 +804,12 @@ zpass4_kernel(const HT* __restrict__ H, int B, int64_t rows, int h2,
   const int nrows = (int)min((int64_t)RW, rows - row0);
   const int64_t row = row0 + rho;
   const bool active = rho < RW && rho < nrows;
-  const int nel = nrows * h2;
+  const int nel = nrows * hp;
   // rows of this CTA are contiguous in every rotation's H: stage them with cp.async,
   // one rotation ahead of the transform
   auto stage_copy = [&](int bb) {
-    const HT* src = H + (int64_t)bb * S + row0 * h2;
-    HT* dst = stage + (bb & 1) * RW * h2;
+    const HT* src = H + (int64_t)bb * S + row0 * hp;
+    HT* dst = stage + (bb & 1) * RW * hp;
     for (int e = tid; e < nel; e += NT) cp_async<sizeof(HT)>(dst + e, src + e);
     cp_async_commit();
   };
@@ -827,7 +831,7 @@ zpass4_kernel(const HT* __restrict__ H, int B, int64_t rows, int h2,
     __syncthreads();
     float2 a[M2];
     if (active) {
-      const HT* x = stage + (b & 1) * RW * h2 + rho * h2;
+      const HT* x = stage + (b & 1) * RW * hp + rho * hp;
 #pragma unroll
       for (int k2 = 0; k2 < M2; ++k2) {
         const int k = j + M1 * k2;
@@ -884,10 +888,10 @@ zpass4_kernel(const HT* __restrict__ H, int B, int64_t rows, int h2,
 }
 
 template <int M1, int M2, typename HT = float2>
-constexpr size_t zpass4_smem() {
-  // twiddles + exchange + two staged row blocks (h2 = M1*M2 + 1)
+size_t zpass4_smem(int hp) {
+  // twiddles + exchange + two staged row blocks of pitch hp (>= M1*M2 + 1)
   return sizeof(float2) * (2 * M1 * M2 + (256 / M1) * M2 * (M1 + 1)) +
-         2 * sizeof(HT) * (256 / M1) * (M1 * M2 + 1);
+         2 * sizeof(HT) * (256 / M1) * (size_t)hp;
 }
 
 // ------------------------------------------------------------------ helpers
@@ -997,6 +1001,10 @@ static unsigned grid_for(int64_t n, int threads = 256, int64_t cap = 148 * 16) {
 struct Scan {
   tm_scan_desc d{};
   int n0 = 0, n1 = 0, n2 = 0, h2 = 0, t0 = 0, t1 = 0, t2 = 0, th2 = 0;
+  // row pitch of the fused path's intermediate spectra H (and Hm, Hm2): h2 rounded up
+  // to 8 elements so rows start on 32-byte sector boundaries
+  int hp = 0;
+  int64_t SH = 0;
   int64_t N = 0, S = 0, T = 0, TS = 0;
   bool fused = false, half = false;
   int B = 1;
@@ -1101,9 +1109,9 @@ static void launch_zpass_flc(Scan* s, dim3 g4, HT* H, int nb, int64_t rows, floa
                              cudaStream_t st) {
   const double* stats = s->stats_ws + (int64_t)nb * kStatChunks * 3;
   TM_DISPATCH_M(s->n2 / 2, (zpass_flc_kernel<HT, MM><<<g4, kThreads, s->smem4, st>>>(
-                               H, s->Hm, s->Hm2, nb, rows, s->n2, s->h2, s->R4, s->pm, s->tw2,
+                               H, s->Hm, s->Hm2, nb, rows, s->n2, s->hp, s->R4, s->pm, s->tw2,
                                out_scale, out_scale, stats, 1.1920928955078125e-07, first,
-                               state_max, state_rot, s->S, s->graph_first)));
+                               state_max, state_rot, s->SH, s->graph_first)));
 }
 
 static void set_zpass_attrs(int m, int smem) {
@@ -1142,8 +1150,8 @@ static void launch_zpass4(Scan* s, HT* H, int nb, int64_t rows, float out_scale,
   TM_DISPATCH_4STEP(s->n2 / 2, ({
     constexpr int RW = 256 / A1;
     dim3 g(ceil_div(rows, RW));
-    zpass4_kernel<HT, A1, A2><<<g, A1 * RW, zpass4_smem<A1, A2, HT>(), st>>>(
-        H, nb, rows, s->h2, s->tw2, out_scale, s->inv_den, first, state_max, state_rot, s->S,
+    zpass4_kernel<HT, A1, A2><<<g, A1 * RW, zpass4_smem<A1, A2, HT>(s->hp), st>>>(
+        H, nb, rows, s->hp, s->tw2, out_scale, s->inv_den, first, state_max, state_rot, s->SH,
         s->graph_first);
   }));
 }
@@ -1163,8 +1171,8 @@ static void launch_zpass(Scan* s, dim3 g4, HT* H, int nb, int64_t rows, float ou
     return;
   }
   TM_DISPATCH_M(s->n2 / 2, (zpass_kernel<HT, MM><<<g4, kThreads, s->smem4, st>>>(
-                               H, nb, rows, s->n2, s->h2, s->R4, s->pm, s->tw2, out_scale,
-                               s->inv_den, first, state_max, state_rot, s->S, s->graph_first)));
+                               H, nb, rows, s->n2, s->hp, s->R4, s->pm, s->tw2, out_scale,
+                               s->inv_den, first, state_max, state_rot, s->SH, s->graph_first)));
 }
 
 // ---- launch helpers for the register-resident kernels
@@ -1209,7 +1217,7 @@ static void launch_xpass_flc_reg(Scan* s, int nb, float hs, HT* H, cudaStream_t 
   dim3 g(ceil_div(s->h2, W), s->n1);
   xpass_flc_reg_kernel<N, W, HT><<<g, N / 8 * W, reg_smem_bytes<N>(0, 0, 0, false), st>>>(
       s->G, s->Gm, s->ft_target, s->ft_target2, nb, s->t0, s->n1, s->h2, s->tw0, hs, H, s->Hm,
-      s->Hm2);
+      s->Hm2, s->hp);
 }
 
 template <int N, typename HT>
@@ -1217,7 +1225,7 @@ static void launch_xpass_reg(Scan* s, int nb, float hs, HT* H, cudaStream_t st) 
   constexpr int W = reg_lines<N>();
   dim3 g(ceil_div(s->h2, W), s->n1);
   xpass_reg_kernel<N, W, HT><<<g, N / 8 * W, reg_smem_bytes<N>(0, 0, 0, false), st>>>(
-      s->G, s->ft_target, nb, s->t0, s->n1, s->h2, s->tw0, hs, H);
+      s->G, s->ft_target, nb, s->t0, s->n1, s->h2, s->tw0, hs, H, s->hp);
 }
 
 template <int N, typename HT>
@@ -1225,7 +1233,7 @@ static void launch_ypass_reg(Scan* s, int nb, HT* H, cudaStream_t st) {
   constexpr int W = reg_lines<N>();
   dim3 g(ceil_div(s->h2, W), ceil_div(s->n0, kYPlanes), nb);
   ypass_reg_kernel<N, W, HT><<<g, N / 8 * W, ypass_smem_bytes<N, HT>(), st>>>(
-      H, s->n0, s->h2, s->tw1);
+      H, s->n0, s->h2, s->tw1, s->hp);
 }
 
 #define TM_DISPATCH_N(n, CALL)      \
@@ -1258,14 +1266,15 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
   if (flc) {
     TM_DISPATCH_N(s->n0, (launch_xpass_flc_reg<NN, HT>(s, nb, hs, H, stream)));
   } else if (s->xtc) {
-    TM_TRY(xcorr_tc_run(s->xcfg, s->G, s->ctarget, nb, s->t0, s->n0, s->n1, s->h2, hs, H,
-                        std::is_same<HT, __half2>::value, s->tc_err, stream));
+    TM_TRY(xcorr_tc_run(s->xcfg, s->G, s->ctarget, nb, s->t0, s->n0, s->n1, s->h2, s->hp, hs,
+                        H, std::is_same<HT, __half2>::value, s->tc_err, stream));
   } else if (s->reg0) {
     TM_DISPATCH_N(s->n0, (launch_xpass_reg<NN, HT>(s, nb, hs, H, stream)));
   } else {
     dim3 g2(ceil_div(s->h2, s->W2), s->n1);
     xpass_kernel<HT><<<g2, kThreads, s->smem2, stream>>>(s->G, s->ft_target, nb, s->t0, s->n0,
-                                                        s->n1, s->h2, s->W2, s->p0, s->tw0, hs, H);
+                                                        s->n1, s->h2, s->W2, s->p0, s->tw0, hs, H,
+                                                        s->hp);
   }
   TM_TRY(check_launch("x pass"));
   tmr.end(TM_STAGE_XPASS);
@@ -1279,7 +1288,7 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
   } else {
     dim3 g3(ceil_div(s->h2, s->W3), s->n0, nb);
     ypass_kernel<HT><<<g3, kThreads, s->smem3, stream>>>(H, s->n0, s->n1, s->h2, s->W3, s->p1,
-                                                        s->tw1);
+                                                        s->tw1, s->hp);
   }
   TM_TRY(check_launch("y pass"));
   tmr.end(TM_STAGE_YPASS);
@@ -1329,12 +1338,14 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
   s->d = d;
   s->n0 = d.fast_shape[0]; s->n1 = d.fast_shape[1]; s->n2 = d.fast_shape[2];
   s->h2 = s->n2 / 2 + 1;
+  s->hp = (s->h2 + 7) / 8 * 8;
   s->t0 = d.template_shape[0]; s->t1 = d.template_shape[1]; s->t2 = d.template_shape[2];
   s->th2 = s->t2 / 2 + 1;
   s->N = (int64_t)s->n0 * s->n1 * s->n2;
   s->S = (int64_t)s->n0 * s->n1 * s->h2;
   s->T = (int64_t)s->t0 * s->t1 * s->t2;
   s->TS = (int64_t)s->t0 * s->t1 * s->th2;
+  s->SH = (int64_t)s->n0 * s->n1 * s->hp;
   s->fused = !d.plain;
   s->half = d.precision == TM_PREC_MIXED;
   s->B = s->fused ? d.batch : 1;
@@ -1382,11 +1393,11 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     }
   } else {
     o_G = take(sizeof(float2) * (size_t)B * s->t0 * s->n1 * s->h2);
-    o_H = take((s->half ? sizeof(__half2) : sizeof(float2)) * (size_t)B * s->S);
+    o_H = take((s->half ? sizeof(__half2) : sizeof(float2)) * (size_t)B * s->SH);
     if (d.score == TM_SCORE_FLC) {
       o_Gm = take(sizeof(float2) * (size_t)B * s->t0 * s->n1 * s->h2);
-      o_Hm = take(sizeof(float2) * (size_t)B * s->S);
-      o_Hm2 = take(sizeof(float2) * (size_t)B * s->S);
+      o_Hm = take(sizeof(float2) * (size_t)B * s->SH);
+      o_Hm2 = take(sizeof(float2) * (size_t)B * s->SH);
     }
     o_tw0 = take(sizeof(float2) * s->n0);
     o_tw1 = take(sizeof(float2) * s->n1);
@@ -1462,7 +1473,7 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     s->smem1 = sizeof(float2) * (s->n1 + s->n2 + (size_t)s->n1 * s->W1) + sizeof(float) * s->t1 * s->t2;
     s->smem2 = sizeof(float2) * (s->n0 + (size_t)s->n0 * s->W2);
     s->smem3 = sizeof(float2) * (s->n1 + (size_t)s->n1 * s->W3);
-    s->smem4 = sizeof(float2) * (s->n2 + (size_t)s->R4 * s->h2 + (size_t)s->R4 * (s->n2 / 2));
+    s->smem4 = sizeof(float2) * (s->n2 + (size_t)s->R4 * s->hp + (size_t)s->R4 * (s->n2 / 2));
     size_t mx = std::max(std::max(s->smem1, s->smem2), std::max(s->smem3, s->smem4));
     if (mx > 200 * 1024) {
       set_error("scan_create: shared-memory tile of %zu bytes exceeds the limit", mx);

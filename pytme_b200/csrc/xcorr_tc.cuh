@@ -11,15 +11,20 @@ struct XcorrTcConfig {
   bool ok;
   int t0p, K, NB, W;
   size_t smem;
+  // FP16 Hankel-operand variant for half-precision outputs (n0 a multiple of 128)
+  bool hk;
+  int hk_t0p, hk_W;
+  size_t hk_smem;
 };
 
 // Whether the tensor-core x pass handles n0 / t0 / nb, with its launch shape.
 int xcorr_tc_config(int n0, int t0, int nb, XcorrTcConfig* cfg);
 // C = unnormalised inverse DFT along x (axis 0) of the target spectrum F [n0][n1][h2].
 int xcorr_tc_prepare(const float2* F, float2* C, int n0, int n1, int h2, cudaStream_t stream);
-// H[b][x'][k1][k2] = sum_{x<t0} scale * C[(x'-x) mod n0][k1][k2] * G[b][x][k1][k2].
+// H[b][x'][k1][k2] = sum_{x<t0} scale * C[(x'-x) mod n0][k1][k2] * G[b][x][k1][k2];
+// G and C have row pitch h2, H has row pitch hp >= h2.
 int xcorr_tc_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int nb, int t0,
-                 int n0, int n1, int h2, float scale, void* H, bool half, int* err,
+                 int n0, int n1, int h2, int hp, float scale, void* H, bool half, int* err,
                  cudaStream_t stream);
 
 }  // namespace tmb

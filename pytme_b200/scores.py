@@ -222,6 +222,11 @@ def _setup(score: str, matching_data, fast_shape, template_filter=None, target_f
         raise ValueError(f"{score} requires a template mask")
     plan = ScanPlan(score, fast_shape, tmpl.shape, precision=opts["precision"],
                     batch=opts["rotation_batch"], plain=opts["plain"])
+    if opts.get("xpass", "fft") == "tensor" and not plan.plain and score != "FLC":
+        try:
+            plan.set_xpass("tensor")
+        except NotImplementedError:
+            pass  # shapes the tensor-core x pass does not cover keep the FFT x pass
     tf = None
     if template_filter is not None:
         tf = template_filter if isinstance(template_filter, torch.Tensor) else \

@@ -33,11 +33,12 @@ def torch_cuda():
 
 def _scan(score, target, template, mask, rotations, precision="fp32", plain=False, batch=16,
           template_filter=None, target_filter=None, pad=False, splits=None, callback=None,
-          callback_args=None, order=1):
+          callback_args=None, order=1, xpass="fft"):
     import pytme_b200 as P
     from pytme_b200.analyzer import MaxScoreOverRotations
 
-    P.backend.change_backend("b200", precision=precision, rotation_batch=batch, plain=plain)
+    P.backend.change_backend("b200", precision=precision, rotation_batch=batch, plain=plain,
+                             xpass=xpass)
     md = P.MatchingData(target.copy(), template.copy())
     if mask is not None:
         md.template_mask = mask.copy()
@@ -409,3 +410,29 @@ def test_cubic_scan_matches_reference(torch_cuda, golden, score, precision, plai
     assert np.abs(scores - ref64).max() <= tol
     mism = np.argwhere(rot != g[f"{score}_rot32"].astype(np.int32))
     assert len(mism) <= max(1, int(1e-3 * rot.size))
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_tensor_core_xpass_matches_reference(torch_cuda, golden, precision):
+    """The tensor-core x pass in the fused FLCSphericalMask scan (config 1) against the
+    reference's FP32 and FP64 maps, with the same bounds as the FFT x pass."""
+    g = golden("c1_flcsm.npz")
+    res = _scan("FLCSphericalMask", g["target"], g["template"], g["mask"], g["rotations"],
+                precision=precision, batch=32, xpass="tensor")
+    scores, rot = np.asarray(res[0]), np.asarray(res[2])
+    tol = TOL if precision == "fp32" else mixed_tol(g["scores32"])
+    assert np.abs(scores - g["scores32"]).max() <= tol
+    assert np.abs(scores - g["scores64"]).max() <= tol
+    _assert_argmax_ties(g, rot)
+
+
+def test_tensor_core_xpass_cc_and_dc_offset(torch_cuda, golden):
+    g = golden("cc_small.npz")
+    res = _scan("CC", g["target"], g["template"], None, g["rotations"], batch=16,
+                xpass="tensor")
+    scale = max(1.0, float(np.abs(g["scores32"]).max()))
+    assert np.abs(np.asarray(res[0]) - g["scores32"]).max() <= TOL * scale
+    g = golden("flcsm_dc.npz")
+    res = _scan("FLCSphericalMask", g["target"], g["template"], g["mask"], g["rotations"],
+                batch=16, xpass="tensor")
+    assert np.abs(np.asarray(res[0]) - g["scores64"]).max() <= TOL

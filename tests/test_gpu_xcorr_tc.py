@@ -1,4 +1,4 @@
-"""The tensor-core x pass (tcgen05, TF32 with a three-way split) against a direct
+"""The tensor-core x pass (tcgen05, BF16 head/tail operands) against a direct
 evaluation of the circular correlation it computes, for each column:
 H[b][x'] = sum_{x < t0} scale * C[(x' - x) mod n0] * G[b][x]."""
 import numpy as np
@@ -22,6 +22,11 @@ def _reference(G, C, t0, scale):
     (128, 2, 7, 20, 20, False),
     (64, 2, 6, 16, 40, False),
     (128, 2, 9, 48, 32, True),
+    (128, 2, 5, 48, 128, False),
+    (64, 2, 5, 24, 100, True),
+    (256, 2, 9, 48, 32, True),
+    (512, 1, 7, 40, 64, True),
+    (256, 2, 5, 20, 120, True),
 ])
 def test_xcorr_tc_matches_direct(n0, n1, h2, t0, nb, half):
     import torch
@@ -46,4 +51,6 @@ def test_xcorr_tc_matches_direct(n0, n1, h2, t0, nb, half):
     got = got[..., 0] + 1j * got[..., 1]
     want = _reference(G.astype(np.complex128), C.astype(np.complex128), t0, scale)
     err = np.abs(got - want).max() / np.abs(want).max()
-    assert err < (2e-3 if half else 1e-5), err
+    # BF16 head + tail operands: about 16 significant bits per product; the half-output
+    # path takes FP16 operands (11 bits) and FP16 storage
+    assert err < (2e-3 if half else 5e-5), err
