@@ -51,8 +51,9 @@ def parse():
     ap.add_argument("--step-rotations", type=int, default=1024)
     ap.add_argument("--precision", choices=("fp32", "mixed"), default="mixed")
     ap.add_argument("--batch", type=int, default=32)
-    ap.add_argument("--xpass", choices=("tensor", "fft"), default="fft",
-                    help="x pass on the tensor cores or as CUDA-core FFTs")
+    ap.add_argument("--xpass", choices=("auto", "tensor", "fft"), default="auto",
+                    help="x pass on the tensor cores, as CUDA-core FFTs, or the plan default "
+                         "(tensor cores for mixed precision)")
     ap.add_argument("--plain-rotations", type=int, default=12)
     ap.add_argument("--e2e-rotations", type=int, default=0,
                     help="rotations per end-to-end call (0: the whole set)")
@@ -340,13 +341,13 @@ def run_ours(args):
             "data": "synthetic",
             "config": {"workload": WORKLOAD + ("" if not args.small else " [small]"),
                        "step_rotations": R, "rotation_batch": args.batch,
-                       "precision": args.precision, "xpass": args.xpass,
+                       "precision": args.precision, "xpass": plan.xpass,
                        "l2": "inputs larger than L2 (target spectrum 212 MB, state 420 MB)",
                        "fast_shape": list(fast), "template": [TSIZE] * 3},
             "voxel_rotations_per_s": value * float(np.prod(fast)),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": NCU_TRAFFIC.get((dom, args.precision, args.batch, args.xpass))
+                         "traffic": NCU_TRAFFIC.get((dom, args.precision, args.batch, plan.xpass))
                          if not args.small else None,
                          "alg_bytes_per_launch": alg,
                          "avg_launch_ms": avg_ms},

@@ -165,10 +165,13 @@ int tm_scan_set_target(tm_scan* plan, const float* target, void* stream);
 int tm_scan_set_interpolation(tm_scan* plan, int order, void* stream);
 /* x pass of the fused CC / FLCSphericalMask scan (the axis-0 transforms and the product
  * with the target spectrum of corr_scoring, tme/matching_scores.py:610-618): mode 0 runs
- * it on the tensor cores as a per-column circular correlation, mode 1 (the default) as
- * forward and inverse FFTs on the CUDA cores.
+ * it on the tensor cores as a per-column circular correlation, mode 1 as forward and
+ * inverse FFTs on the CUDA cores, mode 2 restores the default (tensor cores for
+ * mixed-precision plans whose x length is a multiple of 128, FFTs otherwise).
  * TM_E_UNSUPPORTED when mode 0 is not available for this plan. */
 int tm_scan_set_xpass(tm_scan* plan, int mode);
+/* The x pass the plan runs: 0 tensor cores, 1 FFT (TM_E_INVALID for a null plan). */
+int tm_scan_xpass_mode(const tm_scan* plan);
 /* Synchronise `stream`; TM_E_TIMEOUT if a bounded wait inside a tensor-core kernel of
  * this plan gave up since the last check (the results of that run are invalid). */
 int tm_scan_check(tm_scan* plan, void* stream);

@@ -224,6 +224,10 @@ int tm_scan_set_xpass(tm_scan* plan, int mode) {
   return tmb::scan_set_xpass(plan->impl, mode);
 }
 
+int tm_scan_xpass_mode(const tm_scan* plan) {
+  return plan ? tmb::scan_xpass_mode(plan->impl) : TM_E_INVALID;
+}
+
 int tm_scan_check(tm_scan* plan, void* stream) {
   TM_REQUIRE(plan, "tm_scan_check: null plan");
   return tmb::scan_check(plan->impl, S(stream));

@@ -1407,7 +1407,9 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
   if (s->fused && d.score != TM_SCORE_FLC) {
     TM_TRY(xcorr_tc_config(s->n0, s->t0, B, &s->xcfg));
     s->xtc_avail = s->xcfg.ok;
-    s->xtc = false;  // FFT x pass by default; tm_scan_set_xpass(plan, 0) selects this one
+    // default: tensor cores for half-precision spectra (the FP16 Hankel kernel), FFTs
+    // otherwise; tm_scan_set_xpass overrides
+    s->xtc = s->xtc_avail && s->half && s->xcfg.hk;
   }
   if (s->xtc_avail) {
     o_ct = take(sizeof(float2) * s->S);
@@ -1616,8 +1618,9 @@ int scan_set_target(Scan* s, const float* target, cudaStream_t stream) {
 // CUDA cores (mode 1). A captured launch-group graph is dropped.
 int scan_set_xpass(Scan* s, int mode) {
   TM_REQUIRE(s, "scan_set_xpass: null plan");
-  TM_REQUIRE(mode == 0 || mode == 1, "scan_set_xpass: mode must be 0 (tensor cores) or 1 (FFT)");
-  const bool want = mode == 0;
+  TM_REQUIRE(mode >= 0 && mode <= 2,
+             "scan_set_xpass: mode must be 0 (tensor cores), 1 (FFT) or 2 (default)");
+  const bool want = mode == 2 ? (s->xtc_avail && s->half && s->xcfg.hk) : mode == 0;
   if (want && !s->xtc_avail) {
     set_error("scan_set_xpass: the tensor-core x pass does not support this plan");
     return TM_E_UNSUPPORTED;
@@ -1626,6 +1629,8 @@ int scan_set_xpass(Scan* s, int mode) {
   s->xtc = want;
   return TM_OK;
 }
+
+int scan_xpass_mode(const Scan* s) { return s && s->xtc ? 0 : 1; }
 
 // Synchronise `stream` and report a timed-out wait of the tensor-core x pass.
 int scan_check(Scan* s, cudaStream_t stream) {

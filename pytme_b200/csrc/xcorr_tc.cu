@@ -105,6 +105,15 @@ __device__ __forceinline__ void tmem_ld8(uint32_t addr, float (&v)[8]) {
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_ld4(uint32_t addr, float (&v)[4]) {
+  uint32_t r[4];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(addr));
+#pragma unroll
+  for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 template <typename HT>
 struct StoreH;
 template <>
@@ -361,8 +370,11 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
   const int zsz = nZ * 64;                // halves per Z array
   uint16_t* zs = smem_h;                                  // [w][re|im][nZ x 64]
   uint16_t* bs = zs + (size_t)W * 2 * zsz;                // [w][NB x K]
-  float2* cst = reinterpret_cast<float2*>(bs + (size_t)W * NB * K);  // [w][n0]
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(cst + (size_t)W * n0);
+  // the kernel columns are staged in the rotation-operand region before it is filled
+  float2* cst = reinterpret_cast<float2*>(bs);            // [w][n0]
+  const size_t breg = ((size_t)W * NB * K * 2 > (size_t)W * n0 * 8 ? (size_t)W * NB * K * 2
+                                                                    : (size_t)W * n0 * 8);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(bs) + ((breg + 15) & ~(size_t)15));
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
   int* fail = reinterpret_cast<int*>(tmem_slot + 1);
 
@@ -372,9 +384,9 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
   const int64_t col0 = (int64_t)k1 * h2 + k20;
   const int64_t rowH = (int64_t)n1 * hp, colH = (int64_t)k1 * hp + k20;
   const int64_t SH = (int64_t)n0 * rowH;
-  const int blk_cols = 2 * W * NB;        // accumulator columns of one row block
+  const int blk_cols = 2 * W * NB;        // accumulator columns of one row block (<= 512)
   uint32_t tmem_cols = 32;
-  while (tmem_cols < (uint32_t)(2 * blk_cols)) tmem_cols <<= 1;
+  while (tmem_cols < (uint32_t)blk_cols) tmem_cols <<= 1;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -395,32 +407,6 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
     const int w = i / n0, m = i - w * n0;
     float2 c = (k20 + w < h2) ? C[(int64_t)m * row + col0 + w] : make_float2(0.f, 0.f);
     cst[i] = make_float2(c.x * cs, c.y * cs);
-  }
-  // rotation operands: B_w[n][k] = (Re g_n[k], Im g_n[k - t0p]) in FP16, K-major; one
-  // task = 8 consecutive x of one rotation, stored as two 16-byte rows
-  const int nxc = t0p / 8;
-  for (int i = tid; i < W * NB * nxc; i += kTcThreads) {
-    const int w = i % W;
-    const int rest = i / W;
-    const int xc = rest % nxc, n = rest / nxc;
-    uint32_t re[4], im[4];
-#pragma unroll
-    for (int q = 0; q < 8; q += 2) {
-      const int x = xc * 8 + q;
-      float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
-      if (n < nb && k20 + w < h2) {
-        if (x < t0) a = G[((int64_t)n * t0 + x) * row + col0 + w];
-        if (x + 1 < t0) b = G[((int64_t)n * t0 + x + 1) * row + col0 + w];
-      }
-      re[q >> 1] = (uint32_t)__half_as_ushort(__float2half_rn(a.x)) |
-                   ((uint32_t)__half_as_ushort(__float2half_rn(b.x)) << 16);
-      im[q >> 1] = (uint32_t)__half_as_ushort(__float2half_rn(a.y)) |
-                   ((uint32_t)__half_as_ushort(__float2half_rn(b.y)) << 16);
-    }
-    uint16_t* bw = bs + (size_t)w * NB * K;
-    *reinterpret_cast<uint4*>(bw + kmajor16(n, xc * 8, K)) = make_uint4(re[0], re[1], re[2], re[3]);
-    *reinterpret_cast<uint4*>(bw + kmajor16(n, t0p + xc * 8, K)) =
-        make_uint4(im[0], im[1], im[2], im[3]);
   }
   __syncthreads();
   // Z arrays: block u, row p = e[8u + p + q], q = 0..7, e[i] = c[(n0 - 1 - i) mod n0]
@@ -447,6 +433,33 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
     *reinterpret_cast<uint4*>(zs + (size_t)wc * zsz + (size_t)(u * 8 + p) * 8) =
         make_uint4(pk[0], pk[1], pk[2], pk[3]);
   }
+  __syncthreads();  // the staging area becomes the rotation operands
+  // rotation operands: B_w[n][k] = (Re g_n[k], Im g_n[k - t0p]) in FP16, K-major; one
+  // task = 8 consecutive x of one rotation, stored as two 16-byte rows
+  const int nxc = t0p / 8;
+  for (int i = tid; i < W * NB * nxc; i += kTcThreads) {
+    const int w = i % W;
+    const int rest = i / W;
+    const int xc = rest % nxc, n = rest / nxc;
+    uint32_t re[4], im[4];
+#pragma unroll
+    for (int q = 0; q < 8; q += 2) {
+      const int x = xc * 8 + q;
+      float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+      if (n < nb && k20 + w < h2) {
+        if (x < t0) a = G[((int64_t)n * t0 + x) * row + col0 + w];
+        if (x + 1 < t0) b = G[((int64_t)n * t0 + x + 1) * row + col0 + w];
+      }
+      re[q >> 1] = (uint32_t)__half_as_ushort(__float2half_rn(a.x)) |
+                   ((uint32_t)__half_as_ushort(__float2half_rn(b.x)) << 16);
+      im[q >> 1] = (uint32_t)__half_as_ushort(__float2half_rn(a.y)) |
+                   ((uint32_t)__half_as_ushort(__float2half_rn(b.y)) << 16);
+    }
+    uint16_t* bw = bs + (size_t)w * NB * K;
+    *reinterpret_cast<uint4*>(bw + kmajor16(n, xc * 8, K)) = make_uint4(re[0], re[1], re[2], re[3]);
+    *reinterpret_cast<uint4*>(bw + kmajor16(n, t0p + xc * 8, K)) =
+        make_uint4(im[0], im[1], im[2], im[3]);
+  }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
@@ -463,7 +476,7 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
     if (tid != 0) return;
     asm volatile("tcgen05.fence::after_thread_sync;");
     const int u0 = (n0 - kTileRows - t * kTileRows) / 8;
-    const uint32_t dbase = tmem + (uint32_t)((t & 1) * blk_cols);
+    const uint32_t dbase = tmem;
     for (int w = 0; w < W; ++w) {
       const uint32_t zr = smem_u32(zs + (size_t)(2 * w) * zsz);
       const uint32_t zi = smem_u32(zs + (size_t)(2 * w + 1) * zsz);
@@ -482,49 +495,62 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
         mma_f16(d_im, imag_g ? ar : ai, bd, idesc, s > 0);
       }
     }
-    mma_commit(smem_u32(mbar + (t & 1)));
+    mma_commit(smem_u32(mbar));
   };
 
   bool ok = true;
   const int quarter = warp & 3, half = warp >> 2;
   const float inv = 1.f / kHankelPrescale;
-  issue(0);
+  // 32-byte row segments need 8 columns per CTA and a row pitch of a multiple of 8
+  const bool vec = (W == 8) && (hp % 8 == 0);
   for (int t = 0; t < ntile && ok; ++t) {
-    if (t + 1 < ntile) issue(t + 1);  // the other accumulator half was drained at t - 1
-    if (tid == 0 && !mbar_wait(smem_u32(mbar + (t & 1)), phase[t & 1])) *fail = 1;
-    phase[t & 1] ^= 1u;
+    issue(t);
+    if (tid == 0 && !mbar_wait(smem_u32(mbar), phase[0])) *fail = 1;
+    phase[0] ^= 1u;
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (*fail) { ok = false; break; }
     const int r = quarter * 32 + lane;
     const int xp = t * kTileRows + kTileRows - 1 - r;
-    const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)((t & 1) * blk_cols);
-    for (int b0 = half * 8; b0 < NB; b0 += 16) {
-      float vr[4][8], vi[4][8];
+    const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16);
+    for (int b0 = half * 4; b0 < NB; b0 += 8) {
+      float vr[8][4], vi[8][4];
 #pragma unroll
-      for (int w = 0; w < 4; ++w)
+      for (int w = 0; w < 8; ++w)
         if (w < W) {
-          tmem_ld8(tb + (uint32_t)(w * 2 * NB + b0), vr[w]);
-          tmem_ld8(tb + (uint32_t)(w * 2 * NB + NB + b0), vi[w]);
+          tmem_ld4(tb + (uint32_t)(w * 2 * NB + b0), vr[w]);
+          tmem_ld4(tb + (uint32_t)(w * 2 * NB + NB + b0), vi[w]);
         }
       asm volatile("tcgen05.wait::ld.sync.aligned;");
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
+      for (int q = 0; q < 4; ++q) {
         const int b = b0 + q;
         if (b >= nb) break;
         __half2* h = H + (int64_t)b * SH + (int64_t)xp * rowH + colH;
+        if (vec) {
+          // eight consecutive k2 of a row (padding columns included): one aligned
+          // 32-byte segment
+          uint32_t pk[8];
 #pragma unroll
-        for (int w = 0; w < 4; ++w)
-          if (w < W && k20 + w < h2) h[w] = __floats2half2_rn(vr[w][q] * inv, vi[w][q] * inv);
+          for (int w = 0; w < 8; ++w) {
+            const __half2 hv = __floats2half2_rn(vr[w][q] * inv, vi[w][q] * inv);
+            pk[w] = *reinterpret_cast<const uint32_t*>(&hv);
+          }
+          uint4* dst = reinterpret_cast<uint4*>(h);
+          dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        } else {
+#pragma unroll
+          for (int w = 0; w < 8; ++w)
+            if (w < W && k20 + w < h2) h[w] = __floats2half2_rn(vr[w][q] * inv, vi[w][q] * inv);
+        }
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();  // this accumulator half is free for tile t + 2
+    __syncthreads();  // accumulators are free for the next row block
   }
-  if (!ok && tid == 0) {
-    for (int q = 0; q < 2; ++q) mbar_wait(smem_u32(mbar + q), phase[q]);
-  }
+  if (!ok && tid == 0) mbar_wait(smem_u32(mbar), phase[0]);
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
@@ -555,12 +581,14 @@ int xcorr_tc_config(int n0, int t0, int nb, XcorrTcConfig* cfg) {
   // Hankel variant: 128-row blocks, K steps that never straddle the Re / Im halves
   cfg->hk = false;
   cfg->hk_t0p = (t0 + 15) / 16 * 16;
-  cfg->hk_W = cfg->NB <= 32 ? 4 : (cfg->NB <= 64 ? 2 : 1);
+  // 2 * W * NB accumulator columns: (8, 32), (4, 64) or (2, 128)
+  cfg->hk_W = cfg->NB <= 32 ? 8 : (cfg->NB <= 64 ? 4 : 2);
   {
     const int K = 2 * cfg->hk_t0p;
     const int nZ = (n0 + cfg->hk_t0p) / 8 + 2;
-    cfg->hk_smem = (size_t)cfg->hk_W * ((size_t)2 * nZ * 64 * 2 + (size_t)cfg->NB * K * 2 +
-                                       (size_t)n0 * sizeof(float2)) + 32;
+    const size_t breg = std::max((size_t)cfg->hk_W * cfg->NB * K * 2,
+                                 (size_t)cfg->hk_W * n0 * sizeof(float2));
+    cfg->hk_smem = (size_t)cfg->hk_W * 2 * nZ * 64 * 2 + ((breg + 15) & ~(size_t)15) + 32;
     cfg->hk = n0 % kTileRows == 0 && cfg->hk_smem <= (size_t)optin;
   }
   if (cfg->hk)

@@ -134,11 +134,16 @@ class ScanPlan:
                                   N.ptr(max_scores), N.ptr(argmax), N.stream_ptr(stream)),
                 "tm_scan_run")
 
-    def set_xpass(self, mode: str = "tensor"):
-        """x pass on the tensor cores ("tensor") or as FFTs on the CUDA cores ("fft",
-        the default)."""
-        N.check(N.lib.tm_scan_set_xpass(self._h, 0 if mode == "tensor" else 1),
-                "tm_scan_set_xpass")
+    def set_xpass(self, mode: str = "auto"):
+        """x pass on the tensor cores ("tensor"), as FFTs on the CUDA cores ("fft"), or
+        the plan's default ("auto": tensor cores for mixed precision where supported)."""
+        code = {"tensor": 0, "fft": 1, "auto": 2}[mode]
+        N.check(N.lib.tm_scan_set_xpass(self._h, code), "tm_scan_set_xpass")
+
+    @property
+    def xpass(self) -> str:
+        """The x pass this plan runs: "tensor" or "fft"."""
+        return "tensor" if N.lib.tm_scan_xpass_mode(self._h) == 0 else "fft"
 
     def check(self, stream=None):
         """Synchronise and raise if a bounded wait of a tensor-core kernel gave up."""
@@ -222,9 +227,9 @@ def _setup(score: str, matching_data, fast_shape, template_filter=None, target_f
         raise ValueError(f"{score} requires a template mask")
     plan = ScanPlan(score, fast_shape, tmpl.shape, precision=opts["precision"],
                     batch=opts["rotation_batch"], plain=opts["plain"])
-    if opts.get("xpass", "fft") == "tensor" and not plan.plain and score != "FLC":
+    if opts.get("xpass", "auto") != "auto" and not plan.plain and score != "FLC":
         try:
-            plan.set_xpass("tensor")
+            plan.set_xpass(opts["xpass"])
         except NotImplementedError:
             pass  # shapes the tensor-core x pass does not cover keep the FFT x pass
     tf = None

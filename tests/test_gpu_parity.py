@@ -33,7 +33,7 @@ def torch_cuda():
 
 def _scan(score, target, template, mask, rotations, precision="fp32", plain=False, batch=16,
           template_filter=None, target_filter=None, pad=False, splits=None, callback=None,
-          callback_args=None, order=1, xpass="fft"):
+          callback_args=None, order=1, xpass="auto"):
     import pytme_b200 as P
     from pytme_b200.analyzer import MaxScoreOverRotations
 
