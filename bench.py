@@ -83,10 +83,11 @@ def make_inputs(small=False):
 
 
 # DRAM bytes (read + write) of one x-pass launch of the benchmark configuration
-# (512x512x200, 48^3 template, mixed precision, 32 rotations per group), from the ncu
-# capture summarised in profiles/xpass_flcsm_512x512x48_t48_b8.md, scaled from the
-# captured 512x512x48 / 8-rotation launch by columns and rotations.
-NCU_TRAFFIC = {("xpass", "mixed", 32, "fft"): 3.91e9}
+# (512x512x200, 48^3 template, mixed precision, 32 rotations per group) from ncu captures
+# of smaller launches of the same kernels, scaled by columns, rotations and row pitch:
+# profiles/xpass_flcsm_512x512x48_t48_b8.md (FFT x pass) and
+# profiles/xcorr_hankel_flcsm_512x512x48_t48_b32.md (tensor-core x pass).
+NCU_TRAFFIC = {("xpass", "mixed", 32, "fft"): 3.91e9, ("xpass", "mixed", 32, "tensor"): 4.19e9}
 
 
 def measured_peaks():
