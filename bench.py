@@ -84,9 +84,8 @@ def make_inputs(small=False):
 
 # DRAM bytes (read + write) of one x-pass launch of the benchmark configuration
 # (512x512x200, 48^3 template, mixed precision, 32 rotations per group) from ncu captures
-# of smaller launches of the same kernels, scaled by columns, rotations and row pitch:
-# profiles/xpass_flcsm_512x512x48_t48_b8.md (FFT x pass) and
-# profiles/xcorr_hankel_flcsm_512x512x48_t48_b32.md (tensor-core x pass).
+# of smaller launches of the same kernels (512x512x48 targets; the FFT x pass with 8
+# rotations, the tensor-core x pass with 32), scaled by columns, rotations and row pitch.
 NCU_TRAFFIC = {("xpass", "mixed", 32, "fft"): 3.91e9, ("xpass", "mixed", 32, "tensor"): 4.19e9}
 
 
