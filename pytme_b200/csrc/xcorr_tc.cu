@@ -359,8 +359,9 @@ __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t a, uint64_t b,
 }
 
 constexpr float kHankelPrescale = 256.f;  // keeps the scaled kernel values in FP16's normal range
+constexpr int kHkThreads = 512;
 
-__global__ void __launch_bounds__(kTcThreads, 1)
+__global__ void __launch_bounds__(kHkThreads, 1)
 xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int nb, int NB,
                     int W, int t0, int t0p, int n0, int n1, int h2, int hp, float scale,
                     __half2* __restrict__ H, int* __restrict__ err) {
@@ -370,10 +371,12 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
   const int zsz = nZ * 64;                // halves per Z array
   uint16_t* zs = smem_h;                                  // [w][re|im][nZ x 64]
   uint16_t* bs = zs + (size_t)W * 2 * zsz;                // [w][NB x K]
-  // the kernel columns are staged in the rotation-operand region before it is filled
-  float2* cst = reinterpret_cast<float2*>(bs);            // [w][n0]
-  const size_t breg = ((size_t)W * NB * K * 2 > (size_t)W * n0 * 8 ? (size_t)W * NB * K * 2
-                                                                    : (size_t)W * n0 * 8);
+  // the kernels' diagonal arrays e (FP16, [w][re|im][E2]) are staged in the
+  // rotation-operand region before it is filled
+  const int E2 = 8 * nZ + 8;
+  uint16_t* eh = bs;
+  const size_t breg = ((size_t)W * NB * K * 2 > (size_t)W * 2 * E2 * 2 ? (size_t)W * NB * K * 2
+                                                                        : (size_t)W * 2 * E2 * 2);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(bs) + ((breg + 15) & ~(size_t)15));
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
   int* fail = reinterpret_cast<int*>(tmem_slot + 1);
@@ -400,36 +403,28 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
     asm volatile("fence.mbarrier_init.release.cluster;");
     *fail = 0;
   }
-  // kernel columns, scaled
+  // diagonal arrays e[i] = s * c[(n0 - 1 - i) mod n0] in FP16, read from the kernel columns
   const float cs = scale * kHankelPrescale;
 #pragma unroll 4
-  for (int i = tid; i < W * n0; i += kTcThreads) {
-    const int w = i / n0, m = i - w * n0;
-    float2 c = (k20 + w < h2) ? C[(int64_t)m * row + col0 + w] : make_float2(0.f, 0.f);
-    cst[i] = make_float2(c.x * cs, c.y * cs);
+  for (int i = tid; i < W * E2; i += kHkThreads) {
+    const int w = i / E2, e = i - w * E2;
+    int m = n0 - 1 - e;
+    m += (m < 0) ? n0 : 0;
+    const float2 c = (k20 + w < h2) ? C[(int64_t)m * row + col0 + w] : make_float2(0.f, 0.f);
+    eh[(size_t)(2 * w) * E2 + e] = __half_as_ushort(__float2half_rn(c.x * cs));
+    eh[(size_t)(2 * w + 1) * E2 + e] = __half_as_ushort(__float2half_rn(c.y * cs));
   }
   __syncthreads();
-  // Z arrays: block u, row p = e[8u + p + q], q = 0..7, e[i] = c[(n0 - 1 - i) mod n0]
-  for (int i = tid; i < W * 2 * nZ * 8; i += kTcThreads) {
+  // Z arrays: block u, row p = e[8u + p + q], q = 0..7
+  for (int i = tid; i < W * 2 * nZ * 8; i += kHkThreads) {
     const int p = i & 7;
     const int rest = i >> 3;
     const int u = rest % nZ;
     const int wc = rest / nZ;            // w * 2 + component
-    const int w = wc >> 1, im = wc & 1;
-    const float2* cw = cst + (size_t)w * n0;
+    const uint16_t* ew = eh + (size_t)wc * E2 + 8 * u + p;
     uint32_t pk[4];
 #pragma unroll
-    for (int q = 0; q < 8; q += 2) {
-      int i0 = n0 - 1 - (8 * u + p + q);
-      i0 %= n0;
-      i0 += (i0 < 0) ? n0 : 0;
-      int i1 = i0 - 1;
-      i1 += (i1 < 0) ? n0 : 0;
-      const float v0 = im ? cw[i0].y : cw[i0].x;
-      const float v1 = im ? cw[i1].y : cw[i1].x;
-      pk[q >> 1] = (uint32_t)__half_as_ushort(__float2half_rn(v0)) |
-                   ((uint32_t)__half_as_ushort(__float2half_rn(v1)) << 16);
-    }
+    for (int q = 0; q < 8; q += 2) pk[q >> 1] = (uint32_t)ew[q] | ((uint32_t)ew[q + 1] << 16);
     *reinterpret_cast<uint4*>(zs + (size_t)wc * zsz + (size_t)(u * 8 + p) * 8) =
         make_uint4(pk[0], pk[1], pk[2], pk[3]);
   }
@@ -437,7 +432,7 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
   // rotation operands: B_w[n][k] = (Re g_n[k], Im g_n[k - t0p]) in FP16, K-major; one
   // task = 8 consecutive x of one rotation, stored as two 16-byte rows
   const int nxc = t0p / 8;
-  for (int i = tid; i < W * NB * nxc; i += kTcThreads) {
+  for (int i = tid; i < W * NB * nxc; i += kHkThreads) {
     const int w = i % W;
     const int rest = i / W;
     const int xc = rest % nxc, n = rest / nxc;
@@ -499,7 +494,9 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
   };
 
   bool ok = true;
-  const int quarter = warp & 3, half = warp >> 2;
+  // warps w and w + 4k share the accumulator lanes 32 (w mod 4) ..; the groups k split
+  // the rotations
+  const int quarter = warp & 3, grp = warp >> 2, ngrp = kHkThreads / 128;
   const float inv = 1.f / kHankelPrescale;
   // 32-byte row segments need 8 columns per CTA and a row pitch of a multiple of 8
   const bool vec = (W == 8) && (hp % 8 == 0);
@@ -514,7 +511,7 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
     const int r = quarter * 32 + lane;
     const int xp = t * kTileRows + kTileRows - 1 - r;
     const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16);
-    for (int b0 = half * 4; b0 < NB; b0 += 8) {
+    for (int b0 = grp * 4; b0 < NB; b0 += 4 * ngrp) {
       float vr[8][4], vi[8][4];
 #pragma unroll
       for (int w = 0; w < 8; ++w)
@@ -587,7 +584,7 @@ int xcorr_tc_config(int n0, int t0, int nb, XcorrTcConfig* cfg) {
     const int K = 2 * cfg->hk_t0p;
     const int nZ = (n0 + cfg->hk_t0p) / 8 + 2;
     const size_t breg = std::max((size_t)cfg->hk_W * cfg->NB * K * 2,
-                                 (size_t)cfg->hk_W * n0 * sizeof(float2));
+                                 (size_t)cfg->hk_W * 2 * (8 * nZ + 8) * 2);
     cfg->hk_smem = (size_t)cfg->hk_W * 2 * nZ * 64 * 2 + ((breg + 15) & ~(size_t)15) + 32;
     cfg->hk = n0 % kTileRows == 0 && cfg->hk_smem <= (size_t)optin;
   }
@@ -645,7 +642,7 @@ int xcorr_tc_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int
   TM_REQUIRE(nb <= cfg.NB, "xcorr_tc_run: %d rotations exceed the configured %d", nb, cfg.NB);
   if (half && cfg.hk) {
     dim3 g((unsigned)ceil_div(h2, cfg.hk_W), (unsigned)n1);
-    xcorr_hankel_kernel<<<g, kTcThreads, cfg.hk_smem, stream>>>(
+    xcorr_hankel_kernel<<<g, kHkThreads, cfg.hk_smem, stream>>>(
         G, C, nb, cfg.NB, cfg.hk_W, t0, cfg.hk_t0p, n0, n1, h2, hp, scale,
         static_cast<__half2*>(H), err);
     return check_launch("xcorr_hankel_kernel");
