@@ -371,13 +371,10 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
   const int zsz = nZ * 64;                // halves per Z array
   uint16_t* zs = smem_h;                                  // [w][re|im][nZ x 64]
   uint16_t* bs = zs + (size_t)W * 2 * zsz;                // [w][NB x K]
-  // the kernels' diagonal arrays e (FP16, [w][re|im][E2]) are staged in the
-  // rotation-operand region before it is filled
+  // the kernels' diagonal arrays e (FP16, [w][re|im][E2]) after the rotation operands
   const int E2 = 8 * nZ + 8;
-  uint16_t* eh = bs;
-  const size_t breg = ((size_t)W * NB * K * 2 > (size_t)W * 2 * E2 * 2 ? (size_t)W * NB * K * 2
-                                                                        : (size_t)W * 2 * E2 * 2);
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(bs) + ((breg + 15) & ~(size_t)15));
+  uint16_t* eh = bs + (size_t)W * NB * K;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(eh + (((size_t)W * 2 * E2 + 7) & ~(size_t)7));
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
   int* fail = reinterpret_cast<int*>(tmem_slot + 1);
 
@@ -403,6 +400,35 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
     asm volatile("fence.mbarrier_init.release.cluster;");
     *fail = 0;
   }
+  // the global loads of the rotation operands and of the kernel columns are independent:
+  // both loops run before the first barrier so their latencies overlap
+  // rotation operands: B_w[n][k] = (Re g_n[k], Im g_n[k - t0p]) in FP16, K-major; one
+  // task = 8 consecutive x of one rotation, stored as two 16-byte rows
+  const int nxc = t0p / 8;
+#pragma unroll 3
+  for (int i = tid; i < W * NB * nxc; i += kHkThreads) {
+    const int w = i % W;
+    const int rest = i / W;
+    const int xc = rest % nxc, n = rest / nxc;
+    uint32_t re[4], im[4];
+#pragma unroll
+    for (int q = 0; q < 8; q += 2) {
+      const int x = xc * 8 + q;
+      float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+      if (n < nb && k20 + w < h2) {
+        if (x < t0) a = G[((int64_t)n * t0 + x) * row + col0 + w];
+        if (x + 1 < t0) b = G[((int64_t)n * t0 + x + 1) * row + col0 + w];
+      }
+      re[q >> 1] = (uint32_t)__half_as_ushort(__float2half_rn(a.x)) |
+                   ((uint32_t)__half_as_ushort(__float2half_rn(b.x)) << 16);
+      im[q >> 1] = (uint32_t)__half_as_ushort(__float2half_rn(a.y)) |
+                   ((uint32_t)__half_as_ushort(__float2half_rn(b.y)) << 16);
+    }
+    uint16_t* bw = bs + (size_t)w * NB * K;
+    *reinterpret_cast<uint4*>(bw + kmajor16(n, xc * 8, K)) = make_uint4(re[0], re[1], re[2], re[3]);
+    *reinterpret_cast<uint4*>(bw + kmajor16(n, t0p + xc * 8, K)) =
+        make_uint4(im[0], im[1], im[2], im[3]);
+  }
   // diagonal arrays e[i] = s * c[(n0 - 1 - i) mod n0] in FP16, read from the kernel columns
   const float cs = scale * kHankelPrescale;
 #pragma unroll 4
@@ -427,33 +453,6 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
     for (int q = 0; q < 8; q += 2) pk[q >> 1] = (uint32_t)ew[q] | ((uint32_t)ew[q + 1] << 16);
     *reinterpret_cast<uint4*>(zs + (size_t)wc * zsz + (size_t)(u * 8 + p) * 8) =
         make_uint4(pk[0], pk[1], pk[2], pk[3]);
-  }
-  __syncthreads();  // the staging area becomes the rotation operands
-  // rotation operands: B_w[n][k] = (Re g_n[k], Im g_n[k - t0p]) in FP16, K-major; one
-  // task = 8 consecutive x of one rotation, stored as two 16-byte rows
-  const int nxc = t0p / 8;
-  for (int i = tid; i < W * NB * nxc; i += kHkThreads) {
-    const int w = i % W;
-    const int rest = i / W;
-    const int xc = rest % nxc, n = rest / nxc;
-    uint32_t re[4], im[4];
-#pragma unroll
-    for (int q = 0; q < 8; q += 2) {
-      const int x = xc * 8 + q;
-      float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
-      if (n < nb && k20 + w < h2) {
-        if (x < t0) a = G[((int64_t)n * t0 + x) * row + col0 + w];
-        if (x + 1 < t0) b = G[((int64_t)n * t0 + x + 1) * row + col0 + w];
-      }
-      re[q >> 1] = (uint32_t)__half_as_ushort(__float2half_rn(a.x)) |
-                   ((uint32_t)__half_as_ushort(__float2half_rn(b.x)) << 16);
-      im[q >> 1] = (uint32_t)__half_as_ushort(__float2half_rn(a.y)) |
-                   ((uint32_t)__half_as_ushort(__float2half_rn(b.y)) << 16);
-    }
-    uint16_t* bw = bs + (size_t)w * NB * K;
-    *reinterpret_cast<uint4*>(bw + kmajor16(n, xc * 8, K)) = make_uint4(re[0], re[1], re[2], re[3]);
-    *reinterpret_cast<uint4*>(bw + kmajor16(n, t0p + xc * 8, K)) =
-        make_uint4(im[0], im[1], im[2], im[3]);
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -499,7 +498,7 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
   const int quarter = warp & 3, grp = warp >> 2, ngrp = kHkThreads / 128;
   const float inv = 1.f / kHankelPrescale;
   // 32-byte row segments need 8 columns per CTA and a row pitch of a multiple of 8
-  const bool vec = (W == 8) && (hp % 8 == 0);
+  const bool vec = (W == 8 || W == 4) && (hp % 8 == 0);
   for (int t = 0; t < ntile && ok; ++t) {
     issue(t);
     if (tid == 0 && !mbar_wait(smem_u32(mbar), phase[0])) *fail = 1;
@@ -526,8 +525,7 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
         if (b >= nb) break;
         __half2* h = H + (int64_t)b * SH + (int64_t)xp * rowH + colH;
         if (vec) {
-          // eight consecutive k2 of a row (padding columns included): one aligned
-          // 32-byte segment
+          // W consecutive k2 of a row (padding columns included): aligned 16-byte stores
           uint32_t pk[8];
 #pragma unroll
           for (int w = 0; w < 8; ++w) {
@@ -536,7 +534,7 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
           }
           uint4* dst = reinterpret_cast<uint4*>(h);
           dst[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-          dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+          if (W == 8) dst[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
         } else {
 #pragma unroll
           for (int w = 0; w < 8; ++w)
@@ -583,9 +581,9 @@ int xcorr_tc_config(int n0, int t0, int nb, XcorrTcConfig* cfg) {
   {
     const int K = 2 * cfg->hk_t0p;
     const int nZ = (n0 + cfg->hk_t0p) / 8 + 2;
-    const size_t breg = std::max((size_t)cfg->hk_W * cfg->NB * K * 2,
-                                 (size_t)cfg->hk_W * 2 * (8 * nZ + 8) * 2);
-    cfg->hk_smem = (size_t)cfg->hk_W * 2 * nZ * 64 * 2 + ((breg + 15) & ~(size_t)15) + 32;
+    const size_t ereg = (((size_t)cfg->hk_W * 2 * (8 * nZ + 8) + 7) & ~(size_t)7) * 2;
+    cfg->hk_smem = (size_t)cfg->hk_W * 2 * nZ * 64 * 2 + (size_t)cfg->hk_W * cfg->NB * K * 2 +
+                   ereg + 32;
     cfg->hk = n0 % kTileRows == 0 && cfg->hk_smem <= (size_t)optin;
   }
   if (cfg->hk)
