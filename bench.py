@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--step-rotations", type=int, default=1024)
     ap.add_argument("--precision", choices=("fp32", "mixed"), default="mixed")
     ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--zpass", choices=("auto", "tensor", "fft"), default="auto",
+                    help="z pass on the tensor cores, as CUDA-core FFTs, or the plan default")
     ap.add_argument("--xpass", choices=("auto", "tensor", "fft"), default="auto",
                     help="x pass on the tensor cores, as CUDA-core FFTs, or the plan default "
                          "(tensor cores for mixed precision)")
@@ -252,6 +254,7 @@ def run_ours(args):
     plan = ScanPlan("FLCSphericalMask", fast, tmpl.shape, precision=args.precision,
                     batch=args.batch)
     plan.set_xpass(args.xpass)
+    plan.set_zpass(args.zpass)
     plan.set_template(t_rev, m_rev)
     tpad = torch.zeros(fast, dtype=torch.float32, device=dev)
     tpad[tuple(slice(0, s) for s in target.shape)] = torch.as_tensor(target, device=dev)
@@ -342,6 +345,7 @@ def run_ours(args):
             "config": {"workload": WORKLOAD + ("" if not args.small else " [small]"),
                        "step_rotations": R, "rotation_batch": args.batch,
                        "precision": args.precision, "xpass": plan.xpass,
+                       "zpass": plan.zpass,
                        "l2": "inputs larger than L2 (target spectrum 212 MB, state 420 MB)",
                        "fast_shape": list(fast), "template": [TSIZE] * 3},
             "voxel_rotations_per_s": value * float(np.prod(fast)),
@@ -362,7 +366,7 @@ def run_ours(args):
     if rank == 0 and not args.no_e2e:
         n_e2e = args.e2e_rotations or n_rot
         P.backend.change_backend("b200", precision=args.precision, rotation_batch=args.batch,
-                                 xpass=args.xpass)
+                                 xpass=args.xpass, zpass=args.zpass)
         setup, scoring = P.MATCHING_EXHAUSTIVE_REGISTER["FLCSphericalMask"]
         del plan, smax, sarg
         torch.cuda.empty_cache()
@@ -420,6 +424,7 @@ def run_profile_case(args):
     plan = ScanPlan("FLCSphericalMask", shape, (t,) * 3, precision=args.precision,
                     batch=args.batch)
     plan.set_xpass(args.xpass)
+    plan.set_zpass(args.zpass)
     plan.set_template(tmpl[::-1, ::-1, ::-1].copy(), mask[::-1, ::-1, ::-1].copy())
     plan.set_target(torch.as_tensor(target, device="cuda"))
     rots = syn.super_fibonacci_rotations(args.batch * args.groups)

@@ -172,6 +172,15 @@ int tm_scan_set_interpolation(tm_scan* plan, int order, void* stream);
 int tm_scan_set_xpass(tm_scan* plan, int mode);
 /* The x pass the plan runs: 0 tensor cores, 1 FFT (TM_E_INVALID for a null plan). */
 int tm_scan_xpass_mode(const tm_scan* plan);
+/* z pass of the fused CC / FLCSphericalMask scan (the inverse transform along axis 2,
+ * the score normalisation and the MaxScoreOverRotations update of corr_scoring,
+ * tme/matching_scores.py:618-624, and tme/analyzer/aggregation.py:142-189): mode 0 runs
+ * the c2r as a GEMM with a fixed operator on the tensor cores and reduces the maximum
+ * over the group's rotations from tensor memory (the default for mixed-precision plans
+ * with n2 <= 256 and at most 32 rotations per group), mode 1 as CUDA-core FFTs, mode 2
+ * restores the default. TM_E_UNSUPPORTED when mode 0 is not available. */
+int tm_scan_set_zpass(tm_scan* plan, int mode);
+int tm_scan_zpass_mode(const tm_scan* plan);
 /* Synchronise `stream`; TM_E_TIMEOUT if a bounded wait inside a tensor-core kernel of
  * this plan gave up since the last check (the results of that run are invalid). */
 int tm_scan_check(tm_scan* plan, void* stream);

@@ -44,7 +44,8 @@ EXPORTED = (
     "tm_euler_zyz", "tm_refine_rotate", "tm_refine_forward", "tm_refine_grad_filtered",
     "tm_refine_backward", "tm_spline_prefilter", "tm_rigid_transform_cubic",
     "tm_scan_set_interpolation", "tm_build_filter", "tm_xcorr_tc_test",
-    "tm_scan_set_xpass", "tm_scan_check", "tm_scan_xpass_mode",
+    "tm_scan_set_xpass", "tm_scan_check", "tm_scan_xpass_mode", "tm_scan_set_zpass",
+    "tm_scan_zpass_mode",
 )
 
 
@@ -132,6 +133,8 @@ def _load():
         "tm_scan_set_xpass": (c_int, [vp, c_int]),
         "tm_scan_check": (c_int, [vp, vp]),
         "tm_scan_xpass_mode": (c_int, [vp]),
+        "tm_scan_set_zpass": (c_int, [vp, c_int]),
+        "tm_scan_zpass_mode": (c_int, [vp]),
         "tm_build_filter": (c_int, [vp, c_int, POINTER(c_int), c_int, f32p, vp]),
         "tm_xcorr_tc_test": (c_int, [vp, vp, c_int, c_int, c_int, c_int, c_int, c_float, vp,
                                      c_int, vp]),

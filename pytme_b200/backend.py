@@ -25,7 +25,8 @@ from . import _native as N
 
 __all__ = ["B200Backend", "backend", "current_options", "fft_plan", "FFTPlan"]
 
-_DEFAULTS = {"precision": "fp32", "rotation_batch": 32, "plain": False, "xpass": "auto"}
+_DEFAULTS = {"precision": "fp32", "rotation_batch": 32, "plain": False, "xpass": "auto",
+             "zpass": "auto"}
 _OPTIONS = dict(_DEFAULTS)
 
 
@@ -42,8 +43,9 @@ def _set_options(**kwargs):
             _OPTIONS[k] = v
     if _OPTIONS["precision"] not in ("fp32", "mixed"):
         raise ValueError("precision must be 'fp32' or 'mixed'")
-    if _OPTIONS["xpass"] not in ("auto", "fft", "tensor"):
-        raise ValueError("xpass must be 'auto', 'fft' or 'tensor'")
+    for key in ("xpass", "zpass"):
+        if _OPTIONS[key] not in ("auto", "fft", "tensor"):
+            raise ValueError(f"{key} must be 'auto', 'fft' or 'tensor'")
     _OPTIONS["rotation_batch"] = int(_OPTIONS["rotation_batch"])
     if not 1 <= _OPTIONS["rotation_batch"] <= 4096:
         raise ValueError("rotation_batch must be in [1, 4096]")

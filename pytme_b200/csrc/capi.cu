@@ -228,6 +228,15 @@ int tm_scan_xpass_mode(const tm_scan* plan) {
   return plan ? tmb::scan_xpass_mode(plan->impl) : TM_E_INVALID;
 }
 
+int tm_scan_set_zpass(tm_scan* plan, int mode) {
+  TM_REQUIRE(plan, "tm_scan_set_zpass: null plan");
+  return tmb::scan_set_zpass(plan->impl, mode);
+}
+
+int tm_scan_zpass_mode(const tm_scan* plan) {
+  return plan ? tmb::scan_zpass_mode(plan->impl) : TM_E_INVALID;
+}
+
 int tm_scan_check(tm_scan* plan, void* stream) {
   TM_REQUIRE(plan, "tm_scan_check: null plan");
   return tmb::scan_check(plan->impl, S(stream));

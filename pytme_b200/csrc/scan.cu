@@ -33,6 +33,7 @@
 #include "ops.cuh"
 #include "scan.cuh"
 #include "xcorr_tc.cuh"
+#include "zpass_tc.cuh"
 
 #include <type_traits>
 
@@ -1031,6 +1032,10 @@ struct Scan {
   XcorrTcConfig xcfg{};
   float2* ctarget = nullptr;
   int* tc_err = nullptr;
+  // tensor-core z pass (CC / FLCSphericalMask, half-precision H): c2r operator table
+  bool ztc_avail = false, ztc = false;
+  ZpassTcConfig zcfg{};
+  uint16_t* ztable = nullptr;
   // per-group scratch
   float* rot_t = nullptr;
   float* rot_m = nullptr;
@@ -1166,6 +1171,11 @@ static void set_zpass4_attrs(int m) {
 template <typename HT>
 static void launch_zpass(Scan* s, dim3 g4, HT* H, int nb, int64_t rows, float out_scale,
                          int32_t first, float* state_max, int32_t* state_rot, cudaStream_t st) {
+  if (s->ztc && std::is_same<HT, __half2>::value) {
+    zpass_tc_run(s->zcfg, H, nb, rows, s->n2, s->h2, s->hp, s->ztable, out_scale, s->inv_den,
+                 first, state_max, state_rot, s->SH, s->graph_first, s->tc_err, st);
+    return;
+  }
   if (zpass4_supported(s->n2 / 2) && !getenv("PYTME_B200_GENERIC_FFT")) {
     launch_zpass4<HT>(s, H, nb, rows, out_scale, first, state_max, state_rot, st);
     return;
@@ -1403,7 +1413,13 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     o_tw1 = take(sizeof(float2) * s->n1);
     o_tw2 = take(sizeof(float2) * s->n2);
   }
-  size_t o_ct = 0, o_err = 0;
+  size_t o_ct = 0, o_err = 0, o_zt = 0;
+  if (s->fused && d.score != TM_SCORE_FLC && s->half) {
+    TM_TRY(zpass_tc_config(s->n2, s->h2, s->hp, B, &s->zcfg));
+    s->ztc_avail = s->zcfg.ok;
+    s->ztc = s->ztc_avail;
+    if (s->ztc_avail) o_zt = take(zpass_tc_table_bytes(s->zcfg));
+  }
   if (s->fused && d.score != TM_SCORE_FLC) {
     TM_TRY(xcorr_tc_config(s->n0, s->t0, B, &s->xcfg));
     s->xtc_avail = s->xcfg.ok;
@@ -1411,10 +1427,8 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     // otherwise; tm_scan_set_xpass overrides
     s->xtc = s->xtc_avail && s->half && s->xcfg.hk;
   }
-  if (s->xtc_avail) {
-    o_ct = take(sizeof(float2) * s->S);
-    o_err = take(sizeof(int) * 4);
-  }
+  if (s->xtc_avail) o_ct = take(sizeof(float2) * s->S);
+  if (s->xtc_avail || s->ztc_avail) o_err = take(sizeof(int) * 4);
   s->bytes = off;
   cudaError_t e = cudaMalloc(&s->base, s->bytes);
   if (e != cudaSuccess) {
@@ -1453,10 +1467,16 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
       s->Hm2 = reinterpret_cast<float2*>(b8 + o_Hm2);
     }
     s->tw0 = reinterpret_cast<float2*>(b8 + o_tw0);
-    if (s->xtc_avail) {
-      s->ctarget = reinterpret_cast<float2*>(b8 + o_ct);
+    if (s->xtc_avail) s->ctarget = reinterpret_cast<float2*>(b8 + o_ct);
+    if (s->xtc_avail || s->ztc_avail) {
       s->tc_err = reinterpret_cast<int*>(b8 + o_err);
       cudaMemset(s->tc_err, 0, sizeof(int));
+    }
+    if (s->ztc_avail) {
+      s->ztable = reinterpret_cast<uint16_t*>(b8 + o_zt);
+      int st = zpass_tc_prepare(s->zcfg, s->ztable, s->n2, s->h2, 0);
+      if (st == TM_OK) st = cuda_status(cudaDeviceSynchronize(), "scan_create: z operator");
+      if (st != TM_OK) { destroy(s); return st; }
     }
     s->tw1 = reinterpret_cast<float2*>(b8 + o_tw1);
     s->tw2 = reinterpret_cast<float2*>(b8 + o_tw2);
@@ -1631,6 +1651,24 @@ int scan_set_xpass(Scan* s, int mode) {
 }
 
 int scan_xpass_mode(const Scan* s) { return s && s->xtc ? 0 : 1; }
+
+// z pass on the tensor cores (mode 0, the default where supported: half-precision
+// CC / FLCSphericalMask plans with n2 <= 256) or as FFTs on the CUDA cores (mode 1).
+int scan_set_zpass(Scan* s, int mode) {
+  TM_REQUIRE(s, "scan_set_zpass: null plan");
+  TM_REQUIRE(mode >= 0 && mode <= 2,
+             "scan_set_zpass: mode must be 0 (tensor cores), 1 (FFT) or 2 (default)");
+  const bool want = mode == 1 ? false : (mode == 0 || s->ztc_avail);
+  if (want && !s->ztc_avail) {
+    set_error("scan_set_zpass: the tensor-core z pass does not support this plan");
+    return TM_E_UNSUPPORTED;
+  }
+  if (want != s->ztc && s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+  s->ztc = want;
+  return TM_OK;
+}
+
+int scan_zpass_mode(const Scan* s) { return s && s->ztc ? 0 : 1; }
 
 // Synchronise `stream` and report a timed-out wait of the tensor-core x pass.
 int scan_check(Scan* s, cudaStream_t stream) {

@@ -21,6 +21,8 @@ int scan_set_target(Scan* s, const float* target, cudaStream_t stream);
 int scan_set_interpolation(Scan* s, int order, cudaStream_t stream);
 int scan_set_xpass(Scan* s, int mode);
 int scan_xpass_mode(const Scan* s);
+int scan_set_zpass(Scan* s, int mode);
+int scan_zpass_mode(const Scan* s);
 int scan_check(Scan* s, cudaStream_t stream);
 int scan_run(Scan* s, const float* matrices, int n, int32_t first_index, float* state_max,
              int32_t* state_rot, cudaStream_t stream);

@@ -1,0 +1,31 @@
+// Tensor-core z pass of the fused CC / FLCSphericalMask scan (zpass_tc.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+namespace tmb {
+
+struct ZpassTcConfig {
+  bool ok;
+  int K;        // 2 * row pitch (FP16 halves per H row)
+  int n2;
+  int sms;      // persistent grid size
+  size_t smem;
+};
+
+// Whether the tensor-core z pass handles n2 / h2 / row pitch hp / nb rotations per group.
+int zpass_tc_config(int n2, int h2, int hp, int nb, ZpassTcConfig* cfg);
+size_t zpass_tc_table_bytes(const ZpassTcConfig& cfg);
+// The c2r operator table (FP16, device memory of zpass_tc_table_bytes).
+int zpass_tc_prepare(const ZpassTcConfig& cfg, uint16_t* table, int n2, int h2,
+                     cudaStream_t stream);
+// c2r of the half-precision rows of H (pitch hp) for nb rotations, scaled by
+// scale * inv_den (inv_den may be null), strict running max / argmax into the state.
+int zpass_tc_run(const ZpassTcConfig& cfg, const void* H, int nb, int64_t rows, int n2, int h2,
+                 int hp, const uint16_t* table, float scale, const float* inv_den,
+                 int32_t first_index, float* state_max, int32_t* state_rot, int64_t SH,
+                 const int32_t* first_dev, int* err, cudaStream_t stream);
+
+}  // namespace tmb

@@ -140,6 +140,17 @@ class ScanPlan:
         code = {"tensor": 0, "fft": 1, "auto": 2}[mode]
         N.check(N.lib.tm_scan_set_xpass(self._h, code), "tm_scan_set_xpass")
 
+    def set_zpass(self, mode: str = "auto"):
+        """z pass on the tensor cores ("tensor"), as FFTs on the CUDA cores ("fft"), or
+        the plan's default ("auto": tensor cores for mixed precision where supported)."""
+        code = {"tensor": 0, "fft": 1, "auto": 2}[mode]
+        N.check(N.lib.tm_scan_set_zpass(self._h, code), "tm_scan_set_zpass")
+
+    @property
+    def zpass(self) -> str:
+        """The z pass this plan runs: "tensor" or "fft"."""
+        return "tensor" if N.lib.tm_scan_zpass_mode(self._h) == 0 else "fft"
+
     @property
     def xpass(self) -> str:
         """The x pass this plan runs: "tensor" or "fft"."""
@@ -232,6 +243,11 @@ def _setup(score: str, matching_data, fast_shape, template_filter=None, target_f
             plan.set_xpass(opts["xpass"])
         except NotImplementedError:
             pass  # shapes the tensor-core x pass does not cover keep the FFT x pass
+    if opts.get("zpass", "auto") != "auto" and not plan.plain and score != "FLC":
+        try:
+            plan.set_zpass(opts["zpass"])
+        except NotImplementedError:
+            pass
     tf = None
     if template_filter is not None:
         tf = template_filter if isinstance(template_filter, torch.Tensor) else \

@@ -33,12 +33,12 @@ def torch_cuda():
 
 def _scan(score, target, template, mask, rotations, precision="fp32", plain=False, batch=16,
           template_filter=None, target_filter=None, pad=False, splits=None, callback=None,
-          callback_args=None, order=1, xpass="auto"):
+          callback_args=None, order=1, xpass="auto", zpass="auto"):
     import pytme_b200 as P
     from pytme_b200.analyzer import MaxScoreOverRotations
 
     P.backend.change_backend("b200", precision=precision, rotation_batch=batch, plain=plain,
-                             xpass=xpass)
+                             xpass=xpass, zpass=zpass)
     md = P.MatchingData(target.copy(), template.copy())
     if mask is not None:
         md.template_mask = mask.copy()
@@ -436,3 +436,18 @@ def test_tensor_core_xpass_cc_and_dc_offset(torch_cuda, golden):
     res = _scan("FLCSphericalMask", g["target"], g["template"], g["mask"], g["rotations"],
                 batch=16, xpass="tensor")
     assert np.abs(np.asarray(res[0]) - g["scores64"]).max() <= TOL
+
+
+@pytest.mark.parametrize("xpass,zpass", [("tensor", "tensor"), ("fft", "tensor"),
+                                         ("tensor", "fft")])
+def test_tensor_core_passes_mixed(torch_cuda, golden, xpass, zpass):
+    """Every combination of tensor-core and FFT x / z passes in the mixed-precision
+    FLCSphericalMask scan (config 1) against the reference's maps."""
+    g = golden("c1_flcsm.npz")
+    res = _scan("FLCSphericalMask", g["target"], g["template"], g["mask"], g["rotations"],
+                precision="mixed", batch=32, xpass=xpass, zpass=zpass)
+    scores, rot = np.asarray(res[0]), np.asarray(res[2])
+    tol = mixed_tol(g["scores32"])
+    assert np.abs(scores - g["scores32"]).max() <= tol
+    assert np.abs(scores - g["scores64"]).max() <= tol
+    _assert_argmax_ties(g, rot)
