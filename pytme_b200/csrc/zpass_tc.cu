@@ -84,8 +84,9 @@ __device__ __forceinline__ void mbar_arrive_cp_async(uint64_t* bar) {
                : "memory");
 }
 
-// Warp roles: warp 0 lane 0 issues the MMAs; warps 4-7 (one per tensor-memory lane
-// quarter) run the epilogue; warps 8-15 load operands, state and denominators. Blocks
+// Warp roles: warp 0 lane 0 issues the MMAs; warps 4-7 and 12-15 (two groups with one
+// warp per tensor-memory lane quarter) run the epilogue; warps 1-3 and 8-11 load
+// operands, state and denominators. Blocks
 // alternate between two operand buffers and two accumulator halves; mbarriers pass
 // them between the roles (no block-wide barrier inside the loop):
 //   bfull[s]  loads of the block landed               (count: loader threads)
@@ -94,7 +95,13 @@ __device__ __forceinline__ void mbar_arrive_cp_async(uint64_t* bar) {
 //             accumulator half and the buffers of parity s are free (count: epilogue
 //             threads)
 // Block j uses s = j % 2, and the u-th use of a barrier (u = j / 2) completes phase u.
-constexpr int kZLoadWarp0 = 8, kZLoaders = 256, kZEpiWarp0 = 4, kZEpi = 128;
+constexpr int kZLoaders = 224, kZEpi = 256;
+__device__ __forceinline__ bool zp_epilogue_warp(int w) { return (w & 4) != 0; }
+__device__ __forceinline__ int zp_loader_index(int tid) {
+  // warps 1-3 -> 0..95, warps 8-11 -> 96..223
+  const int w = tid >> 5;
+  return w < 4 ? tid - 32 : tid - 256 + 96;
+}
 
 __global__ void __launch_bounds__(kZThreads, 1)
 zpass_tc_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int h2, int hp,
@@ -145,9 +152,9 @@ zpass_tc_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
   const uint32_t bsa = smem_u32(Bs);
   const uint32_t bbytes = (uint32_t)kZN * (uint32_t)K * 2u;
 
-  if (warp >= kZLoadWarp0) {
+  if (warp != 0 && !zp_epilogue_warp(warp)) {
     // ---------------------------------------------------------------- loaders
-    const int lt = tid - kZLoadWarp0 * 32;
+    const int lt = zp_loader_index(tid);
     const int npa = 2 * zr * K / 8;  // the operator, with block 0
     for (int i = lt; i < npa; i += kZLoaders) cp_async16(as + 16u * i, Ag + 8 * (size_t)i, 16);
     for (int64_t j = 0; j < mine; ++j) {
@@ -212,9 +219,9 @@ zpass_tc_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
         mma_commit(smem_u32(tfull + sidx));
       }
     }
-  } else if (warp >= kZEpiWarp0 && warp < kZEpiWarp0 + 4) {
+  } else if (zp_epilogue_warp(warp)) {
     // ---------------------------------------------------------------- epilogue
-    const int quarter = warp & 3;
+    const int quarter = warp & 3, egrp = warp >> 3;
     for (int64_t j = 0; j < mine; ++j) {
       const int sidx = (int)(j & 1);
       const uint32_t u = (uint32_t)(j >> 1);
@@ -226,7 +233,7 @@ zpass_tc_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
       const float* st = sst + sidx * kZRows * n2;
       const float* dn = sden + sidx * kZRows * n2;
 #pragma unroll
-      for (int pr = 0; pr < 2 * kZRows; ++pr) {
+      for (int pr = egrp; pr < 2 * kZRows; pr += 2) {
         const int m = pr / kZRows, r = pr % kZRows;
         float v[32];
         tmem_ld32(tb + (uint32_t)(m * kZN + r * kZRot), v);
@@ -252,7 +259,6 @@ zpass_tc_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
       mbar_arrive(tempty + sidx);
     }
   }
-  // warps 1-3 have no role
   asm volatile("cp.async.wait_all;\n" ::);
   __syncthreads();
   if (*fail && tid == 0) {
