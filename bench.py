@@ -84,11 +84,13 @@ def make_inputs(small=False):
     return target, tmpl, mask, rots
 
 
-# DRAM bytes (read + write) of one x-pass launch of the benchmark configuration
+# DRAM bytes (read + write) of one launch of a pass of the benchmark configuration
 # (512x512x200, 48^3 template, mixed precision, 32 rotations per group) from ncu captures
-# of smaller launches of the same kernels (512x512x48 targets; the FFT x pass with 8
-# rotations, the tensor-core x pass with 32), scaled by columns, rotations and row pitch.
-NCU_TRAFFIC = {("xpass", "mixed", 32, "fft"): 3.91e9, ("xpass", "mixed", 32, "tensor"): 4.19e9}
+# of smaller launches of the same kernels, scaled to it: x and y passes from 512x512x48
+# targets (by columns, rotations and row pitch), the z pass from a 256x256x200 target (by
+# rows). Keyed by (pass, precision, rotations per group, variant of the pass).
+NCU_TRAFFIC = {("xpass", "mixed", 32, "fft"): 3.91e9, ("xpass", "mixed", 32, "tensor"): 4.18e9,
+               ("ypass", "mixed", 32, "fft"): 6.81e9, ("zpass", "mixed", 32, "tensor"): 4.31e9}
 
 
 def measured_peaks():
@@ -351,7 +353,9 @@ def run_ours(args):
             "voxel_rotations_per_s": value * float(np.prod(fast)),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": NCU_TRAFFIC.get((dom, args.precision, args.batch, plan.xpass))
+                         "traffic": NCU_TRAFFIC.get((dom, args.precision, args.batch,
+                                                     {"xpass": plan.xpass, "zpass": plan.zpass}
+                                                     .get(dom, "fft")))
                          if not args.small else None,
                          "alg_bytes_per_launch": alg,
                          "avg_launch_ms": avg_ms},

@@ -289,16 +289,33 @@ int tm_xcorr_tc_test(const void* G, const void* C, int nb, int t0, int n0, int n
     tmb::set_error("tm_xcorr_tc_test: configuration n0=%d t0=%d nb=%d not supported", n0, t0, nb);
     return TM_E_UNSUPPORTED;
   }
+  // the scan's layout: output rows padded to a multiple of 8 elements, then copied to the
+  // caller's unpadded rows
+  const int hp = (h2 + 7) / 8 * 8;
+  const size_t esz = half ? 4 : 8;
+  const size_t rows = (size_t)nb * n0 * n1;
   int* err = nullptr;
+  void* Hp = nullptr;
   TM_TRY(tmb::cuda_status(cudaMalloc((void**)&err, sizeof(int)), "tm_xcorr_tc_test: alloc"));
+  if (cudaMalloc(&Hp, rows * hp * esz) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(err);
+    tmb::set_error("tm_xcorr_tc_test: out of device memory");
+    return TM_E_OOM;
+  }
   cudaMemsetAsync(err, 0, sizeof(int), S(stream));
-  int st = tmb::xcorr_tc_run(cfg, (const float2*)G, (const float2*)C, nb, t0, n0, n1, h2, h2,
-                             scale, H, half != 0, err, S(stream));
+  int st = tmb::xcorr_tc_run(cfg, (const float2*)G, (const float2*)C, nb, t0, n0, n1, h2, hp,
+                             scale, Hp, half != 0, err, S(stream));
   int herr = 0;
+  if (st == TM_OK)
+    st = tmb::cuda_status(cudaMemcpy2DAsync(H, h2 * esz, Hp, hp * esz, h2 * esz, rows,
+                                            cudaMemcpyDeviceToDevice, S(stream)),
+                          "tm_xcorr_tc_test: copy");
   if (st == TM_OK) {
     cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, S(stream));
     st = tmb::cuda_status(cudaStreamSynchronize(S(stream)), "tm_xcorr_tc_test");
   }
+  cudaFree(Hp);
   cudaFree(err);
   if (st == TM_OK && herr) {
     tmb::set_error("tm_xcorr_tc_test: tensor-core wait timed out");

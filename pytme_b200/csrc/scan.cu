@@ -405,8 +405,12 @@ xpass_reg_kernel(const float2* __restrict__ G, const float2* __restrict__ Ft, in
 
 // K3': y pass (inverse FFT along axis 1, in place). grid (ceil(h2/W), ceil(n0/XP), B);
 // each CTA walks XP consecutive x planes; the next plane's columns are staged in shared
-// memory with cp.async while the current plane is transformed. N = n1.
-constexpr int kYPlanes = 4;
+// memory with cp.async while the current plane is transformed (each thread stages and
+// later reads only its own elements, so a stage is reused without a barrier). The pass
+// is bound by instruction issue and shared-memory traffic, not by loads in flight:
+// three or four staged planes measured slower than two. N = n1.
+constexpr int kYPlanes = 8;
+constexpr int kYStages = 2;
 
 template <int N, int W, typename HT>
 __global__ void __launch_bounds__(N / 8 * W, 1024 / (N / 8 * W))
@@ -417,7 +421,7 @@ ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ 
   extern __shared__ float4 smem_raw[];
   float2* tw = reinterpret_cast<float2*>(smem_raw);
   float2* sm = tw + N;
-  HT* stage = reinterpret_cast<HT*>(sm + colfft::smem_elems<N>(W));  // 2 x N*W staging
+  HT* stage = reinterpret_cast<HT*>(sm + colfft::smem_elems<N>(W));  // kYStages x N*W staging
   const int tid = threadIdx.x, l = tid % W, t = tid / W;
   const int k2 = blockIdx.x * W + l;
   const int x0 = blockIdx.y * kYPlanes, b = blockIdx.z;
@@ -426,28 +430,23 @@ ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ 
   for (int i = tid; i < N; i += NT) tw[i] = tw1_g[i];
   HT* base = H + ((int64_t)b * n0 + x0) * N * hp + k2;
   const int64_t plane = (int64_t)N * hp;
-  if (valid) {
+  auto fetch = [&](int xi) {
+    if (valid && xi < nx) {
+      HT* dst = stage + (xi % kYStages) * N * W;
+      const HT* src = base + (int64_t)xi * plane;
 #pragma unroll
-    for (int r = 0; r < 8; ++r)
-      cp_async<sizeof(HT)>(stage + (t + T * r) * W + l, base + (int64_t)(t + T * r) * hp);
-  }
-  cp_async_commit();
-  __syncthreads();
-  for (int xi = 0; xi < nx; ++xi) {
-    HT* cur = stage + (xi & 1) * N * W;
-    if (xi + 1 < nx) {
-      HT* nb = stage + ((xi + 1) & 1) * N * W;
-      if (valid) {
-        const HT* hn = base + (int64_t)(xi + 1) * plane;
-#pragma unroll
-        for (int r = 0; r < 8; ++r)
-          cp_async<sizeof(HT)>(nb + (t + T * r) * W + l, hn + (int64_t)(t + T * r) * hp);
-      }
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+      for (int r = 0; r < 8; ++r)
+        cp_async<sizeof(HT)>(dst + (t + T * r) * W + l, src + (int64_t)(t + T * r) * hp);
     }
+    cp_async_commit();  // one group per plane, empty past the last
+  };
+#pragma unroll
+  for (int xi = 0; xi < kYStages - 1; ++xi) fetch(xi);
+  __syncthreads();  // twiddles
+  for (int xi = 0; xi < nx; ++xi) {
+    HT* cur = stage + (xi % kYStages) * N * W;
+    fetch(xi + kYStages - 1);
+    cp_async_wait<kYStages - 1>();  // plane xi landed
     float2 v[8];
 #pragma unroll
     for (int r = 0; r < 8; ++r)
@@ -579,7 +578,7 @@ size_t reg_smem_bytes(int n2, int t1, int t2, bool with_plane) {
 
 template <int N, typename HT>
 size_t ypass_smem_bytes() {
-  return reg_smem_bytes<N>(0, 0, 0, false) + 2 * sizeof(HT) * N * reg_lines<N>();
+  return reg_smem_bytes<N>(0, 0, 0, false) + kYStages * sizeof(HT) * N * reg_lines<N>();
 }
 
 static bool reg_supported(int n) {
@@ -1422,10 +1421,10 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
   }
   if (s->fused && d.score != TM_SCORE_FLC) {
     TM_TRY(xcorr_tc_config(s->n0, s->t0, B, &s->xcfg));
-    s->xtc_avail = s->xcfg.ok;
-    // default: tensor cores for half-precision spectra (the FP16 Hankel kernel), FFTs
+    s->xtc_avail = s->xcfg.ok || (s->half && s->xcfg.ws);
+    // default: tensor cores for half-precision spectra (the FP16 Hankel kernels), FFTs
     // otherwise; tm_scan_set_xpass overrides
-    s->xtc = s->xtc_avail && s->half && s->xcfg.hk;
+    s->xtc = s->xtc_avail && s->half && (s->xcfg.hk || s->xcfg.ws);
   }
   if (s->xtc_avail) o_ct = take(sizeof(float2) * s->S);
   if (s->xtc_avail || s->ztc_avail) o_err = take(sizeof(int) * 4);
@@ -1640,7 +1639,8 @@ int scan_set_xpass(Scan* s, int mode) {
   TM_REQUIRE(s, "scan_set_xpass: null plan");
   TM_REQUIRE(mode >= 0 && mode <= 2,
              "scan_set_xpass: mode must be 0 (tensor cores), 1 (FFT) or 2 (default)");
-  const bool want = mode == 2 ? (s->xtc_avail && s->half && s->xcfg.hk) : mode == 0;
+  const bool want =
+      mode == 2 ? (s->xtc_avail && s->half && (s->xcfg.hk || s->xcfg.ws)) : mode == 0;
   if (want && !s->xtc_avail) {
     set_error("scan_set_xpass: the tensor-core x pass does not support this plan");
     return TM_E_UNSUPPORTED;

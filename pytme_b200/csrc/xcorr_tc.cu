@@ -558,10 +558,13 @@ xcorr_hankel_kernel(const float2* __restrict__ G, const float2* __restrict__ C, 
 
 int xcorr_tc_config(int n0, int t0, int nb, XcorrTcConfig* cfg) {
   cfg->ok = false;
+  cfg->hk = false;
+  TM_TRY(xcorr_ws_config(n0, t0, nb, cfg));
   if (n0 % 64 != 0 || nb < 1) return TM_OK;
   cfg->t0p = (t0 + 7) / 8 * 8;
   cfg->K = 2 * cfg->t0p;
-  cfg->NB = (nb + 7) / 8 * 8;
+  // with M = 128, kind::f16 takes N in steps of 16
+  cfg->NB = (nb + 15) / 16 * 16;
   if (cfg->NB > 128) return TM_OK;
   // W * NB accumulator columns per row block, two blocks in the 512 tensor-memory columns
   cfg->W = cfg->NB <= 32 ? 4 : 2;
@@ -636,6 +639,9 @@ static int launch_xcorr(const XcorrTcConfig& cfg, const float2* G, const float2*
 int xcorr_tc_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int nb, int t0,
                  int n0, int n1, int h2, int hp, float scale, void* H, bool half, int* err,
                  cudaStream_t stream) {
+  if (half && cfg.ws && nb <= cfg.ws_NB && hp % 8 == 0)
+    return xcorr_ws_run(cfg, G, C, nb, t0, n0, n1, h2, hp, scale, static_cast<__half2*>(H), err,
+                        stream);
   TM_REQUIRE(cfg.ok, "xcorr_tc_run: unsupported configuration");
   TM_REQUIRE(nb <= cfg.NB, "xcorr_tc_run: %d rotations exceed the configured %d", nb, cfg.NB);
   if (half && cfg.hk) {

@@ -1,6 +1,7 @@
 // Tensor-core x pass of the fused FLCSphericalMask / CC scan (xcorr_tc.cu).
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
@@ -15,10 +16,20 @@ struct XcorrTcConfig {
   bool hk;
   int hk_t0p, hk_W;
   size_t hk_smem;
+  // persistent warp-specialised FP16 variant (xcorr_ws.cu): at most 32 rotations per
+  // group, t0 <= 64, n0 a multiple of 128, output row pitch a multiple of 8
+  bool ws;
+  int ws_t0p, ws_NB, sms;
+  size_t ws_smem;
 };
 
 // Whether the tensor-core x pass handles n0 / t0 / nb, with its launch shape.
 int xcorr_tc_config(int n0, int t0, int nb, XcorrTcConfig* cfg);
+// Fills the ws fields of cfg (called by xcorr_tc_config).
+int xcorr_ws_config(int n0, int t0, int nb, XcorrTcConfig* cfg);
+int xcorr_ws_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int nb, int t0,
+                 int n0, int n1, int h2, int hp, float scale, __half2* H, int* err,
+                 cudaStream_t stream);
 // C = unnormalised inverse DFT along x (axis 0) of the target spectrum F [n0][n1][h2].
 int xcorr_tc_prepare(const float2* F, float2* C, int n0, int n1, int h2, cudaStream_t stream);
 // H[b][x'][k1][k2] = sum_{x<t0} scale * C[(x'-x) mod n0][k1][k2] * G[b][x][k1][k2];

@@ -1,4 +1,5 @@
-"""The tensor-core x pass (tcgen05, BF16 head/tail operands) against a direct
+"""The tensor-core x pass (tcgen05; BF16 head/tail operands for FP32 output, FP16
+Hankel operands for half output) against a direct
 evaluation of the circular correlation it computes, for each column:
 H[b][x'] = sum_{x < t0} scale * C[(x' - x) mod n0] * G[b][x]."""
 import numpy as np
@@ -27,6 +28,12 @@ def _reference(G, C, t0, scale):
     (256, 2, 9, 48, 32, True),
     (512, 1, 7, 40, 64, True),
     (256, 2, 5, 20, 120, True),
+    # persistent warp-specialised kernel: several items per CTA, both operand buffers
+    # reused, 16- and 32-rotation groups, t0 up to 64
+    (128, 40, 65, 48, 32, True),
+    (256, 40, 33, 20, 7, True),
+    (512, 16, 24, 64, 16, True),
+    (384, 12, 101, 48, 29, True),
 ])
 def test_xcorr_tc_matches_direct(n0, n1, h2, t0, nb, half):
     import torch
