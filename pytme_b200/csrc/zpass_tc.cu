@@ -273,24 +273,383 @@ zpass_tc_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
   if (tid == 0 && *fail) atomicExch(err, 1);
 }
 
+
+// ---------------------------------------------------------------------------------
+// Even/odd variant. With E[z] = sum_k w_k Re X[k] cos(2 pi k z/n2) and
+// O[z] = -sum_k w_k Im X[k] sin(2 pi k z/n2) (w_k = 1 for k = 0 and k = n2/2, else 2),
+//     x[z] = E[z] + O[z],   x[n2 - z] = E[z] - O[z],
+// so z <= n2/2 (one M = 128 tile, n2/2 + 1 <= 128) and K' = h2 rounded up to 16 per GEMM
+// give all n2 outputs: two GEMMs with half the K of the interleaved operator, a quarter
+// of the MMAs of the two-tile form for the same outputs. The rotation operand holds each
+// H row de-interleaved, [Re X[0..K') | Im X[0..K')] (the loaders split the FP16 complex
+// values in registers). Blocks are 4 rows x 32 rotations (N = 128); the E and O
+// accumulators of a block take 256 tensor-memory columns, two blocks in flight.
+constexpr int kEoRows = 4;
+constexpr int kEoN = kEoRows * kZRot;  // 128
+
+__host__ __device__ inline int eo_rows(int n2) { return (n2 / 2 + 1 + 7) / 8 * 8; }
+
+// [C head | C tail | S head | S tail], each zr x K' in the canonical K-major layout:
+// C[z][k] = w_k cos(2 pi k z/n2), S[z][k] = -w_k sin(2 pi k z/n2) for z <= n2/2, k < h2.
+__global__ void eo_table_kernel(uint16_t* __restrict__ A, int n2, int h2, int Kp) {
+  const int zr = eo_rows(n2);
+  const int total = zr * Kp;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const int z = i / Kp, k = i - z * Kp;
+    float c = 0.f, s = 0.f;
+    if (z <= n2 / 2 && k < h2) {
+      const double w = (k == 0 || 2 * k == n2) ? 1.0 : 2.0;
+      const long long kz = ((long long)k * z) % n2;
+      double sn, cs;
+      sincospi(2.0 * (double)kz / (double)n2, &sn, &cs);
+      c = (float)(w * cs);
+      s = (float)(-w * sn);
+    }
+    const size_t tab = (size_t)zr * Kp;
+    const int o = kmajor16(z, k, Kp);
+    const __half ch = __float2half_rn(c), sh = __float2half_rn(s);
+    A[o] = __half_as_ushort(ch);
+    A[tab + o] = __half_as_ushort(__float2half_rn(c - __half2float(ch)));
+    A[2 * tab + o] = __half_as_ushort(sh);
+    A[3 * tab + o] = __half_as_ushort(__float2half_rn(s - __half2float(sh)));
+  }
+}
+
+// tcgen05.mma with the shared-memory descriptors given as (low, high) words: the low
+// word holds the start address >> 4 and the leading byte offset, so operands are
+// advanced by adding byte offsets >> 4 to it (addresses stay below 256 KB)
+__device__ __forceinline__ void mma_f16_w(uint32_t tmem_d, uint32_t alo, uint32_t ahi,
+                                          uint32_t blo, uint32_t bhi, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t.reg .b64 a, b;\n\t"
+      "setp.ne.b32 p, %6, 0;\n\t"
+      "mov.b64 a, {%1, %2};\n\t"
+      "mov.b64 b, {%3, %4};\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], a, b, %5, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "r"(alo), "r"(ahi), "r"(blo), "r"(bhi), "r"(idesc), "r"(accumulate));
+}
+// the barrier's phase also waits for this thread's earlier cp.async copies (net zero on
+// the expected count: the thread arrives separately)
+__device__ __forceinline__ void mbar_track_cp_async(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.shared::cta.b64 [%0];" : : "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Roles as in zpass_tc_kernel. Barriers per buffer s:
+//   bfull[s]   operands of the block stored, its state and denominators landed
+//              (count: loader threads; their cp.async completion tracked as well)
+//   bempty[s]  MMAs of the block done: its rotation-operand buffer is free (commit)
+//   tfull[s]   accumulators of the block written (commit)
+//   tempty[s]  epilogue done: accumulators and state buffers free (count: epilogue)
+// MT: loader tasks per thread, ceil(512 * ceil(ceil(h2 / 4) / 4) / kZLoaders).
+template <int MT>
+__global__ void __launch_bounds__(kZThreads, 1)
+zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int h2, int hp,
+                int Kp, const uint16_t* __restrict__ Ag, float scale,
+                const float* __restrict__ inv_den, int32_t first_index,
+                float* __restrict__ state_max, int32_t* __restrict__ state_rot, int64_t SH,
+                const int32_t* __restrict__ first_dev, int* __restrict__ err) {
+  if (first_dev) first_index = *first_dev;
+  extern __shared__ __align__(128) uint16_t smem_e[];
+  const int zr = eo_rows(n2);
+  const int K2 = 2 * Kp;                          // rotation-operand K: Re block, Im block
+  const size_t tab = (size_t)zr * Kp;             // halves per operator table
+  uint16_t* As = smem_e;                          // 4 tables
+  uint16_t* Bs = As + 4 * tab;                    // 2 buffers x [kEoN x K2]
+  float* sst = reinterpret_cast<float*>(Bs + (size_t)2 * kEoN * K2);  // 2 x [kEoRows x n2]
+  float* sden = sst + 2 * kEoRows * n2;                               // 2 x [kEoRows x n2]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sden + 2 * kEoRows * n2);
+  uint64_t* bfull = bar;
+  uint64_t* bempty = bar + 2;
+  uint64_t* tfull = bar + 4;
+  uint64_t* tempty = bar + 6;
+  uint64_t* mdone = bar + 8;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 9);
+  int* fail = reinterpret_cast<int*>(tmem_slot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :
+                 : "r"(smem_u32(tmem_slot)), "r"(4 * kEoN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  // zero both rotation-operand buffers once: K positions past h2, rotations past nb and
+  // rows past the end are never written and must hold finite values
+  for (int i = tid; i < 2 * kEoN * K2 / 4; i += kZThreads)
+    reinterpret_cast<uint2*>(Bs)[i] = make_uint2(0u, 0u);
+  if (tid == 0) {
+    for (int q = 0; q < 2; ++q) {
+      mbar_init(bfull + q, kZLoaders);
+      mbar_init(bempty + q, 1);
+      mbar_init(tfull + q, 1);
+      mbar_init(tempty + q, kZEpi);
+    }
+    mbar_init(mdone, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;");
+    *fail = 0;
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+
+  const int64_t nblk = (rows + kEoRows - 1) / kEoRows;
+  const int64_t mine = nblk > blockIdx.x ? (nblk - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int zmax = n2 / 2;              // rows z <= zmax of the tile are outputs
+  const int zodd = (n2 + 1) / 2 - 1;    // z in [1, zodd] also gives x[n2 - z]
+
+  if (warp != 0 && !zp_epilogue_warp(warp)) {
+    // ---------------------------------------------------------------- loaders
+    const int lt = zp_loader_index(tid);
+    for (int i = lt; i < (int)(4 * tab / 8); i += kZLoaders)
+      cp_async16(smem_u32(As) + 16u * i, Ag + 8 * (size_t)i, 16);
+    // task i = (quad of 4-value chunks i >> 9, 8-row group (i >> 5) & 15, lane i & 31):
+    // lanes 0-7 take rows 0-7 of chunk 4q, lanes 8-15 chunk 4q + 1, ...: 64 contiguous
+    // bytes per H row per warp access, and 8-byte shared stores that fill two core
+    // matrices without conflicts
+    static_assert(kEoN == 128, "task decomposition: 16 row groups of 8");
+    const int nq = (h2 + 3) / 4;        // 4-value chunks holding values k < h2
+    const int nquad = (nq + 3) / 4;
+    const int ntask = nquad * 512;
+    // per-thread tasks, the same for every block: bits 0-15 shared-memory offset of the
+    // Re values (halves; Im at + 8 K'), 16-20 chunk, 21-25 rotation, 26-27 row in the
+    // block, 28 live (a task of this launch, chunk holding values k < h2, rotation < nb)
+    uint32_t task[MT];
+#pragma unroll
+    for (int m = 0; m < MT; ++m) {
+      const int i = lt + m * kZLoaders;
+      const int ln = i & 31, ng = (i >> 5) & 15;
+      const int n = ng * 8 + (ln & 7), kq = (i >> 9) * 4 + (ln >> 3);
+      const int r = n >> 5, b = n & (kZRot - 1);
+      const bool live = i < ntask && kq < nq && b < nb;
+      task[m] = (uint32_t)kmajor16(n, 4 * (kq & 31), K2) | ((uint32_t)(kq & 31) << 16) |
+                ((uint32_t)b << 21) | ((uint32_t)r << 26) | (live ? 1u << 28 : 0u);
+    }
+    for (int64_t j = 0; j < mine; ++j) {
+      const int sidx = (int)(j & 1);
+      const uint32_t u = (uint32_t)(j >> 1);
+      if (j >= 2 && !mbar_wait(smem_u32(bempty + sidx), (u - 1) & 1u)) { *fail = 1; break; }
+      if (*fail) break;
+      const int64_t row0 = ((int64_t)blockIdx.x + j * gridDim.x) * kEoRows;
+      const int64_t left = rows - row0;
+      const int rlive = left < kEoRows ? (int)left : kEoRows;  // rows in the block
+      uint4 val[MT];
+#pragma unroll
+      for (int m = 0; m < MT; ++m) {
+        const uint32_t tk = task[m];
+        const int kq = (tk >> 16) & 31, b = (tk >> 21) & 31, r = (tk >> 26) & 3;
+        val[m] = make_uint4(0u, 0u, 0u, 0u);
+        if ((tk >> 28) && r < rlive)
+          val[m] = __ldg(reinterpret_cast<const uint4*>(H + (int64_t)b * SH + (row0 + r) * hp) + kq);
+      }
+      if (j >= 2 && !mbar_wait(smem_u32(tempty + sidx), (u - 1) & 1u)) { *fail = 1; break; }
+      // state and denominators of the block's rows
+      const int nqs = kEoRows * n2 / 4;
+      const int64_t g0 = row0 * n2;
+      const int64_t gend = rows * n2;
+      const uint32_t sd = smem_u32(sst + sidx * kEoRows * n2);
+      const uint32_t dd = smem_u32(sden + sidx * kEoRows * n2);
+      for (int q = lt; q < nqs; q += kZLoaders) {
+        const int64_t g = g0 + 4 * q;
+        const uint32_t bytes = g + 4 <= gend ? 16u : (g < gend ? (uint32_t)(gend - g) * 4u : 0u);
+        cp_async16(sd + 16u * q, bytes ? state_max + g : state_max, bytes);
+      }
+      if (inv_den) {
+        for (int q = lt; q < nqs; q += kZLoaders) {
+          const int64_t g = g0 + 4 * q;
+          const uint32_t bytes = g + 4 <= gend ? 16u : (g < gend ? (uint32_t)(gend - g) * 4u : 0u);
+          cp_async16(dd + 16u * q, bytes ? inv_den + g : state_max, bytes);
+        }
+      }
+      mbar_track_cp_async(bfull + sidx);
+      uint16_t* bj = Bs + (size_t)sidx * kEoN * K2;
+#pragma unroll
+      for (int m = 0; m < MT; ++m) {
+        const uint32_t tk = task[m];
+        const int kq = (tk >> 16) & 31, r = (tk >> 26) & 3;
+        if ((tk >> 28) && r < rlive) {
+          uint4 v = val[m];
+          // values k >= h2 of the last chunk are zero in the operand
+          const int live = h2 - 4 * kq;
+          if (live < 4) v.w = 0u;
+          if (live < 3) v.z = 0u;
+          if (live < 2) v.y = 0u;
+          const uint2 re = make_uint2(__byte_perm(v.x, v.y, 0x5410), __byte_perm(v.z, v.w, 0x5410));
+          const uint2 im = make_uint2(__byte_perm(v.x, v.y, 0x7632), __byte_perm(v.z, v.w, 0x7632));
+          uint16_t* dst = bj + (tk & 0xffffu);
+          *reinterpret_cast<uint2*>(dst) = re;
+          *reinterpret_cast<uint2*>(dst + 8 * Kp) = im;  // K' further on: chunk K'/8 later
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(bfull + sidx);
+    }
+  } else if (warp == 0) {
+    // ---------------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = idesc_f16(128, kEoN);
+      const uint64_t ad = smem_desc(smem_u32(As), 128u, (uint32_t)Kp * 16u);
+      const uint64_t bd = smem_desc(smem_u32(Bs), 128u, (uint32_t)K2 * 16u);
+      const uint32_t alo = (uint32_t)ad, ahi = (uint32_t)(ad >> 32);
+      const uint32_t blo = (uint32_t)bd, bhi = (uint32_t)(bd >> 32);
+      const uint32_t tab16 = (uint32_t)(tab * 2 >> 4);            // one table, >> 4
+      const uint32_t bbuf16 = (uint32_t)((size_t)kEoN * K2 * 2 >> 4);
+      const uint32_t im16 = (uint32_t)Kp;                         // Im block: K' * 16 bytes
+      const int steps = Kp / 16;
+      bool ok = true;
+      for (int64_t j = 0; j < mine; ++j) {
+        const int sidx = (int)(j & 1);
+        const uint32_t u = (uint32_t)(j >> 1);
+        if (!mbar_wait(smem_u32(bfull + sidx), u & 1u)) { ok = false; break; }
+        if (j >= 2 && !mbar_wait(smem_u32(tempty + sidx), (u - 1) & 1u)) { ok = false; break; }
+        if (*fail) { ok = false; break; }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t bj = blo + (uint32_t)sidx * bbuf16;
+        const uint32_t dE = tmem + (uint32_t)(sidx * 2 * kEoN), dO = dE + (uint32_t)kEoN;
+        for (int s = 0; s < steps; ++s) {
+          const uint32_t o = 16u * (uint32_t)s;  // 256 bytes per 16 K values
+          mma_f16_w(dE, alo + o, ahi, bj + o, bhi, idesc, s > 0);
+          mma_f16_w(dE, alo + tab16 + o, ahi, bj + o, bhi, idesc, 1);
+          mma_f16_w(dO, alo + 2 * tab16 + o, ahi, bj + im16 + o, bhi, idesc, s > 0);
+          mma_f16_w(dO, alo + 3 * tab16 + o, ahi, bj + im16 + o, bhi, idesc, 1);
+        }
+        mma_commit(smem_u32(tfull + sidx));
+        mma_commit(smem_u32(bempty + sidx));
+      }
+      if (!ok) *fail = 1;
+      // nothing may free tensor memory or shared memory under a running MMA
+      mma_commit(smem_u32(mdone));
+      if (!mbar_wait(smem_u32(mdone), 0u)) *fail = 1;
+    }
+  } else {
+    // ---------------------------------------------------------------- epilogue
+    const int quarter = warp & 3, egrp = warp >> 3;
+    const int z = quarter * 32 + lane;
+    bool ok = true;
+    for (int64_t j = 0; j < mine && ok; ++j) {
+      const int sidx = (int)(j & 1);
+      const uint32_t u = (uint32_t)(j >> 1);
+      const bool got = mbar_wait(smem_u32(tfull + sidx), u & 1u);
+      __syncwarp();  // tcgen05.ld needs the whole warp, converged
+      if (!__all_sync(0xffffffffu, got)) { *fail = 1; ok = false; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const int64_t row0 = ((int64_t)blockIdx.x + j * gridDim.x) * kEoRows;
+      const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(sidx * 2 * kEoN);
+      const float* st = sst + sidx * kEoRows * n2;
+      const float* dn = sden + sidx * kEoRows * n2;
+#pragma unroll 1
+      for (int r = egrp; r < kEoRows; r += 2) {
+        float ev[32], ov[32];
+        tmem_ld32(tb + (uint32_t)(r * kZRot), ev);
+        tmem_ld32(tb + (uint32_t)(kEoN + r * kZRot), ov);
+        asm volatile("tcgen05.wait::ld.sync.aligned;");
+        const int64_t row = row0 + r;
+        if (z <= zmax && row < rows) {
+          // maxima of x[z] = E + O and x[n2 - z] = E - O over the rotations (fmaxf skips
+          // NaN as the strict comparison does); the first rotation reaching a maximum is
+          // looked up only when the scaled maximum beats the running state
+          float b1 = -INFINITY, b2 = -INFINITY;
+          if (nb == kZRot) {
+#pragma unroll
+            for (int b = 0; b < kZRot; ++b) {
+              b1 = fmaxf(b1, ev[b] + ov[b]);
+              b2 = fmaxf(b2, ev[b] - ov[b]);
+            }
+          } else {
+#pragma unroll
+            for (int b = 0; b < kZRot; ++b)
+              if (b < nb) {
+                b1 = fmaxf(b1, ev[b] + ov[b]);
+                b2 = fmaxf(b2, ev[b] - ov[b]);
+              }
+          }
+          const int64_t g = row * n2;
+          const int e1 = r * n2 + z;
+          const float s1 = b1 * scale * (inv_den ? dn[e1] : 1.f);
+          if (b1 > -INFINITY && s1 > st[e1]) {
+            int a1 = 0;
+#pragma unroll
+            for (int b = kZRot - 1; b >= 0; --b)
+              if (b < nb && ev[b] + ov[b] == b1) a1 = b;
+            state_max[g + z] = s1;
+            state_rot[g + z] = first_index + a1;
+          }
+          if (z >= 1 && z <= zodd) {
+            const int e2 = r * n2 + (n2 - z);
+            const float s2 = b2 * scale * (inv_den ? dn[e2] : 1.f);
+            if (b2 > -INFINITY && s2 > st[e2]) {
+              int a2 = 0;
+#pragma unroll
+              for (int b = kZRot - 1; b >= 0; --b)
+                if (b < nb && ev[b] - ov[b] == b2) a2 = b;
+              state_max[g + n2 - z] = s2;
+              state_rot[g + n2 - z] = first_index + a2;
+            }
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      mbar_arrive(tempty + sidx);
+    }
+  }
+  asm volatile("cp.async.wait_all;\n" ::);
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (warp == 0) {
+    __syncwarp();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                 :
+                 : "r"(tmem), "r"(4 * kEoN));
+  }
+  if (tid == 0 && *fail) atomicExch(err, 1);
+}
+
 }  // namespace
+
+// loader tasks per thread of the even/odd kernel
+static int eo_tasks(int h2) {
+  const int nquad = ((h2 + 3) / 4 + 3) / 4;
+  return (nquad * 512 + kZLoaders - 1) / kZLoaders;
+}
 
 int zpass_tc_config(int n2, int h2, int hp, int nb, ZpassTcConfig* cfg) {
   cfg->ok = false;
+  cfg->eo = false;
+  cfg->Kp = (h2 + 15) / 16 * 16;
+  cfg->zr = eo_rows(n2);
+  cfg->eo_smem = ((size_t)4 * cfg->zr * cfg->Kp + (size_t)2 * kEoN * 2 * cfg->Kp) * 2 +
+                 (size_t)4 * kEoRows * n2 * sizeof(float) + 9 * 8 + 16;
   cfg->K = 2 * hp;
   cfg->n2 = n2;
   cfg->smem = (size_t)(2 * zrows(n2) + 2 * kZN) * cfg->K * 2 +
               (size_t)4 * kZRows * n2 * sizeof(float) + 8 * 8 + 16;
   // z < 256 in two M = 128 tiles; the second tile's reads past the tail stay inside the
   // operand buffers when zrows(n2) >= 64
-  if (n2 > kZM || n2 < 128 || n2 % 4 != 0 || hp % 8 != 0 || nb < 1 || nb > kZRot || h2 > hp)
-    return TM_OK;
+  if (hp % 8 != 0 || nb < 1 || nb > kZRot || h2 > hp || h2 != n2 / 2 + 1) return TM_OK;
   int dev = 0, optin = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaGetLastError();
   cfg->sms = sms;
+  // even/odd form: z <= n2/2 in one M = 128 tile
+  if (n2 >= 16 && n2 / 2 + 1 <= 128 && eo_tasks(h2) <= 19 && cfg->eo_smem <= (size_t)optin) {
+    for (auto fn : {zpass_eo_kernel<16>, zpass_eo_kernel<19>})
+      TM_TRY(cuda_status(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              optin),
+                         "zpass_tc: shared memory attribute"));
+    cfg->eo = true;
+    cfg->ok = true;
+    return TM_OK;
+  }
+  // two-tile form: z < 256 in two M = 128 tiles, the operator interleaved like H
+  if (n2 > kZM || n2 < 128 || n2 % 4 != 0) return TM_OK;
   if (cfg->smem > (size_t)optin) return TM_OK;
   TM_TRY(cuda_status(cudaFuncSetAttribute(zpass_tc_kernel,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, optin),
@@ -300,12 +659,17 @@ int zpass_tc_config(int n2, int h2, int hp, int nb, ZpassTcConfig* cfg) {
 }
 
 size_t zpass_tc_table_bytes(const ZpassTcConfig& cfg) {
+  if (cfg.eo) return (size_t)4 * cfg.zr * cfg.Kp * 2;
   return (size_t)2 * zrows(cfg.n2) * cfg.K * 2;
 }
 
 int zpass_tc_prepare(const ZpassTcConfig& cfg, uint16_t* table, int n2, int h2,
                      cudaStream_t stream) {
   TM_REQUIRE(cfg.ok && table, "zpass_tc_prepare: unsupported configuration");
+  if (cfg.eo) {
+    eo_table_kernel<<<64, 256, 0, stream>>>(table, n2, h2, cfg.Kp);
+    return check_launch("eo_table_kernel");
+  }
   zdft_table_kernel<<<64, 256, 0, stream>>>(table, n2, h2, cfg.K);
   return check_launch("zdft_table_kernel");
 }
@@ -316,6 +680,15 @@ int zpass_tc_run(const ZpassTcConfig& cfg, const void* H, int nb, int64_t rows, 
                  const int32_t* first_dev, int* err, cudaStream_t stream) {
   TM_REQUIRE(cfg.ok, "zpass_tc_run: unsupported configuration");
   TM_REQUIRE(nb >= 1 && nb <= kZRot, "zpass_tc_run: %d rotations per group (1..%d)", nb, kZRot);
+  if (cfg.eo) {
+    const int64_t nblk = (rows + kEoRows - 1) / kEoRows;
+    const int grid = (int)std::min<int64_t>(nblk, cfg.sms);
+    auto fn = eo_tasks(h2) <= 16 ? zpass_eo_kernel<16> : zpass_eo_kernel<19>;
+    fn<<<grid, kZThreads, cfg.eo_smem, stream>>>(
+        static_cast<const __half2*>(H), nb, rows, n2, h2, hp, cfg.Kp, table, scale, inv_den,
+        first_index, state_max, state_rot, SH, first_dev, err);
+    return check_launch("zpass_eo_kernel");
+  }
   const int64_t nblk = (rows + kZRows - 1) / kZRows;
   const int grid = (int)std::min<int64_t>(nblk, cfg.sms);
   zpass_tc_kernel<<<grid, kZThreads, cfg.smem, stream>>>(

@@ -13,6 +13,11 @@ struct ZpassTcConfig {
   int n2;
   int sms;      // persistent grid size
   size_t smem;
+  // even/odd variant (n2/2 + 1 <= 128): cosine and sine operators over z <= n2/2,
+  // K' = h2 rounded up to 16 per component
+  bool eo;
+  int Kp, zr;
+  size_t eo_smem;
 };
 
 // Whether the tensor-core z pass handles n2 / h2 / row pitch hp / nb rotations per group.

@@ -309,7 +309,7 @@ def test_flcsm_config3_shape(torch_cuda):
     assert np.abs(r[0] - ref["scores"]).max() <= TOL
 
 
-@pytest.mark.parametrize("n2", [64, 100, 128, 160, 200, 256, 400, 512])
+@pytest.mark.parametrize("n2", [64, 100, 128, 160, 199, 200, 256, 400, 512])
 @pytest.mark.parametrize("precision", ["fp32", "mixed"])
 def test_zpass_lengths(torch_cuda, n2, precision):
     """Every z-axis length with a dedicated c2r kernel (and the generic fallback for the
