@@ -282,10 +282,13 @@ zpass_tc_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
 // give all n2 outputs: two GEMMs with half the K of the interleaved operator, a quarter
 // of the MMAs of the two-tile form for the same outputs. The rotation operand holds each
 // H row de-interleaved, [Re X[0..K') | Im X[0..K')] (the loaders split the FP16 complex
-// values in registers). Blocks are 4 rows x 32 rotations (N = 128); the E and O
-// accumulators of a block take 256 tensor-memory columns, two blocks in flight.
-constexpr int kEoRows = 4;
-constexpr int kEoN = kEoRows * kZRot;  // 128
+// values in registers). Blocks are 2 rows x 32 rotations (N = 64) in a ring of 4 stages
+// (operand buffer, E and O accumulators in 128 tensor-memory columns, state): the loads
+// of three blocks are in flight while one is multiplied. With 4-row blocks in 2 stages
+// the loaders' DRAM round trip set the pace.
+constexpr int kEoRows = 2;
+constexpr int kEoN = kEoRows * kZRot;  // 64
+constexpr int kEoS = 4;                // stages: operand buffers, accumulator pairs, state
 
 __host__ __device__ inline int eo_rows(int n2) { return (n2 / 2 + 1 + 7) / 8 * 8; }
 
@@ -343,7 +346,7 @@ __device__ __forceinline__ void mbar_track_cp_async(uint64_t* bar) {
 //   bempty[s]  MMAs of the block done: its rotation-operand buffer is free (commit)
 //   tfull[s]   accumulators of the block written (commit)
 //   tempty[s]  epilogue done: accumulators and state buffers free (count: epilogue)
-// MT: loader tasks per thread, ceil(512 * ceil(ceil(h2 / 4) / 4) / kZLoaders).
+// MT: loader tasks per thread, ceil(256 * ceil(ceil(h2 / 4) / 4) / kZLoaders).
 template <int MT>
 __global__ void __launch_bounds__(kZThreads, 1)
 zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int h2, int hp,
@@ -357,31 +360,31 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
   const int K2 = 2 * Kp;                          // rotation-operand K: Re block, Im block
   const size_t tab = (size_t)zr * Kp;             // halves per operator table
   uint16_t* As = smem_e;                          // 4 tables
-  uint16_t* Bs = As + 4 * tab;                    // 2 buffers x [kEoN x K2]
-  float* sst = reinterpret_cast<float*>(Bs + (size_t)2 * kEoN * K2);  // 2 x [kEoRows x n2]
-  float* sden = sst + 2 * kEoRows * n2;                               // 2 x [kEoRows x n2]
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sden + 2 * kEoRows * n2);
+  uint16_t* Bs = As + 4 * tab;                    // kEoS buffers x [kEoN x K2]
+  float* sst = reinterpret_cast<float*>(Bs + (size_t)kEoS * kEoN * K2);  // kEoS x [kEoRows x n2]
+  float* sden = sst + kEoS * kEoRows * n2;                               // kEoS x [kEoRows x n2]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sden + kEoS * kEoRows * n2);
   uint64_t* bfull = bar;
-  uint64_t* bempty = bar + 2;
-  uint64_t* tfull = bar + 4;
-  uint64_t* tempty = bar + 6;
-  uint64_t* mdone = bar + 8;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 9);
+  uint64_t* bempty = bar + kEoS;
+  uint64_t* tfull = bar + 2 * kEoS;
+  uint64_t* tempty = bar + 3 * kEoS;
+  uint64_t* mdone = bar + 4 * kEoS;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 4 * kEoS + 1);
   int* fail = reinterpret_cast<int*>(tmem_slot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  :
-                 : "r"(smem_u32(tmem_slot)), "r"(4 * kEoN));
+                 : "r"(smem_u32(tmem_slot)), "r"(2 * kEoS * kEoN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  // zero both rotation-operand buffers once: K positions past h2, rotations past nb and
+  // zero the rotation-operand buffers once: K positions past h2, rotations past nb and
   // rows past the end are never written and must hold finite values
-  for (int i = tid; i < 2 * kEoN * K2 / 4; i += kZThreads)
+  for (int i = tid; i < kEoS * kEoN * K2 / 4; i += kZThreads)
     reinterpret_cast<uint2*>(Bs)[i] = make_uint2(0u, 0u);
   if (tid == 0) {
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < kEoS; ++q) {
       mbar_init(bfull + q, kZLoaders);
       mbar_init(bempty + q, 1);
       mbar_init(tfull + q, 1);
@@ -407,14 +410,14 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
     const int lt = zp_loader_index(tid);
     for (int i = lt; i < (int)(4 * tab / 8); i += kZLoaders)
       cp_async16(smem_u32(As) + 16u * i, Ag + 8 * (size_t)i, 16);
-    // task i = (quad of 4-value chunks i >> 9, 8-row group (i >> 5) & 15, lane i & 31):
+    // task i = (quad of 4-value chunks i >> 8, 8-row group (i >> 5) & 7, lane i & 31):
     // lanes 0-7 take rows 0-7 of chunk 4q, lanes 8-15 chunk 4q + 1, ...: 64 contiguous
     // bytes per H row per warp access, and 8-byte shared stores that fill two core
     // matrices without conflicts
-    static_assert(kEoN == 128, "task decomposition: 16 row groups of 8");
+    static_assert(kEoN == 64, "task decomposition: 8 row groups of 8");
     const int nq = (h2 + 3) / 4;        // 4-value chunks holding values k < h2
     const int nquad = (nq + 3) / 4;
-    const int ntask = nquad * 512;
+    const int ntask = nquad * 256;
     // per-thread tasks, the same for every block: bits 0-15 shared-memory offset of the
     // Re values (halves; Im at + 8 K'), 16-20 chunk, 21-25 rotation, 26-27 row in the
     // block, 28 live (a task of this launch, chunk holding values k < h2, rotation < nb)
@@ -422,17 +425,17 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
 #pragma unroll
     for (int m = 0; m < MT; ++m) {
       const int i = lt + m * kZLoaders;
-      const int ln = i & 31, ng = (i >> 5) & 15;
-      const int n = ng * 8 + (ln & 7), kq = (i >> 9) * 4 + (ln >> 3);
+      const int ln = i & 31, ng = (i >> 5) & 7;
+      const int n = ng * 8 + (ln & 7), kq = (i >> 8) * 4 + (ln >> 3);
       const int r = n >> 5, b = n & (kZRot - 1);
       const bool live = i < ntask && kq < nq && b < nb;
       task[m] = (uint32_t)kmajor16(n, 4 * (kq & 31), K2) | ((uint32_t)(kq & 31) << 16) |
                 ((uint32_t)b << 21) | ((uint32_t)r << 26) | (live ? 1u << 28 : 0u);
     }
     for (int64_t j = 0; j < mine; ++j) {
-      const int sidx = (int)(j & 1);
-      const uint32_t u = (uint32_t)(j >> 1);
-      if (j >= 2 && !mbar_wait(smem_u32(bempty + sidx), (u - 1) & 1u)) { *fail = 1; break; }
+      const int sidx = (int)(j % kEoS);
+      const uint32_t u = (uint32_t)(j / kEoS);
+      if (j >= kEoS && !mbar_wait(smem_u32(bempty + sidx), (u - 1) & 1u)) { *fail = 1; break; }
       if (*fail) break;
       const int64_t row0 = ((int64_t)blockIdx.x + j * gridDim.x) * kEoRows;
       const int64_t left = rows - row0;
@@ -446,7 +449,7 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
         if ((tk >> 28) && r < rlive)
           val[m] = __ldg(reinterpret_cast<const uint4*>(H + (int64_t)b * SH + (row0 + r) * hp) + kq);
       }
-      if (j >= 2 && !mbar_wait(smem_u32(tempty + sidx), (u - 1) & 1u)) { *fail = 1; break; }
+      if (j >= kEoS && !mbar_wait(smem_u32(tempty + sidx), (u - 1) & 1u)) { *fail = 1; break; }
       // state and denominators of the block's rows
       const int nqs = kEoRows * n2 / 4;
       const int64_t g0 = row0 * n2;
@@ -502,10 +505,10 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
       const int steps = Kp / 16;
       bool ok = true;
       for (int64_t j = 0; j < mine; ++j) {
-        const int sidx = (int)(j & 1);
-        const uint32_t u = (uint32_t)(j >> 1);
+        const int sidx = (int)(j % kEoS);
+        const uint32_t u = (uint32_t)(j / kEoS);
         if (!mbar_wait(smem_u32(bfull + sidx), u & 1u)) { ok = false; break; }
-        if (j >= 2 && !mbar_wait(smem_u32(tempty + sidx), (u - 1) & 1u)) { ok = false; break; }
+        if (j >= kEoS && !mbar_wait(smem_u32(tempty + sidx), (u - 1) & 1u)) { ok = false; break; }
         if (*fail) { ok = false; break; }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::after_thread_sync;");
@@ -532,8 +535,8 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
     const int z = quarter * 32 + lane;
     bool ok = true;
     for (int64_t j = 0; j < mine && ok; ++j) {
-      const int sidx = (int)(j & 1);
-      const uint32_t u = (uint32_t)(j >> 1);
+      const int sidx = (int)(j % kEoS);
+      const uint32_t u = (uint32_t)(j / kEoS);
       const bool got = mbar_wait(smem_u32(tfull + sidx), u & 1u);
       __syncwarp();  // tcgen05.ld needs the whole warp, converged
       if (!__all_sync(0xffffffffu, got)) { *fail = 1; ok = false; break; }
@@ -605,7 +608,7 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
     __syncwarp();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
                  :
-                 : "r"(tmem), "r"(4 * kEoN));
+                 : "r"(tmem), "r"(2 * kEoS * kEoN));
   }
   if (tid == 0 && *fail) atomicExch(err, 1);
 }
@@ -615,7 +618,7 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
 // loader tasks per thread of the even/odd kernel
 static int eo_tasks(int h2) {
   const int nquad = ((h2 + 3) / 4 + 3) / 4;
-  return (nquad * 512 + kZLoaders - 1) / kZLoaders;
+  return (nquad * 256 + kZLoaders - 1) / kZLoaders;
 }
 
 int zpass_tc_config(int n2, int h2, int hp, int nb, ZpassTcConfig* cfg) {
@@ -623,8 +626,8 @@ int zpass_tc_config(int n2, int h2, int hp, int nb, ZpassTcConfig* cfg) {
   cfg->eo = false;
   cfg->Kp = (h2 + 15) / 16 * 16;
   cfg->zr = eo_rows(n2);
-  cfg->eo_smem = ((size_t)4 * cfg->zr * cfg->Kp + (size_t)2 * kEoN * 2 * cfg->Kp) * 2 +
-                 (size_t)4 * kEoRows * n2 * sizeof(float) + 9 * 8 + 16;
+  cfg->eo_smem = ((size_t)4 * cfg->zr * cfg->Kp + (size_t)kEoS * kEoN * 2 * cfg->Kp) * 2 +
+                 (size_t)2 * kEoS * kEoRows * n2 * sizeof(float) + (4 * kEoS + 1) * 8 + 16;
   cfg->K = 2 * hp;
   cfg->n2 = n2;
   cfg->smem = (size_t)(2 * zrows(n2) + 2 * kZN) * cfg->K * 2 +
@@ -639,8 +642,8 @@ int zpass_tc_config(int n2, int h2, int hp, int nb, ZpassTcConfig* cfg) {
   cudaGetLastError();
   cfg->sms = sms;
   // even/odd form: z <= n2/2 in one M = 128 tile
-  if (n2 >= 16 && n2 / 2 + 1 <= 128 && eo_tasks(h2) <= 19 && cfg->eo_smem <= (size_t)optin) {
-    for (auto fn : {zpass_eo_kernel<16>, zpass_eo_kernel<19>})
+  if (n2 >= 16 && n2 / 2 + 1 <= 128 && eo_tasks(h2) <= 10 && cfg->eo_smem <= (size_t)optin) {
+    for (auto fn : {zpass_eo_kernel<8>, zpass_eo_kernel<10>})
       TM_TRY(cuda_status(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               optin),
                          "zpass_tc: shared memory attribute"));
@@ -683,7 +686,7 @@ int zpass_tc_run(const ZpassTcConfig& cfg, const void* H, int nb, int64_t rows, 
   if (cfg.eo) {
     const int64_t nblk = (rows + kEoRows - 1) / kEoRows;
     const int grid = (int)std::min<int64_t>(nblk, cfg.sms);
-    auto fn = eo_tasks(h2) <= 16 ? zpass_eo_kernel<16> : zpass_eo_kernel<19>;
+    auto fn = eo_tasks(h2) <= 8 ? zpass_eo_kernel<8> : zpass_eo_kernel<10>;
     fn<<<grid, kZThreads, cfg.eo_smem, stream>>>(
         static_cast<const __half2*>(H), nb, rows, n2, h2, hp, cfg.Kp, table, scale, inv_den,
         first_index, state_max, state_rot, SH, first_dev, err);
