@@ -52,8 +52,10 @@ constexpr int kWsZB = 128;       // kernel-operand builder threads (warps 4-7)
 constexpr int kWsEpi = 256;      // epilogue threads (warps 8-15)
 constexpr int kWsThreads = 32 + kWsGL + kWsZB + kWsEpi;
 constexpr float kWsPrescale = 256.f;  // keeps the scaled kernel values in FP16's normal range
-constexpr int kWsRot = 16;            // rotations per accumulator buffer (MMA N)
-constexpr uint32_t kWsAccCols = 256;  // 8 columns x (Re, Im) x 16 rotations
+constexpr uint32_t kWsTmemCols = 512;  // all of tensor memory
+// A fill of R rotations (MMA N = R) takes 8 columns x (Re, Im) x R accumulator columns:
+// two alternating buffers for R = 16, one for R = 32 (fewer, wider MMAs; each MMA fetches
+// its 4 KB Hankel tile from shared memory once, whatever N is)
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" : : "r"(smem_u32(bar)), "r"(count));
@@ -102,12 +104,12 @@ __device__ __forceinline__ void mma_f16_w(uint32_t tmem_d, uint32_t alo, uint32_
       : "r"(tmem_d), "r"(alo), "r"(ahi), "r"(blo), "r"(bhi), "r"(idesc), "r"(accumulate));
 }
 
-// The MMAs of one accumulator fill: for each of the 8 columns, Re H and Im H of 16
+// The MMAs of one accumulator fill: for each of the 8 columns, Re H and Im H of R
 // rotations over K = (Re g | Im g) in NXC steps of 16 (NXC = t0p / 8; the first half of
 // the steps multiplies Re g, the second Im g). zlo: descriptor low word of the fill's
 // Z segment; blo: of the rotation operand rows of the fill; nzb8 / bst16: the Z array
 // and rotation operand strides >> 4.
-template <int NXC>
+template <int NXC, int R>
 __device__ __forceinline__ void issue_fill(uint32_t d0, uint32_t zlo, uint32_t blo, uint32_t ahi,
                                            uint32_t bhi, uint32_t nzb8, uint32_t bst16,
                                            uint32_t idesc, uint32_t idesc_neg) {
@@ -115,7 +117,7 @@ __device__ __forceinline__ void issue_fill(uint32_t d0, uint32_t zlo, uint32_t b
   for (int w = 0; w < kWsW; ++w) {
     const uint32_t zr = zlo + (uint32_t)(2 * w) * nzb8, zi = zr + nzb8;
     const uint32_t bw = blo + (uint32_t)w * bst16;
-    const uint32_t d_re = d0 + (uint32_t)(w * 2 * kWsRot), d_im = d_re + (uint32_t)kWsRot;
+    const uint32_t d_re = d0 + (uint32_t)(w * 2 * R), d_im = d_re + (uint32_t)R;
 #pragma unroll
     for (int s = 0; s < NXC; ++s) {
       const bool imag_g = 2 * s >= NXC;
@@ -161,12 +163,14 @@ __host__ __device__ inline WsLayout ws_layout(int t0p, int NB) {
   return L;
 }
 
-template <int NXC>
+template <int NXC, int R>
 __global__ void __launch_bounds__(kWsThreads, 1)
 xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int nb, int NB,
                 int t0, int n0, int n1, int h2, int hp, float scale,
                 __half2* __restrict__ H, int* __restrict__ err) {
   constexpr int t0p = 8 * NXC;
+  constexpr uint32_t kAccCols = 16u * R;               // one fill
+  constexpr int kNbuf = (int)(kWsTmemCols / kAccCols);  // 2 (R = 16) or 1 (R = 32)
   extern __shared__ __align__(128) uint8_t smem_ws[];
   const WsLayout L = ws_layout(t0p, NB);
   const int K = L.K, NZB = L.nzb, En = L.En, E = L.E;
@@ -188,7 +192,7 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  :
-                 : "r"(smem_u32(tmem_slot)), "r"(2 * kWsAccCols));
+                 : "r"(smem_u32(tmem_slot)), "r"(kWsTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
@@ -215,14 +219,14 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
   const int ntile = n0 / kWsRows;
   const int64_t row = (int64_t)n1 * h2;  // G and C: [.][x][k1][k2]
   constexpr int nxc = NXC;
-  // accumulator fills: f = tile * nh + h for the h-th 16 rotations of a tile, in buffer
-  // f % 2; the u-th fill of a buffer (u = f / 2) completes phase u of its barriers
-  const int nh = NB / kWsRot;
+  // accumulator fills: f = tile * nh + h for the h-th R rotations of a tile, in buffer
+  // f % kNbuf; the u-th fill of a buffer (u = f / kNbuf) completes phase u of its barriers
+  const int nh = NB / R;
 
   if (warp == 0) {
     // ------------------------------------------------------------------ MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = idesc_f16(kWsRows, kWsRot);
+      const uint32_t idesc = idesc_f16(kWsRows, R);
       const uint32_t idesc_neg = idesc | (1u << 13);
       // descriptor words: Z blocks with both strides 128 bytes; rotation operands with
       // K-adjacent core matrices 128 bytes and 8-row groups K * 16 bytes apart
@@ -243,16 +247,17 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           for (int h = 0; h < nh; ++h) {
             const int64_t f = tau * nh + h;
-            const int buf = (int)(f & 1);
-            if (f >= 2 && !mbar_wait(smem_u32(tempty + buf), (uint32_t)((f >> 1) - 1) & 1u)) {
+            const int buf = (int)(f % kNbuf);
+            const uint32_t uf = (uint32_t)(f / kNbuf);
+            if (f >= kNbuf && !mbar_wait(smem_u32(tempty + buf), (uf - 1) & 1u)) {
               ok = false;
               break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            // rotations 16h.. are row groups 2h.. of the K-major operand
-            issue_fill<NXC>(tmem + (uint32_t)buf * kWsAccCols, zlo + (uint32_t)zsl * zbuf16,
-                            blo + (uint32_t)bsl * bbuf16 + (uint32_t)(2 * h) * (uint32_t)K,
-                            ahi, bhi, nzb8, bst16, idesc, idesc_neg);
+            // rotations R h.. are row groups (R/8) h.. of the K-major operand
+            issue_fill<NXC, R>(tmem + (uint32_t)buf * kAccCols, zlo + (uint32_t)zsl * zbuf16,
+                               blo + (uint32_t)bsl * bbuf16 + (uint32_t)(R / 8 * h) * (uint32_t)K,
+                               ahi, bhi, nzb8, bst16, idesc, idesc_neg);
             mma_commit(smem_u32(tfull + buf));
           }
           if (!ok) break;
@@ -380,7 +385,7 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
     }
   } else {
     // ------------------------------------------------------------------ epilogue
-    const int quarter = warp & 3, eg = (warp - 8) >> 2;  // eg: rotations 8 eg .. of a fill
+    const int quarter = warp & 3, eg = (warp - 8) >> 2;  // eg: rotations (R/2) eg .. of a fill
     const float inv = 1.f / kWsPrescale;
     const int64_t rowH = (int64_t)n1 * hp, SH = (int64_t)n0 * rowH;
     const int r = quarter * 32 + lane;
@@ -395,8 +400,8 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
         __half2* hrow = H + (int64_t)xp * rowH + colH;
         for (int h = 0; h < nh; ++h) {
           const int64_t f = tau * nh + h;
-          const int buf = (int)(f & 1);
-          const bool got = mbar_wait(smem_u32(tfull + buf), (uint32_t)(f >> 1) & 1u);
+          const int buf = (int)(f % kNbuf);
+          const bool got = mbar_wait(smem_u32(tfull + buf), (uint32_t)(f / kNbuf) & 1u);
           __syncwarp();  // tcgen05.ld needs the whole warp, converged
           if (!__all_sync(0xffffffffu, got)) {
             *fail = 1;
@@ -404,18 +409,18 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;");
-          const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)buf * kWsAccCols;
+          const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)buf * kAccCols;
 #pragma unroll
-          for (int rr = 0; rr < 2; ++rr) {
-            const int bl = 8 * eg + 4 * rr;  // rotation within the fill
+          for (int rr = 0; rr < R / 8; ++rr) {
+            const int bl = R / 2 * eg + 4 * rr;  // rotation within the fill
             float v[2 * kWsW][4];            // [column * 2 + component][rotation]
 #pragma unroll
             for (int wc = 0; wc < 2 * kWsW; ++wc)
-              tmem_ld4(tb + (uint32_t)((wc >> 1) * 2 * kWsRot + (wc & 1) * kWsRot + bl), v[wc]);
+              tmem_ld4(tb + (uint32_t)((wc >> 1) * 2 * R + (wc & 1) * R + bl), v[wc]);
             asm volatile("tcgen05.wait::ld.sync.aligned;");
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-              const int b = kWsRot * h + bl + q;
+              const int b = R * h + bl + q;
               if (b >= nb) break;
               uint32_t pk[kWsW];
 #pragma unroll
@@ -439,7 +444,7 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
     __syncwarp();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
                  :
-                 : "r"(tmem), "r"(2 * kWsAccCols));
+                 : "r"(tmem), "r"(kWsTmemCols));
   }
   if (tid == 0 && *fail) atomicExch(err, 1);
 }
@@ -460,8 +465,9 @@ int xcorr_ws_config(int n0, int t0, int nb, XcorrTcConfig* cfg) {
   cudaGetLastError();
   cfg->sms = sms;
   if (cfg->ws_smem > (size_t)optin) return TM_OK;
-  for (auto fn : {xcorr_ws_kernel<2>, xcorr_ws_kernel<4>, xcorr_ws_kernel<6>,
-                  xcorr_ws_kernel<8>})
+  for (auto fn : {xcorr_ws_kernel<2, 16>, xcorr_ws_kernel<4, 16>, xcorr_ws_kernel<6, 16>,
+                  xcorr_ws_kernel<8, 16>, xcorr_ws_kernel<2, 32>, xcorr_ws_kernel<4, 32>,
+                  xcorr_ws_kernel<6, 32>, xcorr_ws_kernel<8, 32>})
     TM_TRY(cuda_status(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             optin),
                        "xcorr_ws: shared memory attribute"));
@@ -478,12 +484,14 @@ int xcorr_ws_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int
              "xcorr_ws_run: unsupported configuration");
   const int64_t nitems = (int64_t)n1 * ((h2 + kWsW - 1) / kWsW);
   const int grid = (int)std::min<int64_t>(nitems, cfg.sms);
-  auto fn = xcorr_ws_kernel<6>;
+  // one fill of all 32 rotations (single buffer) or two alternating fills of 16
+  const bool wide = cfg.ws_NB == 32;
+  auto fn = wide ? xcorr_ws_kernel<6, 32> : xcorr_ws_kernel<6, 16>;
   switch (cfg.ws_t0p) {
-    case 16: fn = xcorr_ws_kernel<2>; break;
-    case 32: fn = xcorr_ws_kernel<4>; break;
-    case 48: fn = xcorr_ws_kernel<6>; break;
-    case 64: fn = xcorr_ws_kernel<8>; break;
+    case 16: fn = wide ? xcorr_ws_kernel<2, 32> : xcorr_ws_kernel<2, 16>; break;
+    case 32: fn = wide ? xcorr_ws_kernel<4, 32> : xcorr_ws_kernel<4, 16>; break;
+    case 48: break;
+    case 64: fn = wide ? xcorr_ws_kernel<8, 32> : xcorr_ws_kernel<8, 16>; break;
     default: TM_REQUIRE(false, "xcorr_ws_run: t0p %d", cfg.ws_t0p);
   }
   fn<<<grid, kWsThreads, cfg.ws_smem, stream>>>(G, C, nb, cfg.ws_NB, t0, n0, n1, h2, hp, scale,
