@@ -17,6 +17,48 @@ import torch
 from .backend import backend as be
 from .matching import apply_convolution_mode
 
+_NUMPY_DTYPES = {torch.float32: np.float32, torch.int32: np.int32, torch.float64: np.float64,
+                 torch.int64: np.int64}
+_CHUNK = 16 << 20
+_staging: Dict[str, torch.Tensor] = {}
+
+
+def download(t: torch.Tensor) -> np.ndarray:
+    """A device tensor as a new host array.
+
+    Large tensors go through two pinned 16 MiB chunks, kept for the life of the process:
+    the copy engine fills one while the host copies the other into the result. A plain
+    ``.cpu()`` stages through pageable memory and moved the 420 MB state of a
+    512x512x200 scan at about 2 GB/s."""
+    t = t.contiguous()
+    nbytes = t.numel() * t.element_size()
+    if not t.is_cuda or nbytes < 2 * _CHUNK or t.dtype not in _NUMPY_DTYPES:
+        return t.cpu().numpy()
+    stage = _staging.get("pinned")
+    if stage is None:
+        stage = torch.empty(2 * _CHUNK, dtype=torch.uint8, pin_memory=True)
+        _staging["pinned"] = stage
+    out = np.empty(tuple(t.shape), dtype=_NUMPY_DTYPES[t.dtype])
+    src = t.view(-1).view(torch.uint8)
+    dst = out.reshape(-1).view(np.uint8)
+    stream = torch.cuda.current_stream(t.device)
+    done = [torch.cuda.Event(), torch.cuda.Event()]
+    pending = None
+    for i, off in enumerate(range(0, nbytes, _CHUNK)):
+        m = min(_CHUNK, nbytes - off)
+        # chunk i - 2 used this half and was copied out in the previous iteration
+        stage[(i % 2) * _CHUNK:(i % 2) * _CHUNK + m].copy_(src[off:off + m], non_blocking=True)
+        done[i % 2].record(stream)
+        if pending is not None:
+            j, poff, pm = pending
+            done[j % 2].synchronize()
+            dst[poff:poff + pm] = stage[(j % 2) * _CHUNK:(j % 2) * _CHUNK + pm].numpy()
+        pending = (i, off, m)
+    j, poff, pm = pending
+    done[j % 2].synchronize()
+    dst[poff:poff + pm] = stage[(j % 2) * _CHUNK:(j % 2) * _CHUNK + pm].numpy()
+    return out
+
 __all__ = [
     "SharedAnalyzerProxy",
     "MaxScoreOverRotations",
@@ -108,8 +150,8 @@ class MaxScoreOverRotations:
                         convolution_shape=convolution_shape)
             scores = apply_convolution_mode(scores, **args)
             rotations = apply_convolution_mode(rotations, **args)
-        scores = scores.contiguous().cpu().numpy()
-        rotations = rotations.contiguous().cpu().numpy()
+        scores = download(scores)
+        rotations = download(rotations)
         if self._inversion_mapping:
             mapping = {np.asarray(v, dtype=np.float32).tobytes(): k for k, v in mapping.items()}
         return scores, np.asarray(self._offset), rotations, self._invert_rmap(mapping)

@@ -227,7 +227,8 @@ class MatchingData:
         out = np.asarray(arr[tuple(slice(int(a), int(b)) for a, b in zip(a0, a1))])
         pads = tuple((int(l), int(r)) for l, r in zip(np.subtract(left, data_left),
                                                      np.subtract(right, data_right)))
-        out = np.pad(out, pads, mode="reflect")
+        if any(l or r for l, r in pads):  # without padding the slice is used as it is
+            out = np.pad(out, pads, mode="reflect")
         if invert:
             out = -out
         return out

@@ -451,3 +451,25 @@ def test_tensor_core_passes_mixed(torch_cuda, golden, xpass, zpass):
     assert np.abs(scores - g["scores32"]).max() <= tol
     assert np.abs(scores - g["scores64"]).max() <= tol
     _assert_argmax_ties(g, rot)
+
+
+@pytest.mark.parametrize("shape,dtype", [((173, 211, 97), "float32"), ((300, 301, 89), "int32"),
+                                         ((5, 7), "float32")])
+def test_state_download_matches_cpu_copy(torch_cuda, shape, dtype):
+    """The chunked download through pinned staging (used for the analyzer's result) is
+    byte-identical to a plain device-to-host copy, for sizes that are not a multiple of
+    the chunk, twice in a row (the staging buffer is reused)."""
+    import torch
+    from pytme_b200.analyzer import download
+
+    for seed in (0, 1):
+        g = torch.Generator(device="cuda").manual_seed(seed)
+        if dtype == "float32":
+            t = torch.randn(shape, generator=g, device="cuda")
+        else:
+            t = torch.randint(-2**31, 2**31 - 1, shape, generator=g, device="cuda",
+                              dtype=torch.int32)
+        got = download(t)
+        want = t.cpu().numpy()
+        assert got.shape == want.shape and got.dtype == want.dtype
+        assert np.array_equal(got.view(np.uint8), want.view(np.uint8))
