@@ -272,6 +272,22 @@ typedef struct {
 int tm_build_filter(const tm_filter_component* components, int n_components,
                     const int* shape, int rfft, float* out, void* stream);
 
+/* LinearWhiteningFilter (tme/filters/whitening.py:23-186) on the device: the inverse
+ * square root of the radially averaged power spectrum of the data, normalised to a
+ * maximum of 1 and interpolated linearly on the frequency grid of a filter of real shape
+ * `shape`, returned like tm_build_filter (float32, DC at index 0, rfft layout when rfft is
+ * non-zero). `data_rfft`: complex64 rfft of the data, rfft shape data_ft_shape (the
+ * reference's bins are defined on this shape); in the scan path the data is the target
+ * padded to the fast shape (tme/matching_exhaustive.py:84-90). n_bins <= 0 selects the
+ * reference's default. `factor` (optional, same layout as out) multiplies the filter in
+ * float64 before the single rounding to float32, as Compose multiplies a float64
+ * whitening array with the product of the other filters. `work`: device scratch of
+ * 3 * tm_whitening_bins(data_ft_shape, n_bins) doubles. */
+int tm_whitening_bins(const int* data_ft_shape, int n_bins);
+int tm_whitening_filter(const void* data_rfft, const int* data_ft_shape, int n_bins,
+                        const int* shape, int rfft, double* work, const float* factor,
+                        float* out, void* stream);
+
 /* ---- local refinement of candidate peaks: the FLC of flc_scoring
  * (tme/matching_scores.py:629-759) at one pose per peak and its adjoint. This
  * replaces the derivative-free score of tme/matching_optimization.py:54-277 and

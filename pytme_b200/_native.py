@@ -43,7 +43,8 @@ EXPORTED = (
     "tm_find_candidate_indices_noalloc", "tm_line_fft_test", "tm_fft_filter",
     "tm_euler_zyz", "tm_refine_rotate", "tm_refine_forward", "tm_refine_grad_filtered",
     "tm_refine_backward", "tm_spline_prefilter", "tm_rigid_transform_cubic",
-    "tm_scan_set_interpolation", "tm_build_filter", "tm_xcorr_tc_test",
+    "tm_scan_set_interpolation", "tm_build_filter", "tm_whitening_bins", "tm_whitening_filter",
+    "tm_xcorr_tc_test",
     "tm_scan_set_xpass", "tm_scan_check", "tm_scan_xpass_mode", "tm_scan_set_zpass",
     "tm_scan_zpass_mode",
 )
@@ -136,6 +137,9 @@ def _load():
         "tm_scan_set_zpass": (c_int, [vp, c_int]),
         "tm_scan_zpass_mode": (c_int, [vp]),
         "tm_build_filter": (c_int, [vp, c_int, POINTER(c_int), c_int, f32p, vp]),
+        "tm_whitening_bins": (c_int, [POINTER(c_int), c_int]),
+        "tm_whitening_filter": (c_int, [vp, POINTER(c_int), c_int, POINTER(c_int), c_int, vp,
+                                        vp, f32p, vp]),
         "tm_xcorr_tc_test": (c_int, [vp, vp, c_int, c_int, c_int, c_int, c_int, c_float, vp,
                                      c_int, vp]),
         "tm_euler_zyz": (c_int, [f32p, c_int, f32p, f32p, vp]),

@@ -21,8 +21,8 @@ from typing import Dict, List, Optional, Sequence, Tuple
 import numpy as np
 import torch
 
-from .matching import (_evaluate_filter, apply_convolution_mode, fourier_padding,
-                       rigid_transform_matrices)
+from .matching import (TargetSpectrum, _evaluate_filter, apply_convolution_mode,
+                       fourier_padding, rigid_transform_matrices)
 from .scores import ScanPlan, _prepare_target
 
 __all__ = ["MatchJob", "scan_batch", "autotune_batch"]
@@ -89,8 +89,10 @@ def autotune_batch(job: MatchJob, precision: str = "mixed",
     t_rev = np.ascontiguousarray(job.template[::-1, ::-1, ::-1], dtype=np.float32)
     m_rev = None if job.mask is None else np.ascontiguousarray(job.mask[::-1, ::-1, ::-1],
                                                                    dtype=np.float32)
-    tf = _evaluate_filter(job.template_filter, job.template.shape)
-    gf = _evaluate_filter(job.target_filter, tuple(fast), weight_type=None)
+    spec = TargetSpectrum(job.target, tuple(fast))
+    tf = _evaluate_filter(job.template_filter, job.template.shape, data_rfft=spec)
+    gf = _evaluate_filter(job.target_filter, tuple(fast), data_rfft=spec, weight_type=None)
+    del spec
     target = _prepare_target(job.target, tuple(fast), gf)
     center = np.divide(np.asarray(job.template.shape) - 1, 2)
     dev = target.device
@@ -155,9 +157,13 @@ def scan_batch(jobs: List[MatchJob], precision: str = "mixed", rotation_batch="a
             t_rev = np.ascontiguousarray(tmpl[::-1, ::-1, ::-1])
             m_rev = None if job.mask is None else np.ascontiguousarray(
                 np.asarray(job.mask, dtype=np.float32)[::-1, ::-1, ::-1])
-            plan.set_template(t_rev, m_rev, _evaluate_filter(job.template_filter, tmpl.shape))
+            spec = TargetSpectrum(job.target, tuple(fast))
+            plan.set_template(t_rev, m_rev, _evaluate_filter(job.template_filter, tmpl.shape,
+                                                             data_rfft=spec))
             plan.set_interpolation(job.interpolation_order)
-            gf = _evaluate_filter(job.target_filter, tuple(fast), weight_type=None)
+            gf = _evaluate_filter(job.target_filter, tuple(fast), data_rfft=spec,
+                                  weight_type=None)
+            del spec
             target = _prepare_target(job.target, tuple(fast), gf)
             plan.set_target(target)
             dev = target.device

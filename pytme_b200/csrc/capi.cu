@@ -345,6 +345,18 @@ int tm_build_filter(const tm_filter_component* components, int n_components, con
   return tmb::build_filter(components, n_components, shape, rfft, out, S(stream));
 }
 
+int tm_whitening_bins(const int* data_ft_shape, int n_bins) {
+  if (!data_ft_shape) return TM_E_INVALID;
+  return tmb::whitening_bins(data_ft_shape, n_bins);
+}
+
+int tm_whitening_filter(const void* data_rfft, const int* data_ft_shape, int n_bins,
+                        const int* shape, int rfft, double* work, const float* factor,
+                        float* out, void* stream) {
+  return tmb::whitening_filter(static_cast<const float2*>(data_rfft), data_ft_shape, n_bins,
+                               shape, rfft, work, factor, out, S(stream));
+}
+
 int tm_euler_zyz(const float* angles, int n, float* rot, float* drot, void* stream) {
   return tmb::euler_zyz(angles, n, rot, drot, S(stream));
 }

@@ -25,6 +25,14 @@ int rigid_transform_cubic(const double* coef, const double* mcoef, int d0, int d
                           const float* matrices, int n_mat, float* out, float* out_mask, int o0,
                           int o1, int o2, cudaStream_t stream);
 
+// Bins of the whitening filter for a data spectrum of rfft shape data_ft_shape
+// (n_bins <= 0: the reference's default).
+int whitening_bins(const int* data_ft_shape, int n_bins);
+// Whitening filter from the complex64 rfft of the data; work: 3 * bins doubles; factor
+// (optional) multiplies the result before the rounding to float32.
+int whitening_filter(const float2* data_rfft, const int* data_ft_shape, int n_bins,
+                     const int* shape, int rfft, double* work, const float* factor, float* out,
+                     cudaStream_t stream);
 int build_filter(const tm_filter_component* comps, int n_comp, const int* shape, int rfft,
                  float* out, cudaStream_t stream);
 

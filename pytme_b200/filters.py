@@ -25,7 +25,7 @@ import numpy as np
 
 __all__ = ["fftfreqn", "shift_fourier", "crop_real_fourier", "create_ctf",
            "CTFReconstructed", "WedgeReconstructed", "LinearWhiteningFilter", "Compose",
-           "device_filter"]
+           "device_filter", "needs_spectrum"]
 
 
 def fftfreqn(shape, sampling_rate, compute_euclidean_norm=False, shape_is_real_fourier=False):
@@ -341,12 +341,24 @@ def _wedge_component(f: "WedgeReconstructed", shape, kwargs: Dict):
                 -1.0 if cutoff is None else float(cutoff)])
 
 
-def device_filter(filt, shape, return_real_fourier: bool = True, **kwargs):
-    """Build ``CTFReconstructed``, ``WedgeReconstructed`` or a ``Compose`` of them on the
-    current GPU (``tm_build_filter``) and return it as a float32 torch tensor with the
-    DC term at index 0, equal to ``filt(shape=shape, return_real_fourier=...)["data"]``.
-    Raises ``NotImplementedError`` for filters it does not cover (astigmatic CTFs,
-    weighted or per-angle wedges, whitening, other classes)."""
+def needs_spectrum(filt) -> bool:
+    """Whether evaluating ``filt`` needs the data spectrum (``data_rfft``): everything but
+    CTFs and wedges (whitening, unknown classes) gets it."""
+    items = filt.transforms if isinstance(filt, Compose) else [filt]
+    return any(type(f) not in (CTFReconstructed, WedgeReconstructed) for f in items)
+
+
+def device_filter(filt, shape, return_real_fourier: bool = True, data_rfft=None, **kwargs):
+    """Build ``CTFReconstructed``, ``WedgeReconstructed``, ``LinearWhiteningFilter`` or a
+    ``Compose`` of them on the current GPU (``tm_build_filter``, ``tm_whitening_filter``)
+    and return it as a float32 torch tensor with the DC term at index 0, equal to
+    ``filt(shape=shape, return_real_fourier=..., data_rfft=data_rfft)["data"]``.
+
+    Whitening needs ``data_rfft``, the complex64 rfft of the data on the device. It is
+    built on the device alone or composed with at most one CTF and any wedges, where the
+    reference's float64 product rounds the same whatever the order. Raises
+    ``NotImplementedError`` for what it does not cover (astigmatic CTFs, weighted or
+    per-angle wedges, several whitening filters or CTFs with whitening, other classes)."""
     import torch
 
     from . import _native as N
@@ -357,24 +369,48 @@ def device_filter(filt, shape, return_real_fourier: bool = True, **kwargs):
     if not torch.cuda.is_available():
         raise NotImplementedError("no CUDA device: filters are built on the host")
     items = filt.transforms if isinstance(filt, Compose) else [filt]
-    comps = []
+    comps, whiten = [], []
     for f in items:
         if type(f) is CTFReconstructed:
             comps.append(_ctf_component(f, kwargs))
         elif type(f) is WedgeReconstructed:
             comps.append(_wedge_component(f, shape, kwargs))
+        elif type(f) is LinearWhiteningFilter:
+            whiten.append(f)
         else:
             raise NotImplementedError(f"{type(f).__name__} is built on the host")
-    if not 1 <= len(comps) <= N.TM_FILTER_MAX_COMPONENTS:
+    if len(comps) > N.TM_FILTER_MAX_COMPONENTS or not (comps or whiten):
         raise NotImplementedError("1 to 4 filter components are built on the device")
-    arr = (N.FilterComponent * len(comps))()
-    for i, (kind, p) in enumerate(comps):
-        arr[i].kind = kind
-        for j, v in enumerate(p):
-            arr[i].p[j] = v
+    if len(whiten) > 1 or (whiten and sum(k == 1 for k, _ in comps) > 1):
+        raise NotImplementedError("this whitening composition is built on the host")
+    if whiten and (not isinstance(data_rfft, torch.Tensor) or not data_rfft.is_cuda
+                   or data_rfft.dim() != 3):
+        raise NotImplementedError("whitening on the device needs the data spectrum on the GPU")
+    if whiten and (kwargs.get("order", 1) != 1 or kwargs.get("batch_dimension") is not None):
+        raise NotImplementedError("whitening with order != 1 or batches is built on the host")
     out_shape = shape[:-1] + ((shape[-1] // 2 + 1) if return_real_fourier else shape[-1],)
     out = torch.empty(out_shape, dtype=torch.float32, device=torch.device("cuda"))
     dims = (N.c_int * 3)(*shape)
-    N.check(N.lib.tm_build_filter(arr, len(comps), dims, int(bool(return_real_fourier)),
-                                  N.ptr(out), N.stream_ptr()), "tm_build_filter")
+    rf = int(bool(return_real_fourier))
+    if comps:
+        arr = (N.FilterComponent * len(comps))()
+        for i, (kind, p) in enumerate(comps):
+            arr[i].kind = kind
+            for j, v in enumerate(p):
+                arr[i].p[j] = v
+        N.check(N.lib.tm_build_filter(arr, len(comps), dims, rf, N.ptr(out), N.stream_ptr()),
+                "tm_build_filter")
+    if whiten:
+        spec = data_rfft.to(torch.complex64).contiguous()
+        ft = (N.c_int * 3)(*spec.shape)
+        n_bins = kwargs.get("n_bins")
+        n_bins = 0 if n_bins is None else int(n_bins)
+        nb = N.lib.tm_whitening_bins(ft, n_bins)
+        if nb < 2:
+            raise ValueError(f"whitening: {nb} bins")
+        work = torch.empty(3 * nb, dtype=torch.float64, device=out.device)
+        # the other components' product (if any) is the float32 factor of the whitening
+        N.check(N.lib.tm_whitening_filter(N.ptr(spec), ft, n_bins, dims, rf, N.ptr(work),
+                                          N.ptr(out) if comps else None, N.ptr(out),
+                                          N.stream_ptr()), "tm_whitening_filter")
     return out

@@ -266,22 +266,51 @@ class MatchingData:
         return out
 
 
+class TargetSpectrum:
+    """The complex64 rfft of the target padded (top-left) to the fast shape, computed on
+    the device the first time a filter asks for it: the ``data_rfft`` that the
+    reference's filter set-up hands to every filter (tme/matching_exhaustive.py:84-90)."""
+
+    def __init__(self, target, fast_shape):
+        self._target, self._fast = target, tuple(int(x) for x in fast_shape)
+        self._ft = None
+
+    def get(self):
+        if self._ft is None:
+            from .backend import backend as be
+
+            t = torch.as_tensor(np.asarray(self._target, dtype=np.float32)) \
+                if not isinstance(self._target, torch.Tensor) else self._target
+            self._ft = be.rfftn(t.to(torch.float32), s=self._fast)
+        return self._ft
+
+
 def _evaluate_filter(filt, shape, data_rfft=None, **kwargs):
     """A filter is either an array (already at the right rfft shape) or a callable
     with the reference's filter interface (``__call__(shape=..., return_real_fourier=
-    True, ...)`` returning a dict with ``data``)."""
+    True, data_rfft=..., ...)`` returning a dict with ``data``). ``data_rfft`` is the
+    target's spectrum, or a ``TargetSpectrum`` that computes it when a filter needs it
+    (whitening)."""
     if filt is None:
         return None
     if callable(filt):
-        from .filters import device_filter
+        from .filters import device_filter, needs_spectrum
 
+        spec = None
+        if data_rfft is not None and needs_spectrum(filt):
+            spec = data_rfft.get() if isinstance(data_rfft, TargetSpectrum) else data_rfft
         try:
-            # CTFs, continuous wedges and their Compose are built on the GPU
-            return device_filter(filt, shape, return_real_fourier=True)
+            # CTFs, continuous wedges, whitening and their Compose are built on the GPU
+            return device_filter(filt, shape, return_real_fourier=True, data_rfft=spec,
+                                 **kwargs)
         except NotImplementedError:
             pass
+        if isinstance(spec, torch.Tensor):
+            from .analyzer import download
+
+            spec = download(spec)
         ret = filt(shape=shape, return_real_fourier=True, shape_is_real_fourier=False,
-                   data_rfft=data_rfft, batch_dimension=None, **kwargs)
+                   data_rfft=spec, batch_dimension=None, **kwargs)
         return np.asarray(ret["data"], dtype=np.float32)
     if isinstance(filt, torch.Tensor):
         return filt.to(torch.float32)
@@ -305,8 +334,10 @@ def scan(matching_data: MatchingData, matching_setup: Callable, matching_score: 
         target_pad=matching_data.target_padding(pad_target=pad_target))
     conv, fwd, inv, shift = md.fourier_padding(pad_target=pad_target)
 
-    template_filter = _evaluate_filter(md.template_filter, md._template.shape)
-    target_filter = _evaluate_filter(md.target_filter, fwd, weight_type=None)
+    spectrum = TargetSpectrum(md._target, fwd)
+    template_filter = _evaluate_filter(md.template_filter, md._template.shape, data_rfft=spectrum)
+    target_filter = _evaluate_filter(md.target_filter, fwd, data_rfft=spectrum, weight_type=None)
+    del spectrum
     if template_filter is not None and pad_template_filter:
         raise NotImplementedError("pad_template_filter=True is not supported; the "
                                   "template filter is applied at template shape")

@@ -35,7 +35,7 @@ import numpy as np
 import torch
 
 from . import _native as N
-from .matching import _evaluate_filter, fourier_padding
+from .matching import TargetSpectrum, _evaluate_filter, fourier_padding
 from .scores import _prepare_target, _to_device
 
 __all__ = [
@@ -156,7 +156,8 @@ class RefineProblem:
         self.template_shape = tuple(int(x) for x in template.shape)
         self.target_shape = tshape
         _, fast, _, _ = fourier_padding(tshape, self.template_shape)
-        tf = _evaluate_filter(target_filter, fast, weight_type=None)
+        spec = TargetSpectrum(target, fast)
+        tf = _evaluate_filter(target_filter, fast, data_rfft=spec, weight_type=None)
         padded = _prepare_target(target, tuple(fast), tf)
         tgt = padded[tuple(slice(0, n) for n in tshape)].contiguous()
         mean = tgt.double().mean().float()
@@ -167,7 +168,8 @@ class RefineProblem:
         self.template = _to_device(template)
         self.mask = _to_device(mask)
         self.eps = float(eps)
-        filt = _evaluate_filter(template_filter, self.template_shape)
+        filt = _evaluate_filter(template_filter, self.template_shape, data_rfft=spec)
+        del spec
         self.template_filter = None if filt is None else _to_device(filt)
         if self.template_filter is not None:
             ft = self.template_shape[:2] + (self.template_shape[2] // 2 + 1,)

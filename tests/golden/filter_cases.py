@@ -33,3 +33,26 @@ def build_filter_case(case, ctf_cls, wedge_cls, compose_cls):
     return compose_cls(objs)(shape=shape, return_real_fourier=rfft)["data"]
 
 
+
+
+# Whitening by the power spectrum of seeded data: (data shape, filter shape,
+# return_real_fourier, n_bins). The data is normal noise times a radial ramp (a spectrum
+# that is not flat), seed = case index; its rfft in complex64 is what the filter gets.
+WHITENING_CASES = [
+    ((24, 20, 16), (24, 20, 16), True, None),
+    ((21, 17, 15), (21, 17, 15), True, None),
+    ((24, 20, 16), (12, 12, 12), True, None),
+    ((16, 16, 16), (16, 16, 16), False, None),
+    ((20, 24, 18), (20, 24, 18), True, 7),
+]
+
+
+def whitening_data(case_index, shape):
+    """The seeded data of a whitening case and its complex64 rfft."""
+    import numpy as np
+
+    rng = np.random.default_rng(case_index)
+    grids = np.meshgrid(*[np.arange(n) - n / 2 for n in shape], indexing="ij")
+    ramp = 1.0 + np.sqrt(sum(g * g for g in grids))
+    data = (rng.normal(size=shape) * ramp).astype(np.float32)
+    return data, np.fft.rfftn(data).astype(np.complex64)

@@ -132,6 +132,21 @@ def _filters():
     np.savez_compressed(os.path.join(HERE, "filters.npz"), **out)
 
 
+def _whitening():
+    """LinearWhiteningFilter arrays of WHITENING_CASES from the reference, given the
+    complex64 spectrum of the case's seeded data."""
+    from tme.filters import LinearWhiteningFilter
+    from filter_cases import WHITENING_CASES, whitening_data
+
+    out = {}
+    for i, (dshape, fshape, rfft, n_bins) in enumerate(WHITENING_CASES):
+        _, data_rfft = whitening_data(i, dshape)
+        ret = LinearWhiteningFilter()(shape=fshape, data_rfft=data_rfft, n_bins=n_bins,
+                                      return_real_fourier=rfft)["data"]
+        out[f"case{i}"] = np.asarray(ret)
+    np.savez_compressed(os.path.join(HERE, "whitening.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("PYTME_REFERENCE",
@@ -153,6 +168,10 @@ def main():
 
     if args.only == "cubic":
         _cubic(be, create_mask, syn)
+        print("golden vectors written to", HERE)
+        return
+    if args.only == "whitening":
+        _whitening()
         print("golden vectors written to", HERE)
         return
     if args.only == "filters":
@@ -268,6 +287,7 @@ def main():
 
     _cubic(be, create_mask, syn)
     _filters()
+    _whitening()
 
     # ---- rigid transforms (order 1, constant mode), both matrix forms
     be.change_backend("numpyfftw")

@@ -84,3 +84,78 @@ def test_device_filters_config4_time():
     print(f"config-4 filters: device {t_dev * 1e3:.1f} ms, host {t_host * 1e3:.0f} ms "
           f"(extrapolated from 6 of {len(jobs)} pairs)")
     assert t_dev < t_host
+
+
+# ----------------------------------------------------------------------------- whitening
+from tests.golden.filter_cases import WHITENING_CASES, whitening_data  # noqa: E402
+
+
+@pytest.mark.parametrize("i", range(len(WHITENING_CASES)))
+def test_host_whitening_bit_exact(golden, i):
+    """The host restatement of LinearWhiteningFilter against the reference's arrays
+    (tests/golden/whitening.npz), from the same complex64 spectrum."""
+    g = golden("whitening.npz")[f"case{i}"]
+    dshape, fshape, rfft, n_bins = WHITENING_CASES[i]
+    _, spec = whitening_data(i, dshape)
+    got = F.LinearWhiteningFilter()(shape=fshape, data_rfft=spec, n_bins=n_bins,
+                                    return_real_fourier=rfft)["data"]
+    assert got.shape == g.shape
+    assert np.array_equal(got, g)
+
+
+def test_whitening_through_filter_evaluation_on_host():
+    """A whitening filter in the scan's filter evaluation gets the target spectrum (the
+    reference hands data_rfft to every filter); without a GPU it is built on the host."""
+    from pytme_b200.matching import _evaluate_filter
+
+    _, spec = whitening_data(0, WHITENING_CASES[0][0])
+    got = _evaluate_filter(F.Compose([F.LinearWhiteningFilter()]), WHITENING_CASES[0][1],
+                           data_rfft=spec, weight_type=None)
+    want = F.LinearWhiteningFilter()(shape=WHITENING_CASES[0][1], data_rfft=spec)["data"]
+    assert np.array_equal(got, want.astype(np.float32))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("i", range(len(WHITENING_CASES)))
+def test_device_whitening_matches_reference(golden, i):
+    """tm_whitening_filter against the reference's arrays from the same spectrum: the
+    per-bin float64 sums run in another order, so values may differ in the last float32
+    bit."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    g = golden("whitening.npz")[f"case{i}"].astype(np.float32)
+    dshape, fshape, rfft, n_bins = WHITENING_CASES[i]
+    _, spec = whitening_data(i, dshape)
+    got = F.device_filter(F.LinearWhiteningFilter(), fshape, return_real_fourier=rfft,
+                          data_rfft=torch.from_numpy(spec).cuda(), n_bins=n_bins)
+    got = got.cpu().numpy()
+    assert got.shape == g.shape
+    ulp = np.abs(got.view(np.int32).astype(np.int64) - g.view(np.int32).astype(np.int64))
+    assert ulp.max() <= 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", [(0, 1, 2), (1, 0, 2), (2, 1, 0)])
+def test_device_whitening_composed_with_ctf_and_wedge(order):
+    """Whitening x CTF x wedge in any order on the device equals the host Compose (float64
+    product rounded once to float32) within one float32 ulp."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    dshape = (24, 20, 16)
+    _, spec = whitening_data(0, dshape)
+    items = [F.LinearWhiteningFilter(),
+             F.CTFReconstructed(defocus_x=30000.0, sampling_rate=6.8),
+             F.WedgeReconstructed(angles=(60, 60), opening_axis=2, tilt_axis=0,
+                                  create_continuous_wedge=True)]
+    filt = F.Compose([items[j] for j in order])
+    want = np.asarray(filt(shape=dshape, return_real_fourier=True, data_rfft=spec)["data"],
+                      dtype=np.float32)
+    got = F.device_filter(filt, dshape, return_real_fourier=True,
+                          data_rfft=torch.from_numpy(spec).cuda()).cpu().numpy()
+    # the device CTF itself may differ from the host's by one ulp at a few voxels
+    ulp = np.abs(got.view(np.int32).astype(np.int64) - want.view(np.int32).astype(np.int64))
+    assert ulp.max() <= 2

@@ -473,3 +473,36 @@ def test_state_download_matches_cpu_copy(torch_cuda, shape, dtype):
         want = t.cpu().numpy()
         assert got.shape == want.shape and got.dtype == want.dtype
         assert np.array_equal(got.view(np.uint8), want.view(np.uint8))
+
+
+@pytest.mark.parametrize("score", ["FLCSphericalMask", "FLC"])
+def test_whitening_filters_in_scan(torch_cuda, score):
+    """Whitening by the target's power spectrum as the target filter, and whitening x CTF
+    x wedge as the template filter, passed to the scan as filter objects: the scan builds
+    them on the device from the spectrum of the padded target, as the reference hands
+    data_rfft to every filter (tme/matching_exhaustive.py:84-90). The oracle gets the
+    arrays of the host restatement (pinned to the reference's whitening arrays) from a
+    NumPy spectrum of the same target."""
+    from pytme_b200 import synthetic as syn
+    from pytme_b200.filters import (Compose, CTFReconstructed, LinearWhiteningFilter,
+                                    WedgeReconstructed)
+
+    rng = np.random.default_rng(37)
+    tmpl = syn.blob_template(10, rng, radius=3.0, sigma=1.1)
+    mask = syn.spherical_mask((10,) * 3, 5, center=(4.5,) * 3)
+    target, _, _ = syn.make_tomogram((48, 40, 32), tmpl, 4, rng, snr=0.5, mask=mask)
+    rots = syn.random_rotation_matrices(9, rng)
+    ctf = CTFReconstructed(defocus_x=25000, sampling_rate=6.8)
+    wedge = WedgeReconstructed(angles=(60, 60), opening_axis=2, tilt_axis=0,
+                               create_continuous_wedge=True)
+    tfilt = Compose([LinearWhiteningFilter(), ctf, wedge])
+    gfilt = Compose([LinearWhiteningFilter()])
+    r = _scan(score, target, tmpl, mask, rots, precision="fp32", batch=4,
+              template_filter=tfilt, target_filter=gfilt)
+    spec = np.fft.rfftn(target).astype(np.complex64)  # fast shape = target shape here
+    tf = tfilt(shape=tmpl.shape, return_real_fourier=True, data_rfft=spec)["data"]
+    gf = gfilt(shape=target.shape, return_real_fourier=True, data_rfft=spec)["data"]
+    ref = O.scan(target, tmpl, rots, score, template_mask=mask,
+                 template_filter=np.asarray(tf, np.float32),
+                 target_filter=np.asarray(gf, np.float32))
+    assert np.abs(r[0] - ref["scores"]).max() <= TOL
