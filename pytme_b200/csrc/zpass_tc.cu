@@ -346,7 +346,24 @@ __device__ __forceinline__ void mbar_track_cp_async(uint64_t* bar) {
 //   bempty[s]  MMAs of the block done: its rotation-operand buffer is free (commit)
 //   tfull[s]   accumulators of the block written (commit)
 //   tempty[s]  epilogue done: accumulators and state buffers free (count: epilogue)
-// MT: loader tasks per thread, ceil(256 * ceil(ceil(h2 / 4) / 4) / kZLoaders).
+// Roles: warp 0 issues the MMAs; warps 4-7 run the epilogue (one per tensor-memory lane
+// quarter, every row of a block); the loaders form two groups, warps 1-3 and 8-10
+// (192 threads) for the blocks of even index and warps 11-15 (160 threads) for the odd
+// ones, so each group has two block periods for the DRAM round trip of its loads. With
+// an even number of stages a stage always belongs to the same group.
+constexpr int kEoEpi = 128;
+constexpr int kEoGroup0 = 192, kEoGroup1 = 160;
+static_assert(kEoS % 2 == 0, "stages alternate between the two loader groups");
+__device__ __forceinline__ bool eo_epilogue_warp(int w) { return w >= 4 && w < 8; }
+__device__ __forceinline__ int eo_loader_group(int w) { return w <= 10 ? 0 : 1; }
+__device__ __forceinline__ int eo_loader_index(int tid) {
+  const int w = tid >> 5;
+  if (w < 4) return tid - 32;           // warps 1-3: 0..95
+  if (w <= 10) return tid - 256 + 96;   // warps 8-10: 96..191
+  return tid - 352;                     // warps 11-15: 0..159
+}
+
+// MT: loader tasks per thread of the smaller group, ceil(256 * ceil(ceil(h2/4)/4) / 160).
 template <int MT>
 __global__ void __launch_bounds__(kZThreads, 1)
 zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int h2, int hp,
@@ -385,10 +402,10 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
     reinterpret_cast<uint2*>(Bs)[i] = make_uint2(0u, 0u);
   if (tid == 0) {
     for (int q = 0; q < kEoS; ++q) {
-      mbar_init(bfull + q, kZLoaders);
+      mbar_init(bfull + q, (q & 1) ? kEoGroup1 : kEoGroup0);
       mbar_init(bempty + q, 1);
       mbar_init(tfull + q, 1);
-      mbar_init(tempty + q, kZEpi);
+      mbar_init(tempty + q, kEoEpi);
     }
     mbar_init(mdone, 1);
     asm volatile("fence.mbarrier_init.release.cluster;");
@@ -405,11 +422,15 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
   const int zmax = n2 / 2;              // rows z <= zmax of the tile are outputs
   const int zodd = (n2 + 1) / 2 - 1;    // z in [1, zodd] also gives x[n2 - z]
 
-  if (warp != 0 && !zp_epilogue_warp(warp)) {
+  if (warp != 0 && !eo_epilogue_warp(warp)) {
     // ---------------------------------------------------------------- loaders
-    const int lt = zp_loader_index(tid);
-    for (int i = lt; i < (int)(4 * tab / 8); i += kZLoaders)
-      cp_async16(smem_u32(As) + 16u * i, Ag + 8 * (size_t)i, 16);
+    const int grp = eo_loader_group(warp);
+    const int gsz = grp ? kEoGroup1 : kEoGroup0;
+    const int lt = eo_loader_index(tid);
+    // the operator tables, tracked by block 0's barrier (group 0)
+    if (grp == 0)
+      for (int i = lt; i < (int)(4 * tab / 8); i += kEoGroup0)
+        cp_async16(smem_u32(As) + 16u * i, Ag + 8 * (size_t)i, 16);
     // task i = (quad of 4-value chunks i >> 8, 8-row group (i >> 5) & 7, lane i & 31):
     // lanes 0-7 take rows 0-7 of chunk 4q, lanes 8-15 chunk 4q + 1, ...: 64 contiguous
     // bytes per H row per warp access, and 8-byte shared stores that fill two core
@@ -424,7 +445,7 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
     uint32_t task[MT];
 #pragma unroll
     for (int m = 0; m < MT; ++m) {
-      const int i = lt + m * kZLoaders;
+      const int i = lt + m * gsz;
       const int ln = i & 31, ng = (i >> 5) & 7;
       const int n = ng * 8 + (ln & 7), kq = (i >> 8) * 4 + (ln >> 3);
       const int r = n >> 5, b = n & (kZRot - 1);
@@ -432,7 +453,7 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
       task[m] = (uint32_t)kmajor16(n, 4 * (kq & 31), K2) | ((uint32_t)(kq & 31) << 16) |
                 ((uint32_t)b << 21) | ((uint32_t)r << 26) | (live ? 1u << 28 : 0u);
     }
-    for (int64_t j = 0; j < mine; ++j) {
+    for (int64_t j = grp; j < mine; j += 2) {
       const int sidx = (int)(j % kEoS);
       const uint32_t u = (uint32_t)(j / kEoS);
       if (j >= kEoS && !mbar_wait(smem_u32(bempty + sidx), (u - 1) & 1u)) { *fail = 1; break; }
@@ -456,13 +477,13 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
       const int64_t gend = rows * n2;
       const uint32_t sd = smem_u32(sst + sidx * kEoRows * n2);
       const uint32_t dd = smem_u32(sden + sidx * kEoRows * n2);
-      for (int q = lt; q < nqs; q += kZLoaders) {
+      for (int q = lt; q < nqs; q += gsz) {
         const int64_t g = g0 + 4 * q;
         const uint32_t bytes = g + 4 <= gend ? 16u : (g < gend ? (uint32_t)(gend - g) * 4u : 0u);
         cp_async16(sd + 16u * q, bytes ? state_max + g : state_max, bytes);
       }
       if (inv_den) {
-        for (int q = lt; q < nqs; q += kZLoaders) {
+        for (int q = lt; q < nqs; q += gsz) {
           const int64_t g = g0 + 4 * q;
           const uint32_t bytes = g + 4 <= gend ? 16u : (g < gend ? (uint32_t)(gend - g) * 4u : 0u);
           cp_async16(dd + 16u * q, bytes ? inv_den + g : state_max, bytes);
@@ -531,7 +552,7 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
     }
   } else {
     // ---------------------------------------------------------------- epilogue
-    const int quarter = warp & 3, egrp = warp >> 3;
+    const int quarter = warp & 3;
     const int z = quarter * 32 + lane;
     bool ok = true;
     for (int64_t j = 0; j < mine && ok; ++j) {
@@ -546,7 +567,7 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
       const float* st = sst + sidx * kEoRows * n2;
       const float* dn = sden + sidx * kEoRows * n2;
 #pragma unroll 1
-      for (int r = egrp; r < kEoRows; r += 2) {
+      for (int r = 0; r < kEoRows; ++r) {
         float ev[32], ov[32];
         tmem_ld32(tb + (uint32_t)(r * kZRot), ev);
         tmem_ld32(tb + (uint32_t)(kEoN + r * kZRot), ov);
@@ -618,7 +639,7 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
 // loader tasks per thread of the even/odd kernel
 static int eo_tasks(int h2) {
   const int nquad = ((h2 + 3) / 4 + 3) / 4;
-  return (nquad * 256 + kZLoaders - 1) / kZLoaders;
+  return (nquad * 256 + kEoGroup1 - 1) / kEoGroup1;
 }
 
 int zpass_tc_config(int n2, int h2, int hp, int nb, ZpassTcConfig* cfg) {
@@ -642,8 +663,8 @@ int zpass_tc_config(int n2, int h2, int hp, int nb, ZpassTcConfig* cfg) {
   cudaGetLastError();
   cfg->sms = sms;
   // even/odd form: z <= n2/2 in one M = 128 tile
-  if (n2 >= 16 && n2 / 2 + 1 <= 128 && eo_tasks(h2) <= 10 && cfg->eo_smem <= (size_t)optin) {
-    for (auto fn : {zpass_eo_kernel<8>, zpass_eo_kernel<10>})
+  if (n2 >= 16 && n2 / 2 + 1 <= 128 && eo_tasks(h2) <= 13 && cfg->eo_smem <= (size_t)optin) {
+    for (auto fn : {zpass_eo_kernel<12>, zpass_eo_kernel<13>})
       TM_TRY(cuda_status(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               optin),
                          "zpass_tc: shared memory attribute"));
@@ -686,7 +707,7 @@ int zpass_tc_run(const ZpassTcConfig& cfg, const void* H, int nb, int64_t rows, 
   if (cfg.eo) {
     const int64_t nblk = (rows + kEoRows - 1) / kEoRows;
     const int grid = (int)std::min<int64_t>(nblk, cfg.sms);
-    auto fn = eo_tasks(h2) <= 8 ? zpass_eo_kernel<8> : zpass_eo_kernel<10>;
+    auto fn = eo_tasks(h2) <= 12 ? zpass_eo_kernel<12> : zpass_eo_kernel<13>;
     fn<<<grid, kZThreads, cfg.eo_smem, stream>>>(
         static_cast<const __half2*>(H), nb, rows, n2, h2, hp, cfg.Kp, table, scale, inv_den,
         first_index, state_max, state_rot, SH, first_dev, err);
