@@ -283,9 +283,10 @@ zpass_tc_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
 // of the MMAs of the two-tile form for the same outputs. The rotation operand holds each
 // H row de-interleaved, [Re X[0..K') | Im X[0..K')] (the loaders split the FP16 complex
 // values in registers). Blocks are 2 rows x 32 rotations (N = 64) in a ring of 4 stages
-// (operand buffer, E and O accumulators in 128 tensor-memory columns, state): the loads
-// of three blocks are in flight while one is multiplied. With 4-row blocks in 2 stages
-// the loaders' DRAM round trip set the pace.
+// (operand buffer, E and O accumulators in 128 tensor-memory columns, state); two loader
+// groups take alternate blocks, so the loads of two blocks are in flight while earlier
+// ones are multiplied. A loader that waits for its loads before storing them holds one
+// block in flight: with one group, the DRAM round trip set the pace.
 constexpr int kEoRows = 2;
 constexpr int kEoN = kEoRows * kZRot;  // 64
 constexpr int kEoS = 4;                // stages: operand buffers, accumulator pairs, state
