@@ -334,6 +334,12 @@ __device__ __forceinline__ void mma_f16_w(uint32_t tmem_d, uint32_t alo, uint32_
       :
       : "r"(tmem_d), "r"(alo), "r"(ahi), "r"(blo), "r"(bhi), "r"(idesc), "r"(accumulate));
 }
+// max of three (NaN operands are skipped, as fmaxf skips them)
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+  float d;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
 // the barrier's phase also waits for this thread's earlier cp.async copies (net zero on
 // the expected count: the thread arrives separately)
 __device__ __forceinline__ void mbar_track_cp_async(uint64_t* bar) {
@@ -580,10 +586,11 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
           // looked up only when the scaled maximum beats the running state
           float b1 = -INFINITY, b2 = -INFINITY;
           if (nb == kZRot) {
+            // three-input max: two rotations per instruction
 #pragma unroll
-            for (int b = 0; b < kZRot; ++b) {
-              b1 = fmaxf(b1, ev[b] + ov[b]);
-              b2 = fmaxf(b2, ev[b] - ov[b]);
+            for (int b = 0; b < kZRot; b += 2) {
+              b1 = fmax3(b1, ev[b] + ov[b], ev[b + 1] + ov[b + 1]);
+              b2 = fmax3(b2, ev[b] - ov[b], ev[b + 1] - ov[b + 1]);
             }
           } else {
 #pragma unroll
