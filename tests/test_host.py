@@ -93,3 +93,39 @@ def test_synthetic_generators():
                                atol=1e-6)
     assert syn.rotation_count_for_angle(7) == 27672
     assert syn.rotation_count_for_angle(30) == 360
+
+
+def test_subset_without_padding_is_the_slice():
+    """Without padding the subset is the slice itself (no copy before the upload); with
+    padding it is NumPy's reflect padding of the slice."""
+    rng = np.random.default_rng(5)
+    a = rng.normal(size=(9, 8, 7)).astype(np.float32)
+    sl = (slice(1, 8), slice(0, 8), slice(2, 6))
+    out = M.MatchingData._subset_array(a, sl, (0, 0, 0))
+    assert np.shares_memory(out, a) and np.array_equal(out, a[sl])
+    full = tuple(slice(0, n) for n in a.shape)
+    out = M.MatchingData._subset_array(a, full, (2, 0, 3))
+    assert np.array_equal(out, np.pad(a, ((1, 1), (0, 0), (2, 1)), mode="reflect"))
+
+
+def test_filter_spectrum_need():
+    """Only filters other than CTFs and wedges ask for the target spectrum."""
+    from pytme_b200 import filters as F
+
+    ctf = F.CTFReconstructed(defocus_x=20000.0)
+    wedge = F.WedgeReconstructed(angles=(60, 60), opening_axis=2, tilt_axis=0)
+    assert not F.needs_spectrum(ctf)
+    assert not F.needs_spectrum(F.Compose([ctf, wedge]))
+    assert F.needs_spectrum(F.LinearWhiteningFilter())
+    assert F.needs_spectrum(F.Compose([wedge, F.LinearWhiteningFilter()]))
+
+
+def test_download_host_tensor():
+    """download() of a host tensor is a plain copy to NumPy."""
+    import torch
+
+    from pytme_b200.analyzer import download
+
+    t = torch.arange(24, dtype=torch.float32).reshape(2, 3, 4)
+    got = download(t)
+    assert got.dtype == np.float32 and np.array_equal(got, t.numpy())
