@@ -506,3 +506,23 @@ def test_whitening_filters_in_scan(torch_cuda, score):
                  template_filter=np.asarray(tf, np.float32),
                  target_filter=np.asarray(gf, np.float32))
     assert np.abs(r[0] - ref["scores"]).max() <= TOL
+
+
+@pytest.mark.parametrize("score", ["FLCSphericalMask", "CC"])
+def test_default_passes_odd_z_length(torch_cuda, score):
+    """The default mixed-precision passes (persistent tensor-core x pass, register y pass,
+    even/odd tensor-core z pass) on an odd z length, with a partial last launch group,
+    against the oracle in FP32 and FP64."""
+    from pytme_b200 import synthetic as syn
+
+    rng = np.random.default_rng(41)
+    tmpl = syn.blob_template(12, rng, radius=3.5, sigma=1.2)
+    mask = syn.spherical_mask((12,) * 3, 6, center=(5.5,) * 3) if score != "CC" else None
+    target, _, _ = syn.make_tomogram((128, 64, 199), tmpl, 5, rng, scale=0.5)
+    rots = syn.random_rotation_matrices(40, rng)
+    r = _scan(score, target, tmpl, mask, rots, precision="mixed", batch=32)
+    ref = O.scan(target, tmpl, rots, score, template_mask=mask)
+    ref64 = O.scan(target, tmpl, rots, score, template_mask=mask, dtype=np.float64)
+    tol = mixed_tol(ref64["scores"])
+    assert np.abs(r[0] - ref["scores"]).max() <= tol
+    assert np.abs(r[0] - ref64["scores"]).max() <= tol
