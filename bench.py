@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--zpass", choices=("auto", "tensor", "fft"), default="auto",
                     help="z pass on the tensor cores, as CUDA-core FFTs, or the plan default")
+    ap.add_argument("--ypass", choices=("auto", "tensor", "fft"), default="auto",
+                    help="y pass on the tensor cores, as CUDA-core FFTs, or the plan default")
     ap.add_argument("--xpass", choices=("auto", "tensor", "fft"), default="auto",
                     help="x pass on the tensor cores, as CUDA-core FFTs, or the plan default "
                          "(tensor cores for mixed precision)")
@@ -61,7 +63,12 @@ def parse():
                     help="rotations per end-to-end call (0: the whole set)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="scoring-loop seconds of the cpu_baseline leg of this arm")
+    ap.add_argument("--ref-seconds", type=float, default=60.0,
+                    help="scoring-loop seconds of --impl reference (at least)")
+    ap.add_argument("--err-rotations", type=int, default=32,
+                    help="rotations of the measured error against the FP64 oracle (0: skip)")
     ap.add_argument("--small", action="store_true", help="128x128x64 / 24^3 quick check")
     ap.add_argument("--profile-case", default=None, metavar="N0,N1,N2",
                     help="run --groups launch groups of the fused scan on a target of this "
@@ -70,9 +77,27 @@ def parse():
     return ap.parse_args()
 
 
-def make_inputs(small=False):
-    from pytme_b200 import synthetic as syn
+def _synthetic():
+    """pytme_b200/synthetic.py loaded by file path: the input generators are plain NumPy,
+    and loading them this way keeps the reference arm from importing the package (and
+    its CUDA library)."""
+    import importlib.util
 
+    mod = sys.modules.get("_pytme_b200_synthetic")
+    if mod is None:
+        path = os.path.join(ROOT, "pytme_b200", "synthetic.py")
+        spec = importlib.util.spec_from_file_location("_pytme_b200_synthetic", path)
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["_pytme_b200_synthetic"] = mod
+        spec.loader.exec_module(mod)
+    return mod
+
+
+def make_inputs(small=False):
+    """The headline workload: a 512x512x200 tomogram (N(0,1) noise plus 300 rotated
+    copies at SNR 0.05), a 48^3 blob template, its spherical mask (r = 24) and the
+    7-degree rotation set."""
+    syn = _synthetic()
     rng = np.random.default_rng(2024)
     shape = (128, 128, 64) if small else SHAPE
     t = 24 if small else TSIZE
@@ -84,13 +109,50 @@ def make_inputs(small=False):
     return target, tmpl, mask, rots
 
 
-# DRAM bytes (read + write) of one launch of a pass of the benchmark configuration
-# (512x512x200, 48^3 template, mixed precision, 32 rotations per group) from ncu captures
-# of smaller launches of the same kernels, scaled to it: x and y passes from 512x512x48
-# targets (by columns, rotations and row pitch), the z pass from a 256x256x200 target (by
-# rows). Keyed by (pass, precision, rotations per group, variant of the pass).
-NCU_TRAFFIC = {("xpass", "mixed", 32, "fft"): 3.91e9, ("xpass", "mixed", 32, "tensor"): 4.18e9,
-               ("ypass", "mixed", 32, "fft"): 6.81e9, ("zpass", "mixed", 32, "tensor"): 4.23e9}
+CONFIG2_SHAPE = (256, 256, 128)
+CONFIG2_ANGLE = 15.0
+
+
+def make_config2_inputs():
+    """The filtered-FLC workload: a 256x256x128 tomogram (N(0,1) noise plus 40 rotated
+    copies at SNR 0.1), a 32^3 blob template, the mask (template > 0.1 max) dilated by 2
+    voxels, and the 15-degree rotation set. Filter parameters: ``config2_filters``."""
+    syn = _synthetic()
+    rng = np.random.default_rng(2025)
+    tmpl = syn.blob_template(32, rng, n_blobs=6, sigma=3.0, radius=10.0)
+    mask = syn.dilated_threshold_mask(tmpl, 0.1, 2)
+    target, _, _ = syn.make_tomogram(CONFIG2_SHAPE, tmpl, 40, rng, snr=0.1, mask=mask)
+    rots = syn.rotations_for_angle(CONFIG2_ANGLE)
+    return target, tmpl, mask, rots
+
+
+# CTF (300 kV, Cs 2.7 mm, amplitude contrast 0.07, defocus 3 um, 6.8 A pixels, phase
+# flipped) and a continuous missing wedge of +-60 degrees (opening axis 2, tilt axis 0):
+# the template gets CTF x wedge, the target the wedge.
+CONFIG2_CTF = dict(defocus_x=30000, amplitude_contrast=0.07, spherical_aberration=2.7e7,
+                   acceleration_voltage=300e3, sampling_rate=6.8, flip_phase=True)
+CONFIG2_WEDGE = dict(angles=(60, 60), opening_axis=2, tilt_axis=0,
+                     create_continuous_wedge=True)
+
+
+def profile_traffic(stage, precision, batch, variant):
+    """DRAM bytes (read + write) of one bench-size launch of ``stage`` from the committed
+    ncu summaries: each holds a line ``bench-traffic: stage=... precision=... batch=...
+    variant=... bytes=... <how the capture was scaled>``. Returns (bytes, source) or
+    (None, None) when no summary covers the kernel the bench ran."""
+    import glob
+    import re
+
+    pat = re.compile(r"^bench-traffic: stage=(\S+) precision=(\S+) batch=(\d+) variant=(\S+) "
+                     r"bytes=(\S+)\s*(.*)$")
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        with open(path) as f:
+            for line in f:
+                m = pat.match(line.strip())
+                if m and m.group(1) == stage and m.group(2) == precision and \
+                        int(m.group(3)) == batch and m.group(4) == variant:
+                    return float(m.group(5)), f"{os.path.relpath(path, ROOT)}: {m.group(6)}"
+    return None, None
 
 
 def measured_peaks():
@@ -152,46 +214,186 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def cpu_oracle_rate(target, tmpl, mask, rots, seconds, cores=None):
-    """The oracle scan on host cores (spawned workers over rotation chunks); returns
-    (rotations/s of the scoring loop, cores, sample description)."""
-    import multiprocessing as mp
+# ------------------------------------------------------------------ CPU arms
+REF_INSTALL = os.path.join(ROOT, "baseline", "_ref")
+REF_SHIM = os.path.join(ROOT, "tests", "golden", "refshim")
 
+
+def _host_workers(gb_per_worker: float, cap: int = 64) -> int:
     import psutil
 
-    cores = cores or os.cpu_count() or 1
-    # each process holds about 3 GB of full-size arrays during setup
-    by_mem = int(psutil.virtual_memory().available // (3 * 1024 ** 3))
-    cores = max(1, min(cores, 32, by_mem))
-    # per-rotation cost ~2.3 s on one core at this size; size the sample for `seconds`
-    per_worker = max(1, int(round(seconds / 2.5)))
-    n = cores * per_worker
-    sample = np.ascontiguousarray(rots[:n])
+    avail = psutil.virtual_memory().available / 1024 ** 3
+    return max(1, min(os.cpu_count() or 1, cap, int(avail // gb_per_worker)))
+
+
+class TmeScanLoop:
+    """The reference's own scan (tme/matching_exhaustive.py:144-295) on the host cores,
+    split into steps: ``scan``'s set-up once (MatchingData padding, the target filter,
+    ``flcSphericalMask_setup``, the SharedAnalyzerProxy instances), then every step runs
+    ``scan``'s joblib ``Parallel(n_jobs)`` over ``corr_scoring`` with one rotation chunk per
+    job, into the same analyzer state. NumpyFFTWBackend, FP32, interpolation order 1,
+    ``job_schedule=(1, n_jobs)``; pyFFTW is replaced by scipy.fft (tests/golden/refshim).
+    The package comes from baseline/_ref (oracle/build_ref.py --baseline)."""
+
+    kind = "reference"
+
+    def __init__(self, target, tmpl, mask, n_rotations, n_jobs):
+        for p, front in ((REF_SHIM, True), (REF_INSTALL, False)):
+            if p not in sys.path:
+                sys.path.insert(0, p) if front else sys.path.append(p)
+        from multiprocessing.managers import SharedMemoryManager
+
+        from joblib import Parallel
+        from tme.analyzer import MaxScoreOverRotations
+        from tme.analyzer.proxy import SharedAnalyzerProxy
+        from tme.backends import backend as be
+        from tme.matching_data import MatchingData
+        from tme.matching_exhaustive import (_setup_template_filter_apply_target_filter,
+                                             _wrap_backend)
+        from tme.matching_scores import MATCHING_EXHAUSTIVE_REGISTER
+
+        t0 = time.perf_counter()
+        be.change_backend("numpyfftw")
+        self.be = be
+        self.n_jobs = n_jobs
+        self.smh = SharedMemoryManager()
+        self.smh.start()
+        md = MatchingData(target.copy(), tmpl.copy())
+        md.template_mask = mask.copy()
+        md.rotations = np.eye(3, dtype=np.float32)[None]
+        md, offset = md.subset_by_slice(target_pad=md.target_padding(pad_target=False))
+        md.to_backend()
+        conv, fwd, inv, shift = md.fourier_padding(pad_target=False)
+        tf = _setup_template_filter_apply_target_filter(md, fwd, inv, pad_template_filter=False)
+        setup_fn, self.score_fn = MATCHING_EXHAUSTIVE_REGISTER["FLCSphericalMask"]
+        args = {"shape": fwd, "offset": offset, "fourier_shift": shift, "fast_shape": fwd,
+                "targetshape": md._output_shape, "templateshape": md.template.shape,
+                "convolution_shape": conv, "thread_safe": n_jobs > 1,
+                "convolution_mode": "same", "shm_handler": self.smh,
+                "only_unique_rotations": True, "n_rotations": n_rotations,
+                "aggregate_axis": md._batch_axis(md._batch_mask),
+                "inversion_mapping": n_jobs == 1, "score_threshold": 0}
+        self.setup = setup_fn(matching_data=md, template_filter=tf, fast_shape=fwd,
+                              fast_ft_shape=inv, shm_handler=self.smh)
+        self.setup["interpolation_order"] = 1
+        self.setup["template_filter"] = be.to_sharedarr(tf, self.smh)
+        self.callbacks = [SharedAnalyzerProxy(MaxScoreOverRotations, args,
+                                              shm_handler=self.smh if n_jobs > 1 else None)
+                          for _ in range(max(n_jobs // 8, 1))]
+        self.wrapped = _wrap_backend(self.score_fn)
+        self.parallel = Parallel(n_jobs=n_jobs)
+        self.parallel.__enter__()  # keep the workers for every step
+        self.setup_s = time.perf_counter() - t0
+
+    def step(self, chunks):
+        from joblib import delayed
+
+        nc = len(self.callbacks)
+        self.parallel(delayed(self.wrapped)(
+            backend_name=self.be._backend_name, backend_args=self.be._backend_args,
+            rotations=r, callback=self.callbacks[i % nc], **self.setup)
+            for i, r in enumerate(chunks))
+
+    def close(self):
+        self.parallel.__exit__(None, None, None)
+        self.smh.shutdown()
+
+
+_PORT_STATE = {}
+
+
+def _port_init(target, tmpl, mask):
     from oracle import tm_oracle as O
 
-    ctx = mp.get_context("spawn")
-    chunks = [(target, tmpl, mask, sample[i * per_worker:(i + 1) * per_worker])
-              for i in range(cores)]
-    with ctx.Pool(cores) as pool:
-        outs = pool.map(_cpu_chunk, chunks)
-    loop = max(o[1] for o in outs)
-    setup = max(o[0] for o in outs)
-    desc = (f"{n} rotations of the 7-degree set on the full 512x512x200 map, {cores} "
-            f"processes x {per_worker} rotations; scoring loop {loop:.1f} s, per-process "
-            f"setup {setup:.1f} s excluded")
-    return n / loop, cores, desc
+    t, t_rev, m_rev = O._prepare(target, tmpl, mask, False, None, np.float32)
+    _, fast, _, _ = O.fourier_padding(t.shape, t_rev.shape)
+    _PORT_STATE.update(O=O, t_rev=t_rev, m_rev=m_rev, fast=fast,
+                       setup=O._setup("FLCSphericalMask", t, t_rev, m_rev, fast, np.float32,
+                                      np.complex64),
+                       ms=np.zeros(fast, np.float32), am=np.full(fast, -1, np.int32))
 
 
-def _cpu_chunk(args):
-    target, tmpl, mask, rots = args
-    from oracle import tm_oracle as O
+def _port_step(rots):
+    st = _PORT_STATE
+    st["O"]._loop("FLCSphericalMask", st["setup"], st["t_rev"], st["m_rev"], rots, st["fast"],
+                  np.float32, np.complex64, None, 0, st["ms"], st["am"])
+    return 0
 
-    t0 = time.perf_counter()
-    O.scan(target, tmpl, rots[:0], "FLCSphericalMask", template_mask=mask)
-    t1 = time.perf_counter()
-    O.scan(target, tmpl, rots, "FLCSphericalMask", template_mask=mask)
-    t2 = time.perf_counter()
-    return t1 - t0, (t2 - t1) - (t1 - t0)
+
+class PortScanLoop:
+    """The oracle (the reference's loop restated in NumPy/SciPy) with the same step
+    structure as TmeScanLoop: spawned worker processes do the set-up once, then every
+    step scores one rotation chunk per worker. Used when the reference package is not
+    installed."""
+
+    kind = "port"
+
+    def __init__(self, target, tmpl, mask, n_rotations, n_jobs):
+        import multiprocessing as mp
+
+        t0 = time.perf_counter()
+        self.n_jobs = n_jobs
+        self.pool = mp.get_context("spawn").Pool(n_jobs, initializer=_port_init,
+                                                 initargs=(target, tmpl, mask))
+        self.pool.map(_port_step, [np.zeros((0, 3, 3), np.float32)] * n_jobs)
+        self.setup_s = time.perf_counter() - t0
+
+    def step(self, chunks):
+        self.pool.map(_port_step, chunks, chunksize=1)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def cpu_scan_loop(target, tmpl, mask, n_rotations, prefer_reference=True):
+    """The reference's loop on the host cores: tme itself when baseline/_ref holds it,
+    else the oracle port."""
+    if prefer_reference and os.path.isdir(os.path.join(REF_INSTALL, "tme")):
+        try:
+            return TmeScanLoop(target, tmpl, mask, n_rotations, _host_workers(2.0))
+        except ImportError:
+            pass
+    return PortScanLoop(target, tmpl, mask, n_rotations, _host_workers(3.0))
+
+
+def time_cpu_loop(loop, rots, steps, warmup, min_seconds):
+    """``warmup`` steps of one rotation per worker, then ``steps`` timed steps of r
+    rotations per worker, r sized from the warm-up so the timed loop lasts at least
+    ``min_seconds``. Returns (rotations/s, ms per step, rotations timed, r)."""
+    w = loop.n_jobs
+    pos = 0
+
+    def chunks(r):
+        nonlocal pos
+        out = []
+        for _ in range(w):
+            out.append(np.ascontiguousarray(rots[pos % len(rots):pos % len(rots) + r]))
+            pos += r
+        return out
+
+    t_warm = []
+    for _ in range(max(1, warmup)):
+        t0 = time.perf_counter()
+        loop.step(chunks(1))
+        t_warm.append(time.perf_counter() - t0)
+    per_rot = min(t_warm)
+    r = int(min(8, max(1, np.ceil(min_seconds / max(steps, 1) / per_rot))))
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        loop.step(chunks(r))
+        times.append(time.perf_counter() - t0)
+    n = steps * w * r
+    return n / sum(times), 1000.0 * float(np.mean(times)), n, r
+
+
+def cpu_sample_desc(loop, n, r, steps, total_s):
+    what = ("tme's own scan (NumpyFFTWBackend, scipy.fft for pyFFTW) via joblib"
+            if loop.kind == "reference" else "the oracle port in spawned processes")
+    return (f"{what}: {steps} steps x {loop.n_jobs} workers x {r} rotation(s) of the 7-degree "
+            f"set on the full 512x512x200 map ({n} rotations, scoring loop {total_s:.1f} s); "
+            f"set-up {loop.setup_s:.1f} s excluded")
 
 
 def run_reference(args):
@@ -199,29 +401,47 @@ def run_reference(args):
     if rank != 0:
         return 0
     target, tmpl, mask, rots = make_inputs(args.small)
-    steps = max(1, args.steps)
-    rates = []
-    cores = None
-    desc = ""
-    secs = max(5.0, min(args.cpu_seconds, 120.0 / (steps + args.warmup)))
-    for i in range(args.warmup + steps):
-        r, cores, desc = cpu_oracle_rate(target, tmpl, mask, rots[i * 7 % 1000:], secs)
-        if i >= args.warmup:
-            rates.append(r)
-    value = float(np.median(rates))
+    loop = cpu_scan_loop(target, tmpl, mask, len(rots))
+    try:
+        value, ms, n, r = time_cpu_loop(loop, rots, max(1, args.steps), args.warmup,
+                                        args.ref_seconds)
+    finally:
+        loop.close()
+    total = n / value
     line = {
         "metric": METRIC, "value": value, "unit": "rotations/s", "n_gpus": args.gpus,
-        "steps": steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+        "steps": max(1, args.steps), "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "impl": "reference",
-        "config": {"workload": WORKLOAD, "step": "one rotation per step (rate of the sample)"},
-        "cpu_baseline": {"value": value, "unit": "rotations/s", "cores": cores,
-                         "kind": "port", "sample": desc},
+        "data": "synthetic", "impl": "reference", "config": workload_config(args.small),
+        "cpu_baseline": {"value": value, "unit": "rotations/s", "cores": loop.n_jobs,
+                         "kind": loop.kind,
+                         "sample": cpu_sample_desc(loop, n, r, max(1, args.steps), total),
+                         "setup_s": loop.setup_s},
         "e2e": {"value": value, "unit": "rotations/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def workload_config(small=False):
+    """The workload both arms report (identical keys and values)."""
+    shape = (128, 128, 64) if small else SHAPE
+    t = 24 if small else TSIZE
+    return {"workload": WORKLOAD + (" [small]" if small else ""), "target_shape": list(shape),
+            "template_shape": [t] * 3, "rotations": 27672, "score": "FLCSphericalMask",
+            "analyzer": "MaxScoreOverRotations", "interpolation_order": 1,
+            "l2": "inputs larger than L2 (target spectrum 212 MB, state 420 MB)"}
+
+
+def fp64_error(target, tmpl, mask, rots, gpu_map, n_workers):
+    """Max |GPU map - FP64 oracle map| over the 'same'-mode map of a scan of ``rots``
+    (the oracle on the host cores, spawned workers)."""
+    from oracle import tm_oracle as O
+
+    ref = O.scan_parallel(target, tmpl, rots, "FLCSphericalMask", template_mask=mask,
+                          dtype=np.float64, n_workers=n_workers)
+    return float(np.abs(np.asarray(gpu_map, np.float64) - ref["scores"]).max())
 
 
 def run_ours(args):
@@ -256,6 +476,7 @@ def run_ours(args):
     plan = ScanPlan("FLCSphericalMask", fast, tmpl.shape, precision=args.precision,
                     batch=args.batch)
     plan.set_xpass(args.xpass)
+    plan.set_ypass(args.ypass)
     plan.set_zpass(args.zpass)
     plan.set_template(t_rev, m_rev)
     tpad = torch.zeros(fast, dtype=torch.float32, device=dev)
@@ -338,25 +559,23 @@ def run_ours(args):
         plain.close()
         del pm, pa
 
+        variant = {"xpass": plan.xpass, "zpass": plan.zpass, "ypass": plan.ypass}.get(dom, "fft")
+        traffic, traffic_src = (None, None) if args.small else profile_traffic(
+            dom, args.precision, args.batch, variant)
         result = {
             "metric": METRIC, "value": value, "unit": "rotations/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.precision == "fp32" else "f32 (f16 spectra, f64 denominator)",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD + ("" if not args.small else " [small]"),
-                       "step_rotations": R, "rotation_batch": args.batch,
-                       "precision": args.precision, "xpass": plan.xpass,
-                       "zpass": plan.zpass,
-                       "l2": "inputs larger than L2 (target spectrum 212 MB, state 420 MB)",
-                       "fast_shape": list(fast), "template": [TSIZE] * 3},
+            "config": workload_config(args.small),
+            "impl_config": {"step_rotations": R, "rotation_batch": args.batch,
+                            "precision": args.precision, "xpass": plan.xpass,
+                            "ypass": plan.ypass, "zpass": plan.zpass, "fast_shape": list(fast)},
             "voxel_rotations_per_s": value * float(np.prod(fast)),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": NCU_TRAFFIC.get((dom, args.precision, args.batch,
-                                                     {"xpass": plan.xpass, "zpass": plan.zpass}
-                                                     .get(dom, "fft")))
-                         if not args.small else None,
+                         "traffic": traffic, "traffic_source": traffic_src,
                          "alg_bytes_per_launch": alg,
                          "avg_launch_ms": avg_ms},
             "stages": stages,
@@ -370,7 +589,7 @@ def run_ours(args):
     if rank == 0 and not args.no_e2e:
         n_e2e = args.e2e_rotations or n_rot
         P.backend.change_backend("b200", precision=args.precision, rotation_batch=args.batch,
-                                 xpass=args.xpass, zpass=args.zpass)
+                                 xpass=args.xpass, ypass=args.ypass, zpass=args.zpass)
         setup, scoring = P.MATCHING_EXHAUSTIVE_REGISTER["FLCSphericalMask"]
         del plan, smax, sarg
         torch.cuda.empty_cache()
@@ -397,10 +616,38 @@ def run_ours(args):
                          "d2h_bytes_per_step": d2h, "rotations_per_step": n_e2e,
                          "seconds_per_step": dt,
                          "call": "pytme_b200.scan_subsets on host NumPy arrays"}
+    if rank == 0 and args.err_rotations > 0:
+        # measured score error of the GPU map against the FP64 oracle on a rotation subset
+        # spread over the set (the public API on the GPU, the oracle on the host cores)
+        stride = max(1, n_rot // args.err_rotations)
+        sub = np.ascontiguousarray(rots[::stride][:args.err_rotations])
+        P.backend.change_backend("b200", precision=args.precision, rotation_batch=args.batch,
+                                 xpass=args.xpass, ypass=args.ypass, zpass=args.zpass)
+        setup, scoring = P.MATCHING_EXHAUSTIVE_REGISTER["FLCSphericalMask"]
+        md = P.MatchingData(target, tmpl)
+        md.template_mask = mask
+        md.rotations = sub
+        gmap = P.scan_subsets(md, matching_score=scoring, matching_setup=setup,
+                              callback_class=P.MaxScoreOverRotations,
+                              callback_class_args={"score_threshold": 0},
+                              interpolation_order=1)[0]
+        torch.cuda.empty_cache()
+        t0 = time.perf_counter()
+        err = fp64_error(target, tmpl, mask, sub, gmap, _host_workers(6.0, cap=32))
+        result["error_vs_fp64"] = {
+            "max_abs": err, "bound": 1e-4, "rotations": int(sub.shape[0]),
+            "what": "max |score - FP64 oracle| over the 'same'-mode map, rotations spread "
+                    "over the 7-degree set", "oracle_s": time.perf_counter() - t0}
     if rank == 0 and not args.no_cpu:
-        r, cores, desc = cpu_oracle_rate(target, tmpl, mask, rots, args.cpu_seconds)
-        result["cpu_baseline"] = {"value": r, "unit": "rotations/s", "cores": cores,
-                                  "kind": "port", "sample": desc}
+        loop = cpu_scan_loop(target, tmpl, mask, n_rot)
+        try:
+            rate, cms, n, r = time_cpu_loop(loop, rots, 3, 1, args.cpu_seconds)
+        finally:
+            loop.close()
+        result["cpu_baseline"] = {"value": rate, "unit": "rotations/s", "cores": loop.n_jobs,
+                                  "kind": loop.kind,
+                                  "sample": cpu_sample_desc(loop, n, r, 3, n / rate),
+                                  "setup_s": loop.setup_s}
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:
@@ -428,6 +675,7 @@ def run_profile_case(args):
     plan = ScanPlan("FLCSphericalMask", shape, (t,) * 3, precision=args.precision,
                     batch=args.batch)
     plan.set_xpass(args.xpass)
+    plan.set_ypass(args.ypass)
     plan.set_zpass(args.zpass)
     plan.set_template(tmpl[::-1, ::-1, ::-1].copy(), mask[::-1, ::-1, ::-1].copy())
     plan.set_target(torch.as_tensor(target, device="cuda"))

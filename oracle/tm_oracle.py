@@ -36,6 +36,7 @@ __all__ = [
     "apply_target_filter",
     "scan",
     "scan_parallel",
+    "raw_index",
     "result_map",
     "max_filter_coordinates",
     "find_candidate_indices",
@@ -220,10 +221,12 @@ def _setup(score, target, template_rev, mask_rev, fast, dtype, cdtype):
 
 
 def _loop(score, setup, template_rev, mask_rev, rotations, fast, dtype, cdtype,
-          template_filter, first_index, max_scores, argmax, order=1):
+          template_filter, first_index, max_scores, argmax, order=1, on_scores=None):
     """Per-rotation loops ``corr_scoring`` (tme/matching_scores.py:600-624) and
     ``flc_scoring`` (tme/matching_scores.py:727-757) with ``MaxScoreOverRotations``
-    state updates (tme/analyzer/aggregation.py:142-189)."""
+    state updates (tme/analyzer/aggregation.py:142-189). ``on_scores(i, scores)``, when
+    given, sees every rotation's full score map before the update (the callback
+    position of the reference loops)."""
     eps = np.finfo(dtype).eps
     tshape = template_rev.shape
     center = np.divide(np.asarray(tshape) - 1, 2)
@@ -247,6 +250,8 @@ def _loop(score, setup, template_rev, mask_rev, rotations, fast, dtype, cdtype,
             cc = sfft.irfftn(setup["ft_target"] * ft_temp, s=fast).astype(dtype, copy=False)
             cc = norm_scores(cc, cc_m2.astype(dtype, copy=False), cc_m.astype(dtype, copy=False),
                              n_obs, eps, cc)
+            if on_scores is not None:
+                on_scores(i, cc)
             _max_update(cc, max_scores, argmax, first_index + i)
         return
     template_rot = np.zeros(tshape, dtype=dtype)
@@ -266,6 +271,8 @@ def _loop(score, setup, template_rev, mask_rev, rotations, fast, dtype, cdtype,
         arr = sfft.irfftn(ft_temp, s=fast).astype(dtype, copy=False)
         if "inv_denominator" in setup:
             arr = np.multiply(arr, setup["inv_denominator"], out=arr)
+        if on_scores is not None:
+            on_scores(i, arr)
         _max_update(arr, max_scores, argmax, first_index + i)
         arr = np.ascontiguousarray(arr)
 
@@ -318,50 +325,80 @@ def scan(target: np.ndarray, template: np.ndarray, rotations: np.ndarray,
 
 
 def _scan_chunk(args):
-    (score, tgt, t_rev, m_rev, rotations, fast, dtype, tf, first, thr) = args
+    (score, tgt, t_rev, m_rev, rotations, fast, dtype, tf, first, thr, order, probe) = args
     cdtype = np.complex128 if dtype == np.float64 else np.complex64
     setup = _setup(score, tgt, t_rev, m_rev, fast, dtype, cdtype)
     ms = np.full(fast, thr, dtype=dtype)
     am = np.full(fast, -1, dtype=np.int32)
-    _loop(score, setup, t_rev, m_rev, rotations, fast, dtype, cdtype, tf, first, ms, am)
-    return ms, am
+    vals = None
+    hook = None
+    if probe is not None:
+        vals = np.zeros((rotations.shape[0], probe.size), dtype=np.float64)
+
+        def hook(i, arr):
+            vals[i] = np.asarray(arr).reshape(-1)[probe]
+    _loop(score, setup, t_rev, m_rev, rotations, fast, dtype, cdtype, tf, first, ms, am,
+          order=order, on_scores=hook)
+    return ms, am, vals
+
+
+def raw_index(result_coords, fast, shift, conv, target_shape, template_shape, mode="same"):
+    """Flat indices into the raw (fast-shaped) state of the voxels at ``result_coords``
+    ((m, 3) coordinates of the map ``result_map`` returns): ``result_map`` applied to the
+    index volume."""
+    idx = np.arange(int(np.prod(fast)), dtype=np.int64).reshape(fast)
+    ridx, _ = result_map(idx, idx, shift, conv, target_shape, template_shape, mode)
+    c = np.asarray(result_coords, dtype=np.int64).reshape(-1, len(fast))
+    return np.ascontiguousarray(ridx[tuple(c.T)])
 
 
 def scan_parallel(target, template, rotations, score="FLCSphericalMask", template_mask=None,
-                  template_filter=None, dtype=np.float32, n_workers: int = 1,
-                  score_threshold: float = 0.0):
+                  template_filter=None, target_filter=None, dtype=np.float32,
+                  n_workers: int = 1, score_threshold: float = 0.0,
+                  interpolation_order: int = 1, probe=None):
     """``scan`` with the rotation set split into contiguous chunks over ``n_workers``
     spawned processes (the reference's inner joblib parallelism,
     tme/matching_exhaustive.py:276-285 and ``_split_rotations_on_jobs``
     tme/matching_data.py:822-844); chunk states are merged in rotation order, which
-    keeps the first rotation on ties."""
+    keeps the first rotation on ties. ``probe`` ((m, 3) coordinates in the returned
+    ``same``-mode map) adds ``"probe"``: every rotation's score at those voxels,
+    (rotations, m) float64."""
     import multiprocessing as mp
 
     rotations = np.asarray(rotations, dtype=np.float32)
     tgt, t_rev, m_rev = _prepare(target, template, template_mask, False, None, dtype)
     conv, fast, fast_ft, shift = fourier_padding(tgt.shape, t_rev.shape, False)
+    if target_filter is not None:
+        tgt = apply_target_filter(tgt, fast, target_filter).astype(dtype)
     tf = None if template_filter is None else np.asarray(template_filter, dtype=dtype)
+    pidx = None
+    if probe is not None:
+        pidx = raw_index(probe, fast, shift, conv, tgt.shape, t_rev.shape)
     n = rotations.shape[0]
-    per = n // n_workers if n_workers > 0 else n
+    n_workers = max(1, min(int(n_workers), n))
+    per = n // n_workers
     chunks = []
     for j in range(n_workers):
         lo = j * per
         hi = n if j == n_workers - 1 else lo + per
         chunks.append((score, tgt, t_rev, m_rev, rotations[lo:hi], fast, dtype, tf, lo,
-                       score_threshold))
+                       score_threshold, interpolation_order, pidx))
     if n_workers == 1:
         outs = [_scan_chunk(chunks[0])]
     else:
         ctx = mp.get_context("spawn")
         with ctx.Pool(n_workers) as pool:
             outs = pool.map(_scan_chunk, chunks)
-    ms, am = outs[0]
-    for ms2, am2 in outs[1:]:
+    ms, am, _ = outs[0]
+    for ms2, am2, _ in outs[1:]:
         upd = ms2 > ms
         ms[upd] = ms2[upd]
         am[upd] = am2[upd]
     scores, rot = result_map(ms, am, shift, conv, tgt.shape, t_rev.shape, "same")
-    return {"scores": scores, "rotations": rot}
+    out = {"scores": scores, "rotations": rot}
+    if probe is not None:
+        out["probe"] = np.concatenate([o[2] for o in outs], axis=0)
+    return out
 
 
 def _center_slice(current_shape, new_shape):
@@ -401,23 +438,29 @@ def find_candidate_indices(coordinates: np.ndarray, min_distance) -> np.ndarray:
     distance in the coordinates' type; for integer coordinates (the int64 overload the
     peak callers reach, bindings.cpp:251-256) the squared distance and its square root
     are truncated to integers, so a point is rejected iff
-    ``floor(sqrt(d2)) <= min_distance``."""
+    ``floor(sqrt(d2)) <= min_distance``. Each point is tested against the kept list at
+    once (integer squared distances; the floor of the float64 square root equals the
+    integer square root for the squared distances of coordinates below 2**24)."""
     coords = np.asarray(coordinates)
     n = coords.shape[0]
-    kept = [0]
+    if n == 0:
+        return np.zeros(0, dtype=np.int64)
     integer = np.issubdtype(coords.dtype, np.integer)
     c = coords.astype(np.int64 if integer else np.float64)
+    if integer and np.abs(c).max(initial=0) >= 2 ** 24:
+        raise ValueError("integer coordinates beyond 2**24 are outside the oracle's range")
+    kept_c = np.empty_like(c)
+    kept = [0]
+    kept_c[0] = c[0]
+    k = 1
     for i in range(1, n):
-        ok = True
-        for j in kept:
-            d = c[i] - c[j]
-            d2 = int(np.dot(d, d)) if integer else float(np.dot(d, d))
-            dist = math.isqrt(d2) if integer else math.sqrt(d2)
-            if dist <= min_distance:
-                ok = False
-                break
-        if ok:
+        d = kept_c[:k] - c[i]
+        d2 = np.einsum("ij,ij->i", d, d)
+        dist = np.floor(np.sqrt(d2.astype(np.float64))) if integer else np.sqrt(d2)
+        if not np.any(dist <= min_distance):
             kept.append(i)
+            kept_c[k] = c[i]
+            k += 1
     return np.asarray(kept, dtype=np.int64)
 
 

@@ -100,22 +100,20 @@ def rigid_transform_matrices(rotations: np.ndarray, center) -> np.ndarray:
 
 
 def split_shape(shape, splits: Dict, equal_shape: bool = True):
-    """tme/matching_utils.py:573-618."""
-    ndim = len(shape)
-    splits = {k: max(splits.get(k, 1), 1) for k in range(ndim)}
-    ret_shape = np.divide(shape, tuple(splits[i] for i in range(ndim)))
-    if equal_shape:
-        ret_shape = np.ceil(ret_shape).astype(int)
-    ret_shape = ret_shape.astype(int)
-    slice_list = [
-        tuple(
-            (slice((n * length), (n + 1) * length)) if n < splits.get(axis, 1) - 1
-            else ((slice(shape[axis] - length, shape[axis])) if equal_shape
-                  else (slice((n * length), shape[axis])))
-            for n in range(splits.get(axis, 1)))
-        for length, axis in zip(ret_shape, splits.keys())
-    ]
-    return tuple(product(*slice_list))
+    """The split slices of tme/matching_utils.py:573-618. Axis ``a`` is cut into
+    ``p = max(splits.get(a, 1), 1)`` parts of length ``ceil(n/p)`` (``equal_shape``; the
+    last part is moved back to end at the edge, overlapping its neighbour) or
+    ``floor(n/p)`` (the last part runs to the edge); the result lists every combination
+    of the axes' parts with the last axis varying fastest."""
+    per_axis = []
+    for axis, n in enumerate(int(x) for x in shape):
+        parts = max(int(splits.get(axis, 1)), 1)
+        step = -(-n // parts) if equal_shape else n // parts
+        starts = [i * step for i in range(parts - 1)]
+        cuts = [slice(a, a + step) for a in starts]
+        cuts.append(slice(n - step, n) if equal_shape else slice((parts - 1) * step, n))
+        per_axis.append(tuple(cuts))
+    return tuple(product(*per_axis))
 
 
 def _center_slice(current_shape, new_shape):

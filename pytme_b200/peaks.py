@@ -17,7 +17,7 @@ import torch
 from . import _native as N
 
 __all__ = ["max_filter_coordinates", "find_candidate_indices", "filter_points_indices",
-           "topk_indices", "topk_indices_device"]
+           "filter_bucket", "topk_indices", "topk_indices_device"]
 
 
 def _dev():
@@ -61,18 +61,70 @@ def find_candidate_indices(coordinates, min_distance: int) -> np.ndarray:
     return out[:k].cpu().numpy().astype(np.int64)
 
 
-def filter_points_indices(coordinates, min_distance: float, scores=None) -> np.ndarray:
-    """tme/analyzer/peaks.py:68-106 (unbatched, below the bucketing cutoff)."""
+def filter_bucket(coordinates, min_distance: float, scores=None) -> np.ndarray:
+    """One point per grid cell of edge ``min_distance`` (the reference's rule for large
+    point sets, tme/analyzer/peaks.py:39-64): cells from the integer part of
+    (coordinate - minimum) / min_distance, flattened with per-axis strides of
+    (max cell + 1)^axis. With scores, each cell keeps its highest-scoring point (an
+    argsort of cell rank minus the score scaled into [0, 1)), listed by cell; without,
+    the first point of each cell in input order."""
+    c = np.asarray(coordinates)
+    c = c - c.min(axis=0)
+    cells = (c / min_distance).astype(int)
+    strides = np.power(cells.max(axis=0) + 1, np.arange(cells.shape[1]))
+    flat = (cells * strides).sum(axis=1)
+    if scores is None:
+        _, first = np.unique(flat, return_index=True)
+        return first[np.argsort(first)]
+    _, rank = np.unique(flat, return_inverse=True)
+    sc = np.asarray(scores)
+    sc = sc - sc.min()
+    sc = sc / (sc.max() + 0.1)
+    order = np.argsort(rank - sc)
+    cell_of = rank[order]
+    first_of_cell = np.concatenate(([True], cell_of[1:] != cell_of[:-1]))
+    return order[first_of_cell]
+
+
+def _filter_lower_triangle(coordinates, min_distance: float) -> np.ndarray:
+    """The reference's rule at exactly its point cutoff (tme/analyzer/peaks.py:101-106):
+    point i is kept when every earlier point lies farther than ``min_distance`` (Euclidean,
+    float64), in input order; evaluated on the device in blocks of rows."""
+    c = torch.as_tensor(np.asarray(coordinates), device=_dev(), dtype=torch.float64)
+    n = c.shape[0]
+    keep = np.zeros(n, dtype=bool)
+    block = 2048
+    for i0 in range(0, n, block):
+        i1 = min(n, i0 + block)
+        d = torch.cdist(c[i0:i1], c[:i1], compute_mode="donot_use_mm_for_euclid_dist")
+        earlier = (torch.arange(i1, device=c.device)[None, :] <
+                   torch.arange(i0, i1, device=c.device)[:, None])
+        far = ((d > min_distance) | ~earlier).all(dim=1)
+        keep[i0:i1] = far.cpu().numpy()
+    return np.nonzero(keep)[0]
+
+
+def filter_points_indices(coordinates, min_distance: float, scores=None,
+                          bucket_cutoff: int = 100000) -> np.ndarray:
+    """tme/analyzer/peaks.py:68-106 (unbatched). Below ``bucket_cutoff`` points: the
+    greedy filter on the device in descending score order; above it: ``filter_bucket``;
+    at exactly the cutoff the reference falls through to its lower-triangle distance
+    rule in input order, reproduced by ``_filter_lower_triangle``."""
     coordinates = np.asarray(coordinates)
     if min_distance <= 0:
         return np.arange(coordinates.shape[0])
-    if coordinates.shape[0] == 0:
+    n = coordinates.shape[0]
+    if n == 0:
         return np.zeros(0, dtype=np.int64)
+    if n > bucket_cutoff:
+        return filter_bucket(coordinates, min_distance, scores)
+    if n == bucket_cutoff:
+        return _filter_lower_triangle(coordinates, min_distance)
     if scores is not None:
         order = np.argsort(-np.asarray(scores))
         kept = find_candidate_indices(coordinates[order], int(min_distance))
         return order[kept]
-    return find_candidate_indices(coordinates, int(min_distance))
+    return _filter_lower_triangle(coordinates, min_distance)
 
 
 def topk_indices(arr, k: int) -> np.ndarray:

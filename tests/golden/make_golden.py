@@ -23,6 +23,8 @@ mrcfile; scikit-image stubs). Its own public API then produces:
 * ``filters.npz``    CTF, continuous wedge and Compose arrays for ``FILTER_CASES``.
 * ``cubic.npz``      FLCSphericalMask, FLC and CC scans with ``interpolation_order=3``
                      (FP32 and FP64), and one order-3 rigid transform of data and mask.
+* ``splits.npz``     ``split_shape`` slices and the bucket filter of peak calling
+                     (``--only splits``).
 
 Inputs are stored next to the outputs so the tests never need the reference.
 """
@@ -147,6 +149,36 @@ def _whitening():
     np.savez_compressed(os.path.join(HERE, "whitening.npz"), **out)
 
 
+SPLIT_CASES = (((80, 80, 80), {0: 2}), ((81, 64, 33), {0: 3, 2: 2}), ((7, 5, 3), {0: 4, 1: 5}),
+               ((3, 9, 10), {1: 4, 2: 3}), ((100,), {0: 7}), ((64, 64), {}),
+               ((10, 11, 12), {0: 1, 1: 2, 2: 5}))
+
+
+def _splits():
+    """``split_shape`` slices for SPLIT_CASES (both equal_shape settings) and the
+    reference's bucket filter (``_filter_bucket``, used by filter_points_indices above its
+    point cutoff) on random points with and without scores."""
+    from tme.analyzer.peaks import _filter_bucket
+    from tme.matching_utils import split_shape
+
+    out = {}
+    for i, (shape, splits) in enumerate(SPLIT_CASES):
+        for eq in (True, False):
+            sl = split_shape(shape, dict(splits), equal_shape=eq)
+            out[f"case{i}_{int(eq)}"] = np.array(
+                [[(x.start, x.stop) for x in combo] for combo in sl], dtype=np.int64)
+    rng = np.random.default_rng(12)
+    for j, (n, md) in enumerate(((5000, 6), (20000, 10), (3000, 1))):
+        c = rng.integers(0, 200, size=(n, 3)).astype(np.int64)
+        sc = rng.normal(size=n).astype(np.float32)
+        out[f"bucket{j}_coords"] = c
+        out[f"bucket{j}_scores"] = sc
+        out[f"bucket{j}_md"] = np.int64(md)
+        out[f"bucket{j}_idx"] = np.asarray(_filter_bucket(c, md, sc))
+        out[f"bucket{j}_idx_noscore"] = np.asarray(_filter_bucket(c, md, None))
+    np.savez_compressed(os.path.join(HERE, "splits.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("PYTME_REFERENCE",
@@ -176,6 +208,10 @@ def main():
         return
     if args.only == "filters":
         _filters()
+        print("golden vectors written to", HERE)
+        return
+    if args.only == "splits":
+        _splits()
         print("golden vectors written to", HERE)
         return
 

@@ -129,3 +129,32 @@ def test_download_host_tensor():
     t = torch.arange(24, dtype=torch.float32).reshape(2, 3, 4)
     got = download(t)
     assert got.dtype == np.float32 and np.array_equal(got, t.numpy())
+
+
+def test_split_shape_matches_reference(golden):
+    """split_shape against the reference's slices (tests/golden/splits.npz)."""
+    from pytme_b200.matching import split_shape
+    from tests.golden.make_golden import SPLIT_CASES
+
+    g = golden("splits.npz")
+    for i, (shape, splits) in enumerate(SPLIT_CASES):
+        for eq in (True, False):
+            got = np.array([[(x.start, x.stop) for x in combo]
+                            for combo in split_shape(shape, dict(splits), equal_shape=eq)],
+                           dtype=np.int64)
+            assert np.array_equal(got, g[f"case{i}_{int(eq)}"]), (shape, splits, eq)
+
+
+def test_filter_bucket_matches_reference(golden):
+    """The bucket rule peak calling uses above 1e5 candidate points, against the
+    reference's _filter_bucket on random points with and without scores."""
+    from pytme_b200.peaks import filter_bucket, filter_points_indices
+
+    g = golden("splits.npz")
+    for j in range(3):
+        c, sc, md = g[f"bucket{j}_coords"], g[f"bucket{j}_scores"], int(g[f"bucket{j}_md"])
+        assert np.array_equal(filter_bucket(c, md, sc), g[f"bucket{j}_idx"])
+        assert np.array_equal(filter_bucket(c, md, None), g[f"bucket{j}_idx_noscore"])
+        # the dispatch takes the bucket path above the cutoff
+        assert np.array_equal(filter_points_indices(c, md, scores=sc, bucket_cutoff=len(c) - 1),
+                              g[f"bucket{j}_idx"])
