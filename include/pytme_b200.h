@@ -49,6 +49,14 @@ int tm_version(void);
  * len). Returns the full message length. */
 int tm_last_error(char* buf, size_t len);
 
+/* Caps the device memory one scan plan may allocate (bytes; 0 removes the cap). A plan
+ * that would need more fails in tm_scan_create with TM_E_OOM, as a failed allocation
+ * does, before touching the device: for hosts that run within a fixed memory budget,
+ * and to exercise the out-of-memory path. The reference has no such setting; its
+ * allocation failures surface through device_memory_handler
+ * (tme/matching_exhaustive.py:122-141), which this error path mirrors. */
+int tm_set_device_memory_limit(int64_t bytes);
+
 /* Order-1 rigid transform of `n_mat` copies of a (d0,d1,d2) volume.
  * Replaces NumpyFFTWBackend.rigid_transform / _rigid_transform with order=1
  * (tme/backends/npfftw_backend.py:357-449), i.e. scipy.ndimage.affine_transform
@@ -181,6 +189,21 @@ int tm_scan_xpass_mode(const tm_scan* plan);
  * restores the default. TM_E_UNSUPPORTED when mode 0 is not available. */
 int tm_scan_set_zpass(tm_scan* plan, int mode);
 int tm_scan_zpass_mode(const tm_scan* plan);
+/* y pass of the fused CC / FLCSphericalMask scan (the inverse transform along axis 1 of
+ * corr_scoring's irfftn, tme/matching_scores.py:618-620): mode 0 runs it on the tensor
+ * cores as two FP16 DFT GEMM stages (radix 16, then radix n1/16, twiddles between them;
+ * mixed-precision plans with n1 of 256 or 512), mode 1 as CUDA-core FFTs, mode 2 restores
+ * the default. TM_E_UNSUPPORTED when mode 0 is not available. */
+int tm_scan_set_ypass(tm_scan* plan, int mode);
+int tm_scan_ypass_mode(const tm_scan* plan);
+/* Bound of every data wait inside the plan's tensor-core kernels, in mbarrier polls
+ * (0 restores the default of 4,194,304, on the order of a second). A wait that runs out
+ * makes its kernel stop early; the next tm_scan_check then returns TM_E_TIMEOUT and the
+ * results of that run are invalid. The waits that keep tensor memory and shared memory
+ * alive until in-flight MMAs finish always use the default. No counterpart in the
+ * reference, which has no device waits; it plays the role of the reference's error
+ * surfacing in device_memory_handler (tme/matching_exhaustive.py:122-141). */
+int tm_scan_set_wait_budget(tm_scan* plan, uint32_t iters);
 /* Synchronise `stream`; TM_E_TIMEOUT if a bounded wait inside a tensor-core kernel of
  * this plan gave up since the last check (the results of that run are invalid). */
 int tm_scan_check(tm_scan* plan, void* stream);
@@ -243,8 +266,9 @@ int tm_find_candidate_indices(const int64_t* coords, int n, int64_t min_distance
  * GPU that loads the library holds until the process exits. It allocates nothing:
  * no cudaMalloc, cudaFree or allocating library call. n above
  * TM_NOALLOC_MAX_POINTS returns TM_E_INVALID. The first call on each device looks
- * up the scratch address (cudaGetSymbolAddress) with that device current; make
- * that first call before any stream capture. All calls share the one scratch
+ * up the scratch address (cudaGetSymbolAddress) with that device current, and again
+ * after the device's context was replaced (cudaDeviceReset); make that first call
+ * before any stream capture. All calls share the one scratch
  * array, so calls that overlap on the GPU (different streams, or different host
  * threads on one device) race and must be serialised by the caller. Results are
  * identical to tm_find_candidate_indices. */
@@ -338,17 +362,6 @@ int tm_refine_backward(const tm_refine_desc* d, const float* tmpl_filtered,
                        const float* grad_rotated, const double* sums, const float* grad_scores,
                        const float* drot, double* grad_rot, double* grad_shift,
                        double* grad_angles, float* grad_tmpl, void* stream);
-
-/* Diagnostic: the tensor-core x pass alone (complex64 G [nb][t0][n1][h2] and C
- * [n0][n1][h2] in, H [nb][n0][n1][h2] complex64 or half2 out):
- * H[b][x'] = sum_{x<t0} scale * C[(x'-x) mod n0] * G[b][x] per column. Synchronises. */
-int tm_xcorr_tc_test(const void* G, const void* C, int nb, int t0, int n0, int n1, int h2,
-                     float scale, void* H, int half, void* stream);
-
-/* Diagnostic: `lines` complex FFTs of length n (dir -1 forward, +1 unnormalised
- * inverse) with the shared-memory line-FFT routine of the fused scan.
- * Synchronises. */
-int tm_line_fft_test(const void* x, void* y, int n, int lines, int dir, void* stream);
 
 #ifdef __cplusplus
 }

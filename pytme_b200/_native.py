@@ -4,7 +4,8 @@ The library is required: importing this module raises if it is missing, and no
 operation of the package falls back to a CPU implementation. Status codes are
 mapped to the exception types the reference raises for the same conditions
 (``ValueError`` for bad arguments, ``MemoryError`` for allocation failures,
-``NotImplementedError`` for unsupported requests, ``RuntimeError`` otherwise).
+``NotImplementedError`` for unsupported requests, ``TimeoutError`` for a device wait
+that gave up, ``RuntimeError`` otherwise).
 """
 from __future__ import annotations
 
@@ -32,7 +33,7 @@ TM_PREC_MIXED = 1
 STAGES = ("prepare", "template", "xpass", "ypass", "zpass")
 
 EXPORTED = (
-    "tm_version", "tm_last_error", "tm_rigid_transform", "tm_normalize_template_workspace",
+    "tm_version", "tm_last_error", "tm_set_device_memory_limit", "tm_rigid_transform", "tm_normalize_template_workspace",
     "tm_normalize_template", "tm_norm_scores", "tm_max_score_over_rotations",
     "tm_fft_plan_create", "tm_fft_plan_destroy", "tm_fft_r2c", "tm_fft_c2r",
     "tm_scan_create", "tm_scan_destroy", "tm_scan_device_bytes", "tm_scan_set_template",
@@ -40,14 +41,15 @@ EXPORTED = (
     "tm_scan_get_timing",
     "tm_scan_stage_bytes", "tm_max_filter_peaks",
     "tm_find_candidate_indices_workspace", "tm_find_candidate_indices",
-    "tm_find_candidate_indices_noalloc", "tm_line_fft_test", "tm_fft_filter",
+    "tm_find_candidate_indices_noalloc", "tm_fft_filter",
     "tm_euler_zyz", "tm_refine_rotate", "tm_refine_forward", "tm_refine_grad_filtered",
     "tm_refine_backward", "tm_spline_prefilter", "tm_rigid_transform_cubic",
     "tm_scan_set_interpolation", "tm_build_filter", "tm_whitening_bins", "tm_whitening_filter",
-    "tm_xcorr_tc_test",
     "tm_scan_set_xpass", "tm_scan_check", "tm_scan_xpass_mode", "tm_scan_set_zpass",
-    "tm_scan_zpass_mode",
+    "tm_scan_zpass_mode", "tm_scan_set_ypass", "tm_scan_ypass_mode", "tm_scan_set_wait_budget",
 )
+# exported for the test suite only (pytme_b200/csrc/diagnostics.h), not public interface
+DIAGNOSTICS = ("tm_line_fft_test", "tm_xcorr_tc_test")
 
 
 class ScanDesc(Structure):
@@ -101,6 +103,7 @@ def _load():
     sig = {
         "tm_version": (c_int, []),
         "tm_last_error": (c_int, [c_char_p, c_size_t]),
+        "tm_set_device_memory_limit": (c_int, [c_int64]),
         "tm_rigid_transform": (c_int, [f32p, f32p, c_int, c_int, c_int, f32p, c_int, f32p, f32p,
                                        c_int, c_int, c_int, vp]),
         "tm_normalize_template_workspace": (c_int64, [c_int]),
@@ -136,6 +139,9 @@ def _load():
         "tm_scan_xpass_mode": (c_int, [vp]),
         "tm_scan_set_zpass": (c_int, [vp, c_int]),
         "tm_scan_zpass_mode": (c_int, [vp]),
+        "tm_scan_set_ypass": (c_int, [vp, c_int]),
+        "tm_scan_ypass_mode": (c_int, [vp]),
+        "tm_scan_set_wait_budget": (c_int, [vp, ctypes.c_uint32]),
         "tm_build_filter": (c_int, [vp, c_int, POINTER(c_int), c_int, f32p, vp]),
         "tm_whitening_bins": (c_int, [POINTER(c_int), c_int]),
         "tm_whitening_filter": (c_int, [vp, POINTER(c_int), c_int, POINTER(c_int), c_int, vp,
@@ -176,13 +182,19 @@ def check(status: int, what: str = "") -> None:
         raise MemoryError(msg)
     if status == TM_E_UNSUPPORTED:
         raise NotImplementedError(msg)
+    if status == TM_E_TIMEOUT:
+        raise TimeoutError(msg)
     raise NativeError(f"{msg} (status {status})")
 
 
 def ptr(t) -> int:
-    """Device address of a torch tensor (0 for None)."""
+    """Device address of a CUDA torch tensor (None for None). A host tensor raises
+    ValueError: every kernel argument of the library is device memory."""
     if t is None:
         return None
+    if not getattr(t, "is_cuda", False):
+        raise ValueError("pytme_b200 kernels take CUDA tensors; got "
+                         f"{type(t).__name__} on {getattr(t, 'device', 'host')}")
     return t.data_ptr()
 
 

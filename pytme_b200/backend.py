@@ -26,7 +26,7 @@ from . import _native as N
 __all__ = ["B200Backend", "backend", "current_options", "fft_plan", "FFTPlan"]
 
 _DEFAULTS = {"precision": "fp32", "rotation_batch": 32, "plain": False, "xpass": "auto",
-             "zpass": "auto"}
+             "ypass": "auto", "zpass": "auto"}
 _OPTIONS = dict(_DEFAULTS)
 
 
@@ -43,7 +43,7 @@ def _set_options(**kwargs):
             _OPTIONS[k] = v
     if _OPTIONS["precision"] not in ("fp32", "mixed"):
         raise ValueError("precision must be 'fp32' or 'mixed'")
-    for key in ("xpass", "zpass"):
+    for key in ("xpass", "ypass", "zpass"):
         if _OPTIONS[key] not in ("auto", "fft", "tensor"):
             raise ValueError(f"{key} must be 'auto', 'fft' or 'tensor'")
     _OPTIONS["rotation_batch"] = int(_OPTIONS["rotation_batch"])
@@ -134,6 +134,8 @@ class B200Backend:
         if not torch.cuda.is_available():
             raise RuntimeError("B200Backend needs a CUDA device; there is no CPU fallback")
         self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise ValueError(f"B200Backend runs on CUDA devices only, not {device!r}")
         self._array_backend = torch
         self._float_dtype = _tdtype(float_dtype)
         self._complex_dtype = _tdtype(complex_dtype)

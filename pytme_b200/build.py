@@ -35,7 +35,8 @@ def _nvcc() -> str:
 
 
 def _newest_header() -> float:
-    hs = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    hs = (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
+          + glob.glob(os.path.join(INCLUDE, "*.h")))
     return max((os.path.getmtime(h) for h in hs), default=0.0)
 
 

@@ -1,6 +1,7 @@
 // Exported C ABI (include/pytme_b200.h). Thin wrappers over the internal ops;
 // argument checking lives here and in the ops.
 #include "common.cuh"
+#include "diagnostics.h"
 #include "ops.cuh"
 #include "peaks.cuh"
 #include "refine.cuh"
@@ -47,6 +48,11 @@ static tmb::RefineArgs refine_args(const tm_refine_desc* d) {
 extern "C" {
 
 int tm_version(void) { return 100; }
+
+int tm_set_device_memory_limit(int64_t bytes) {
+  tmb::set_device_memory_limit(bytes);
+  return TM_OK;
+}
 
 int tm_last_error(char* buf, size_t len) {
   const char* msg = tmb::last_error();
@@ -235,6 +241,20 @@ int tm_scan_set_zpass(tm_scan* plan, int mode) {
 
 int tm_scan_zpass_mode(const tm_scan* plan) {
   return plan ? tmb::scan_zpass_mode(plan->impl) : TM_E_INVALID;
+}
+
+int tm_scan_set_ypass(tm_scan* plan, int mode) {
+  TM_REQUIRE(plan, "tm_scan_set_ypass: null plan");
+  return tmb::scan_set_ypass(plan->impl, mode);
+}
+
+int tm_scan_ypass_mode(const tm_scan* plan) {
+  return plan ? tmb::scan_ypass_mode(plan->impl) : TM_E_INVALID;
+}
+
+int tm_scan_set_wait_budget(tm_scan* plan, uint32_t iters) {
+  TM_REQUIRE(plan, "tm_scan_set_wait_budget: null plan");
+  return tmb::scan_set_wait_budget(plan->impl, iters);
 }
 
 int tm_scan_check(tm_scan* plan, void* stream) {

@@ -25,6 +25,9 @@ def test_library_exports_every_declared_symbol():
     for name in names:
         assert hasattr(lib, name), f"{name} declared in include/pytme_b200.h but not exported"
     assert set(N.EXPORTED) == set(names)
+    # the test-only diagnostics are exported too, but declared outside the public header
+    for name in N.DIAGNOSTICS:
+        assert hasattr(lib, name) and name not in names
 
 
 def test_version_and_error_buffer():
