@@ -14,6 +14,8 @@
 namespace tmb {
 
 void set_error(const char* fmt, ...);
+void set_device_memory_limit(int64_t bytes);
+int64_t device_memory_limit();
 
 inline int cuda_status(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return TM_OK;

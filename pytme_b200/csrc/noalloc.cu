@@ -11,6 +11,9 @@
 #include "common.cuh"
 #include "peaks.cuh"
 
+#include <cuda.h>  // CUcontext and CUresult types only; the driver calls go through
+                   // cudaGetDriverEntryPointByVersion
+
 #include <mutex>
 #include <unordered_map>
 
@@ -20,17 +23,53 @@ namespace {
 // TM_NOALLOC_MAX_POINTS points
 __device__ __align__(256) int64_t g_candidate_scratch[3 * TM_NOALLOC_MAX_POINTS];
 
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
 std::mutex g_scratch_mutex;
-std::unordered_map<int, void*> g_scratch_address;  // device ordinal -> device address
+// CUDA context ID -> device address of g_candidate_scratch in that context. Context
+// IDs are unique for the life of the process, so a context created after
+// cudaDeviceReset (which unloads this module and loads it again) gets a new entry.
+std::unordered_map<unsigned long long, void*> g_scratch_address;
+
+template <typename F>
+F driver_function(const char* name) {
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+  if (cudaGetDriverEntryPointByVersion(name, &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess)
+    return nullptr;
+  return reinterpret_cast<F>(fn);
+}
+
+// ID of the calling thread's current context (the device's primary context once the
+// runtime has initialised it).
+int current_context_id(unsigned long long* id) {
+  static const CtxGetCurrentFn get_current = driver_function<CtxGetCurrentFn>("cuCtxGetCurrent");
+  static const CtxGetIdFn get_id = driver_function<CtxGetIdFn>("cuCtxGetId");
+  TM_REQUIRE(get_current && get_id,
+             "tm_find_candidate_indices_noalloc: the driver has no cuCtxGetCurrent/cuCtxGetId");
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr || get_id(ctx, id) != CUDA_SUCCESS) {
+    tmb::set_error("tm_find_candidate_indices_noalloc: no current CUDA context");
+    return TM_E_CUDA;
+  }
+  return TM_OK;
+}
 
 // Host code cannot pass g_candidate_scratch itself to a kernel: on the host that
 // name is a stand-in object, not a device address. Look the address up once per
-// device, with that device current.
+// device (per context), with that device current.
 int scratch_address(void** out) {
+  // cudaSetDevice initialises the current device's primary context and makes it current
+  // (CUDA 12), without allocating anything
   int dev = 0;
   TM_TRY(tmb::cuda_status(cudaGetDevice(&dev), "tm_find_candidate_indices_noalloc: device"));
+  TM_TRY(tmb::cuda_status(cudaSetDevice(dev), "tm_find_candidate_indices_noalloc: device"));
+  unsigned long long ctx = 0;
+  TM_TRY(current_context_id(&ctx));
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  auto it = g_scratch_address.find(dev);
+  auto it = g_scratch_address.find(ctx);
   if (it != g_scratch_address.end()) {
     *out = it->second;
     return TM_OK;
@@ -38,7 +77,7 @@ int scratch_address(void** out) {
   void* ptr = nullptr;
   TM_TRY(tmb::cuda_status(cudaGetSymbolAddress(&ptr, g_candidate_scratch),
                           "tm_find_candidate_indices_noalloc: cudaGetSymbolAddress"));
-  g_scratch_address[dev] = ptr;
+  g_scratch_address[ctx] = ptr;
   *out = ptr;
   return TM_OK;
 }

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <mutex>
+#include <atomic>
 #include <string>
 
 namespace tmb {
@@ -24,6 +25,12 @@ void set_error(const char* fmt, ...) {
 }
 
 const char* last_error() { return g_last_error.c_str(); }
+
+// Process-wide cap on the device memory a plan may hold (0: none), see
+// tm_set_device_memory_limit.
+static std::atomic<int64_t> g_memory_limit{0};
+void set_device_memory_limit(int64_t bytes) { g_memory_limit.store(bytes > 0 ? bytes : 0); }
+int64_t device_memory_limit() { return g_memory_limit.load(); }
 
 // --------------------------------------------------------------- rigid transform
 // Pull-interpolation out[o] = interp(in, M[:3,:3] o + M[:3,3]) with SciPy's

@@ -62,6 +62,10 @@ int max_filter_peaks(const float* scores, int n0, int n1, int n2, int size, floa
 constexpr int kNmsThreads = 1024;
 
 __device__ __forceinline__ bool too_close(int64_t dx, int64_t dy, int64_t dz, int64_t md) {
+  // floor(sqrt(d2)) <= md is never true for md < 0 (every point is kept) and always
+  // true once (md + 1)^2 exceeds any squared distance of 32-bit coordinates
+  if (md < 0) return false;
+  if (md >= (int64_t)3037000499LL) return true;
   int64_t d2 = dx * dx + dy * dy + dz * dz;
   // floor(sqrt(d2)) <= md  <=>  d2 < (md + 1)^2 for non-negative integers
   return d2 < (md + 1) * (md + 1);

@@ -32,7 +32,9 @@
 #include "fft_smem.cuh"
 #include "ops.cuh"
 #include "scan.cuh"
+#include "tc_common.cuh"
 #include "xcorr_tc.cuh"
+#include "ypass_tc.cuh"
 #include "zpass_tc.cuh"
 
 #include <type_traits>
@@ -1035,6 +1037,13 @@ struct Scan {
   bool ztc_avail = false, ztc = false;
   ZpassTcConfig zcfg{};
   uint16_t* ztable = nullptr;
+  // tensor-core y pass (CC / FLCSphericalMask, half-precision H, n1 in {256, 512}): the
+  // two DFT operators
+  bool ytc_avail = false, ytc = false;
+  YpassTcConfig ycfg{};
+  uint16_t* ytable = nullptr;
+  // polls of every data wait of the tensor-core kernels before they give up
+  uint32_t wait_iters = tc_wait_iters_default();
   // per-group scratch
   float* rot_t = nullptr;
   float* rot_m = nullptr;
@@ -1172,7 +1181,8 @@ static void launch_zpass(Scan* s, dim3 g4, HT* H, int nb, int64_t rows, float ou
                          int32_t first, float* state_max, int32_t* state_rot, cudaStream_t st) {
   if (s->ztc && std::is_same<HT, __half2>::value) {
     zpass_tc_run(s->zcfg, H, nb, rows, s->n2, s->h2, s->hp, s->ztable, out_scale, s->inv_den,
-                 first, state_max, state_rot, s->SH, s->graph_first, s->tc_err, st);
+                 first, state_max, state_rot, s->SH, s->graph_first, s->tc_err, st,
+                 s->wait_iters);
     return;
   }
   if (zpass4_supported(s->n2 / 2) && !getenv("PYTME_B200_GENERIC_FFT")) {
@@ -1276,7 +1286,8 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
     TM_DISPATCH_N(s->n0, (launch_xpass_flc_reg<NN, HT>(s, nb, hs, H, stream)));
   } else if (s->xtc) {
     TM_TRY(xcorr_tc_run(s->xcfg, s->G, s->ctarget, nb, s->t0, s->n0, s->n1, s->h2, s->hp, hs,
-                        H, std::is_same<HT, __half2>::value, s->tc_err, stream));
+                        H, std::is_same<HT, __half2>::value, s->tc_err, stream,
+                        s->wait_iters));
   } else if (s->reg0) {
     TM_DISPATCH_N(s->n0, (launch_xpass_reg<NN, HT>(s, nb, hs, H, stream)));
   } else {
@@ -1288,7 +1299,10 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
   TM_TRY(check_launch("x pass"));
   tmr.end(TM_STAGE_XPASS);
   tmr.begin();
-  if (s->reg1) {
+  if (s->ytc && std::is_same<HT, __half2>::value) {
+    TM_TRY(ypass_tc_run(s->ycfg, H, nb, s->n0, s->hp, s->ytable, s->wait_iters, s->tc_err,
+                        stream));
+  } else if (s->reg1) {
     TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, HT>(s, nb, H, stream)));
     if (flc) {
       TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, float2>(s, nb, s->Hm, stream)));
@@ -1412,12 +1426,16 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     o_tw1 = take(sizeof(float2) * s->n1);
     o_tw2 = take(sizeof(float2) * s->n2);
   }
-  size_t o_ct = 0, o_err = 0, o_zt = 0;
+  size_t o_ct = 0, o_err = 0, o_zt = 0, o_yt = 0;
   if (s->fused && d.score != TM_SCORE_FLC && s->half) {
     TM_TRY(zpass_tc_config(s->n2, s->h2, s->hp, B, &s->zcfg));
     s->ztc_avail = s->zcfg.ok;
     s->ztc = s->ztc_avail;
     if (s->ztc_avail) o_zt = take(zpass_tc_table_bytes(s->zcfg));
+    TM_TRY(ypass_tc_config(s->n1, s->hp, &s->ycfg));
+    s->ytc_avail = s->ycfg.ok;
+    s->ytc = false;  // opt-in through tm_scan_set_ypass
+    if (s->ytc_avail) o_yt = take(ypass_tc_table_bytes(s->ycfg));
   }
   if (s->fused && d.score != TM_SCORE_FLC) {
     TM_TRY(xcorr_tc_config(s->n0, s->t0, B, &s->xcfg));
@@ -1427,8 +1445,15 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     s->xtc = s->xtc_avail && s->half && (s->xcfg.hk || s->xcfg.ws);
   }
   if (s->xtc_avail) o_ct = take(sizeof(float2) * s->S);
-  if (s->xtc_avail || s->ztc_avail) o_err = take(sizeof(int) * 4);
+  if (s->xtc_avail || s->ztc_avail || s->ytc_avail) o_err = take(sizeof(int) * 4);
   s->bytes = off;
+  const int64_t cap = device_memory_limit();
+  if (cap > 0 && (int64_t)s->bytes > cap) {
+    set_error("scan_create: the plan needs %zu bytes of device memory, above the limit of %lld "
+              "bytes set by tm_set_device_memory_limit", s->bytes, (long long)cap);
+    delete s;
+    return TM_E_OOM;
+  }
   cudaError_t e = cudaMalloc(&s->base, s->bytes);
   if (e != cudaSuccess) {
     set_error("scan_create: cudaMalloc of %zu bytes failed: %s", s->bytes, cudaGetErrorString(e));
@@ -1467,9 +1492,15 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     }
     s->tw0 = reinterpret_cast<float2*>(b8 + o_tw0);
     if (s->xtc_avail) s->ctarget = reinterpret_cast<float2*>(b8 + o_ct);
-    if (s->xtc_avail || s->ztc_avail) {
+    if (s->xtc_avail || s->ztc_avail || s->ytc_avail) {
       s->tc_err = reinterpret_cast<int*>(b8 + o_err);
       cudaMemset(s->tc_err, 0, sizeof(int));
+    }
+    if (s->ytc_avail) {
+      s->ytable = reinterpret_cast<uint16_t*>(b8 + o_yt);
+      int st = ypass_tc_prepare(s->ycfg, s->ytable, 0);
+      if (st == TM_OK) st = cuda_status(cudaDeviceSynchronize(), "scan_create: y operators");
+      if (st != TM_OK) { destroy(s); return st; }
     }
     if (s->ztc_avail) {
       s->ztable = reinterpret_cast<uint16_t*>(b8 + o_zt);
@@ -1670,7 +1701,37 @@ int scan_set_zpass(Scan* s, int mode) {
 
 int scan_zpass_mode(const Scan* s) { return s && s->ztc ? 0 : 1; }
 
-// Synchronise `stream` and report a timed-out wait of the tensor-core x pass.
+// y pass on the tensor cores (mode 0: two FP16 GEMM stages, half-precision CC /
+// FLCSphericalMask plans with n1 in {256, 512}) or as FFTs on the CUDA cores (mode 1);
+// mode 2 restores the default.
+int scan_set_ypass(Scan* s, int mode) {
+  TM_REQUIRE(s, "scan_set_ypass: null plan");
+  TM_REQUIRE(mode >= 0 && mode <= 2,
+             "scan_set_ypass: mode must be 0 (tensor cores), 1 (FFT) or 2 (default)");
+  const bool want = mode == 0;
+  if (want && !s->ytc_avail) {
+    set_error("scan_set_ypass: the tensor-core y pass does not support this plan");
+    return TM_E_UNSUPPORTED;
+  }
+  if (want != s->ytc && s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+  s->ytc = want;
+  return TM_OK;
+}
+
+int scan_ypass_mode(const Scan* s) { return s && s->ytc ? 0 : 1; }
+
+// Polls of every data wait in the plan's tensor-core kernels (0 restores the default).
+int scan_set_wait_budget(Scan* s, uint32_t iters) {
+  TM_REQUIRE(s, "scan_set_wait_budget: null plan");
+  const uint32_t v = iters ? iters : tc_wait_iters_default();
+  if (v != s->wait_iters && s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+  s->wait_iters = v;
+  return TM_OK;
+}
+
+uint32_t tc_wait_iters_default() { return tc::kWaitIters; }
+
+// Synchronise `stream` and report a timed-out wait of the tensor-core passes.
 int scan_check(Scan* s, cudaStream_t stream) {
   TM_REQUIRE(s, "scan_check: null plan");
   TM_TRY(cuda_status(cudaStreamSynchronize(stream), "scan_check"));

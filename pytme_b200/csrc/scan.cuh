@@ -23,6 +23,11 @@ int scan_set_xpass(Scan* s, int mode);
 int scan_xpass_mode(const Scan* s);
 int scan_set_zpass(Scan* s, int mode);
 int scan_zpass_mode(const Scan* s);
+int scan_set_ypass(Scan* s, int mode);
+int scan_ypass_mode(const Scan* s);
+int scan_set_wait_budget(Scan* s, uint32_t iters);
+// default poll budget of a tensor-core wait (tc_common.cuh kWaitIters)
+uint32_t tc_wait_iters_default();
 int scan_check(Scan* s, cudaStream_t stream);
 int scan_run(Scan* s, const float* matrices, int n, int32_t first_index, float* state_max,
              int32_t* state_rot, cudaStream_t stream);

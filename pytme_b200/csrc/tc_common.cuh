@@ -56,6 +56,23 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
 
 constexpr uint32_t kWaitIters = 1u << 22;
 
+// Wait for the completion of the mbarrier phase with the given parity, polling at most
+// `iters` times; false when it did not complete.
+__device__ __forceinline__ bool mbar_wait_n(uint32_t mbar, uint32_t phase, uint32_t iters) {
+  for (uint32_t i = 0; i < iters; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // Bounded wait for the completion of the mbarrier phase with the given parity.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
   for (uint32_t i = 0; i < kWaitIters; ++i) {

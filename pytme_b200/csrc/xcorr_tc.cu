@@ -28,6 +28,7 @@
 // Every wait is bounded; on a timeout the kernel records an error, frees its tensor
 // memory and returns.
 #include "common.cuh"
+#include "tc_common.cuh"
 #include "xcorr_tc.cuh"
 
 #include <cuda_bf16.h>
@@ -42,26 +43,12 @@ namespace {
 
 constexpr int kTcThreads = 256;
 constexpr int kTileRows = 128;          // MMA M: 64 values of x' as (Re, Im) row pairs
-constexpr uint32_t kWaitIters = 1u << 22;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// Canonical K-major, no-swizzle BF16 operand: element (r, k) of a rows x K tile, in
-// 8-row x 16-byte core matrices (K-adjacent core matrices 128 bytes apart).
-__device__ __forceinline__ int kmajor16(int r, int k, int K) {
-  return (r >> 3) * (K * 8) + (k >> 3) * 64 + (r & 7) * 8 + (k & 7);
-}
-
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr >> 4) & 0x3fffu);
-  d |= (uint64_t)((lbo >> 4) & 0x3fffu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3fffu) << 32;
-  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
-  return d;                // base offset 0, no swizzle
-}
+using tc::kmajor16;
+using tc::kWaitIters;
+using tc::mbar_wait;
+using tc::mma_commit;
+using tc::smem_desc;
+using tc::smem_u32;
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
                                          uint32_t accumulate) {
@@ -71,28 +58,6 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
       :
       : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t mbar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-               :
-               : "r"(mbar)
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-  for (uint32_t i = 0; i < kWaitIters; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(mbar), "r"(phase)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
 }
 
 __device__ __forceinline__ void tmem_ld8(uint32_t addr, float (&v)[8]) {
@@ -638,10 +603,10 @@ static int launch_xcorr(const XcorrTcConfig& cfg, const float2* G, const float2*
 
 int xcorr_tc_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int nb, int t0,
                  int n0, int n1, int h2, int hp, float scale, void* H, bool half, int* err,
-                 cudaStream_t stream) {
+                 cudaStream_t stream, uint32_t wait_iters) {
   if (half && cfg.ws && nb <= cfg.ws_NB && hp % 8 == 0)
     return xcorr_ws_run(cfg, G, C, nb, t0, n0, n1, h2, hp, scale, static_cast<__half2*>(H), err,
-                        stream);
+                        stream, wait_iters);
   TM_REQUIRE(cfg.ok, "xcorr_tc_run: unsupported configuration");
   TM_REQUIRE(nb <= cfg.NB, "xcorr_tc_run: %d rotations exceed the configured %d", nb, cfg.NB);
   if (half && cfg.hk) {

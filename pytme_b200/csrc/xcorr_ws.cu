@@ -167,8 +167,9 @@ template <int NXC, int R>
 __global__ void __launch_bounds__(kWsThreads, 1)
 xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int nb, int NB,
                 int t0, int n0, int n1, int h2, int hp, float scale,
-                __half2* __restrict__ H, int* __restrict__ err) {
+                __half2* __restrict__ H, int* __restrict__ err, uint32_t wait_iters) {
   constexpr int t0p = 8 * NXC;
+  const uint32_t wi = wait_iters ? wait_iters : kWaitIters;  // data waits
   constexpr uint32_t kAccCols = 16u * R;               // one fill
   constexpr int kNbuf = (int)(kWsTmemCols / kAccCols);  // 2 (R = 16) or 1 (R = 32)
   extern __shared__ __align__(128) uint8_t smem_ws[];
@@ -239,17 +240,17 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
       bool ok = true;
       for (int64_t j = 0; j < mine && ok; ++j) {
         const int bsl = (int)(j & 1);
-        if (!mbar_wait(smem_u32(bfull + bsl), (uint32_t)(j >> 1) & 1u)) { ok = false; break; }
+        if (!mbar_wait_n(smem_u32(bfull + bsl), (uint32_t)(j >> 1) & 1u, wi)) { ok = false; break; }
         for (int t = 0; t < ntile; ++t) {
           const int64_t tau = j * ntile + t;
           const int zsl = (int)(tau & 1);
-          if (!mbar_wait(smem_u32(zfull + zsl), (uint32_t)(tau >> 1) & 1u)) { ok = false; break; }
+          if (!mbar_wait_n(smem_u32(zfull + zsl), (uint32_t)(tau >> 1) & 1u, wi)) { ok = false; break; }
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           for (int h = 0; h < nh; ++h) {
             const int64_t f = tau * nh + h;
             const int buf = (int)(f % kNbuf);
             const uint32_t uf = (uint32_t)(f / kNbuf);
-            if (f >= kNbuf && !mbar_wait(smem_u32(tempty + buf), (uf - 1) & 1u)) {
+            if (f >= kNbuf && !mbar_wait_n(smem_u32(tempty + buf), (uf - 1) & 1u, wi)) {
               ok = false;
               break;
             }
@@ -277,7 +278,7 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
     const int ntask = kWsW * NB * nxc;
     for (int64_t j = 0; j < mine; ++j) {
       const int bsl = (int)(j & 1);
-      if (j >= 2 && !mbar_wait(smem_u32(bempty + bsl), (uint32_t)((j >> 1) - 1) & 1u)) {
+      if (j >= 2 && !mbar_wait_n(smem_u32(bempty + bsl), (uint32_t)((j >> 1) - 1) & 1u, wi)) {
         *fail = 1;
         break;
       }
@@ -358,7 +359,7 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
         if (t + 1 < ntile) fetch(j, t + 1);
         else if (j + 1 < mine) fetch(j + 1, 0);
         bool bad = false;
-        if (tau >= 2) bad = !mbar_wait(smem_u32(zempty + zsl), (uint32_t)((tau >> 1) - 1) & 1u);
+        if (tau >= 2) bad = !mbar_wait_n(smem_u32(zempty + zsl), (uint32_t)((tau >> 1) - 1) & 1u, wi);
         if (builders_any(bad)) {  // also: e of this tile complete
           *fail = 1;
           stop = true;
@@ -401,7 +402,7 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
         for (int h = 0; h < nh; ++h) {
           const int64_t f = tau * nh + h;
           const int buf = (int)(f % kNbuf);
-          const bool got = mbar_wait(smem_u32(tfull + buf), (uint32_t)(f / kNbuf) & 1u);
+          const bool got = mbar_wait_n(smem_u32(tfull + buf), (uint32_t)(f / kNbuf) & 1u, wi);
           __syncwarp();  // tcgen05.ld needs the whole warp, converged
           if (!__all_sync(0xffffffffu, got)) {
             *fail = 1;
@@ -477,7 +478,7 @@ int xcorr_ws_config(int n0, int t0, int nb, XcorrTcConfig* cfg) {
 
 int xcorr_ws_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int nb, int t0,
                  int n0, int n1, int h2, int hp, float scale, __half2* H, int* err,
-                 cudaStream_t stream) {
+                 cudaStream_t stream, uint32_t wait_iters) {
   // 32-byte row segments: pitch a multiple of 8 complex values, aligned base
   TM_REQUIRE(cfg.ws && nb <= cfg.ws_NB && hp % 8 == 0 && hp >= h2 &&
                  reinterpret_cast<uintptr_t>(H) % 32 == 0,
@@ -495,7 +496,7 @@ int xcorr_ws_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int
     default: TM_REQUIRE(false, "xcorr_ws_run: t0p %d", cfg.ws_t0p);
   }
   fn<<<grid, kWsThreads, cfg.ws_smem, stream>>>(G, C, nb, cfg.ws_NB, t0, n0, n1, h2, hp, scale,
-                                               H, err);
+                                               H, err, wait_iters);
   return check_launch("xcorr_ws_kernel");
 }
 

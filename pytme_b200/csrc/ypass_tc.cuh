@@ -1,0 +1,30 @@
+// Tensor-core y pass of the fused CC / FLCSphericalMask scan (ypass_tc.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+namespace tmb {
+
+struct YpassTcConfig {
+  bool ok;
+  int n1;      // transform length along y: 16 * Q, Q in {16, 32}
+  int Q;
+  int sms;     // persistent grid size
+  size_t smem;
+};
+
+// Whether the tensor-core y pass handles n1 (and the row pitch hp of H).
+int ypass_tc_config(int n1, int hp, YpassTcConfig* cfg);
+size_t ypass_tc_table_bytes(const YpassTcConfig& cfg);
+// The two DFT operators (FP16 head and rounded remainder), device memory of
+// ypass_tc_table_bytes.
+int ypass_tc_prepare(const YpassTcConfig& cfg, uint16_t* table, cudaStream_t stream);
+// Unnormalised inverse DFT along axis 1 of the half-precision spectra
+// H[nb][n0][n1][hp], in place. wait_iters bounds every mbarrier wait; a wait that runs
+// out sets *err and the kernel returns early (its output is then invalid).
+int ypass_tc_run(const YpassTcConfig& cfg, void* H, int nb, int n0, int hp,
+                 const uint16_t* table, uint32_t wait_iters, int* err, cudaStream_t stream);
+
+}  // namespace tmb

@@ -108,8 +108,9 @@ zpass_tc_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
                 const uint16_t* __restrict__ Ag, float scale, const float* __restrict__ inv_den,
                 int32_t first_index, float* __restrict__ state_max,
                 int32_t* __restrict__ state_rot, int64_t SH, const int32_t* __restrict__ first_dev,
-                int* __restrict__ err) {
+                int* __restrict__ err, uint32_t wait_iters) {
   if (first_dev) first_index = *first_dev;
+  const uint32_t wi = wait_iters ? wait_iters : kWaitIters;  // data waits
   extern __shared__ __align__(128) uint16_t smem_z[];
   const int K = 2 * hp;  // multiple of 16
   const int zr = zrows(n2);
@@ -160,7 +161,7 @@ zpass_tc_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
     for (int64_t j = 0; j < mine; ++j) {
       const int sidx = (int)(j & 1);
       const uint32_t u = (uint32_t)(j >> 1);
-      if (j >= 2 && !mbar_wait(smem_u32(tempty + sidx), (u - 1) & 1u)) { *fail = 1; break; }
+      if (j >= 2 && !mbar_wait_n(smem_u32(tempty + sidx), (u - 1) & 1u, wi)) { *fail = 1; break; }
       if (*fail) break;
       const int64_t row0 = ((int64_t)blockIdx.x + j * gridDim.x) * kZRows;
       const uint32_t dst = bsa + (uint32_t)sidx * bbytes;
@@ -200,8 +201,8 @@ zpass_tc_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
       for (int64_t j = 0; j < mine; ++j) {
         const int sidx = (int)(j & 1);
         const uint32_t u = (uint32_t)(j >> 1);
-        if (!mbar_wait(smem_u32(bfull + sidx), u & 1u)) { *fail = 1; break; }
-        if (j >= 2 && !mbar_wait(smem_u32(tempty + sidx), (u - 1) & 1u)) { *fail = 1; break; }
+        if (!mbar_wait_n(smem_u32(bfull + sidx), u & 1u, wi)) { *fail = 1; break; }
+        if (j >= 2 && !mbar_wait_n(smem_u32(tempty + sidx), (u - 1) & 1u, wi)) { *fail = 1; break; }
         if (*fail) break;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::after_thread_sync;");
@@ -225,7 +226,7 @@ zpass_tc_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
     for (int64_t j = 0; j < mine; ++j) {
       const int sidx = (int)(j & 1);
       const uint32_t u = (uint32_t)(j >> 1);
-      if (!mbar_wait(smem_u32(tfull + sidx), u & 1u)) { *fail = 1; break; }
+      if (!mbar_wait_n(smem_u32(tfull + sidx), u & 1u, wi)) { *fail = 1; break; }
       if (*fail) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
       const int64_t row0 = ((int64_t)blockIdx.x + j * gridDim.x) * kZRows;
@@ -377,8 +378,10 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
                 int Kp, const uint16_t* __restrict__ Ag, float scale,
                 const float* __restrict__ inv_den, int32_t first_index,
                 float* __restrict__ state_max, int32_t* __restrict__ state_rot, int64_t SH,
-                const int32_t* __restrict__ first_dev, int* __restrict__ err) {
+                const int32_t* __restrict__ first_dev, int* __restrict__ err,
+                uint32_t wait_iters) {
   if (first_dev) first_index = *first_dev;
+  const uint32_t wi = wait_iters ? wait_iters : kWaitIters;  // data waits
   extern __shared__ __align__(128) uint16_t smem_e[];
   const int zr = eo_rows(n2);
   const int K2 = 2 * Kp;                          // rotation-operand K: Re block, Im block
@@ -463,7 +466,7 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
     for (int64_t j = grp; j < mine; j += 2) {
       const int sidx = (int)(j % kEoS);
       const uint32_t u = (uint32_t)(j / kEoS);
-      if (j >= kEoS && !mbar_wait(smem_u32(bempty + sidx), (u - 1) & 1u)) { *fail = 1; break; }
+      if (j >= kEoS && !mbar_wait_n(smem_u32(bempty + sidx), (u - 1) & 1u, wi)) { *fail = 1; break; }
       if (*fail) break;
       const int64_t row0 = ((int64_t)blockIdx.x + j * gridDim.x) * kEoRows;
       const int64_t left = rows - row0;
@@ -477,7 +480,7 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
         if ((tk >> 28) && r < rlive)
           val[m] = __ldg(reinterpret_cast<const uint4*>(H + (int64_t)b * SH + (row0 + r) * hp) + kq);
       }
-      if (j >= kEoS && !mbar_wait(smem_u32(tempty + sidx), (u - 1) & 1u)) { *fail = 1; break; }
+      if (j >= kEoS && !mbar_wait_n(smem_u32(tempty + sidx), (u - 1) & 1u, wi)) { *fail = 1; break; }
       // state and denominators of the block's rows
       const int nqs = kEoRows * n2 / 4;
       const int64_t g0 = row0 * n2;
@@ -535,8 +538,8 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
       for (int64_t j = 0; j < mine; ++j) {
         const int sidx = (int)(j % kEoS);
         const uint32_t u = (uint32_t)(j / kEoS);
-        if (!mbar_wait(smem_u32(bfull + sidx), u & 1u)) { ok = false; break; }
-        if (j >= kEoS && !mbar_wait(smem_u32(tempty + sidx), (u - 1) & 1u)) { ok = false; break; }
+        if (!mbar_wait_n(smem_u32(bfull + sidx), u & 1u, wi)) { ok = false; break; }
+        if (j >= kEoS && !mbar_wait_n(smem_u32(tempty + sidx), (u - 1) & 1u, wi)) { ok = false; break; }
         if (*fail) { ok = false; break; }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::after_thread_sync;");
@@ -565,7 +568,7 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
     for (int64_t j = 0; j < mine && ok; ++j) {
       const int sidx = (int)(j % kEoS);
       const uint32_t u = (uint32_t)(j / kEoS);
-      const bool got = mbar_wait(smem_u32(tfull + sidx), u & 1u);
+      const bool got = mbar_wait_n(smem_u32(tfull + sidx), u & 1u, wi);
       __syncwarp();  // tcgen05.ld needs the whole warp, converged
       if (!__all_sync(0xffffffffu, got)) { *fail = 1; ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;");
@@ -709,7 +712,7 @@ int zpass_tc_prepare(const ZpassTcConfig& cfg, uint16_t* table, int n2, int h2,
 int zpass_tc_run(const ZpassTcConfig& cfg, const void* H, int nb, int64_t rows, int n2, int h2,
                  int hp, const uint16_t* table, float scale, const float* inv_den,
                  int32_t first_index, float* state_max, int32_t* state_rot, int64_t SH,
-                 const int32_t* first_dev, int* err, cudaStream_t stream) {
+                 const int32_t* first_dev, int* err, cudaStream_t stream, uint32_t wait_iters) {
   TM_REQUIRE(cfg.ok, "zpass_tc_run: unsupported configuration");
   TM_REQUIRE(nb >= 1 && nb <= kZRot, "zpass_tc_run: %d rotations per group (1..%d)", nb, kZRot);
   if (cfg.eo) {
@@ -718,14 +721,14 @@ int zpass_tc_run(const ZpassTcConfig& cfg, const void* H, int nb, int64_t rows, 
     auto fn = eo_tasks(h2) <= 12 ? zpass_eo_kernel<12> : zpass_eo_kernel<13>;
     fn<<<grid, kZThreads, cfg.eo_smem, stream>>>(
         static_cast<const __half2*>(H), nb, rows, n2, h2, hp, cfg.Kp, table, scale, inv_den,
-        first_index, state_max, state_rot, SH, first_dev, err);
+        first_index, state_max, state_rot, SH, first_dev, err, wait_iters);
     return check_launch("zpass_eo_kernel");
   }
   const int64_t nblk = (rows + kZRows - 1) / kZRows;
   const int grid = (int)std::min<int64_t>(nblk, cfg.sms);
   zpass_tc_kernel<<<grid, kZThreads, cfg.smem, stream>>>(
       static_cast<const __half2*>(H), nb, rows, n2, h2, hp, table, scale, inv_den, first_index,
-      state_max, state_rot, SH, first_dev, err);
+      state_max, state_rot, SH, first_dev, err, wait_iters);
   return check_launch("zpass_tc_kernel");
 }
 

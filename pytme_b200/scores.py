@@ -146,6 +146,22 @@ class ScanPlan:
         code = {"tensor": 0, "fft": 1, "auto": 2}[mode]
         N.check(N.lib.tm_scan_set_zpass(self._h, code), "tm_scan_set_zpass")
 
+    def set_ypass(self, mode: str = "auto"):
+        """y pass on the tensor cores ("tensor"), as FFTs on the CUDA cores ("fft"), or
+        the plan's default ("auto")."""
+        code = {"tensor": 0, "fft": 1, "auto": 2}[mode]
+        N.check(N.lib.tm_scan_set_ypass(self._h, code), "tm_scan_set_ypass")
+
+    @property
+    def ypass(self) -> str:
+        """The y pass this plan runs: "tensor" or "fft"."""
+        return "tensor" if N.lib.tm_scan_ypass_mode(self._h) == 0 else "fft"
+
+    def set_wait_budget(self, iters: int = 0):
+        """Polls of every data wait in the tensor-core kernels (0: the default). A wait
+        that runs out makes ``check`` raise TimeoutError and invalidates that run."""
+        N.check(N.lib.tm_scan_set_wait_budget(self._h, int(iters)), "tm_scan_set_wait_budget")
+
     @property
     def zpass(self) -> str:
         """The z pass this plan runs: "tensor" or "fft"."""
@@ -246,6 +262,11 @@ def _setup(score: str, matching_data, fast_shape, template_filter=None, target_f
     if opts.get("zpass", "auto") != "auto" and not plan.plain and score != "FLC":
         try:
             plan.set_zpass(opts["zpass"])
+        except NotImplementedError:
+            pass
+    if opts.get("ypass", "auto") != "auto" and not plan.plain and score != "FLC":
+        try:
+            plan.set_ypass(opts["ypass"])
         except NotImplementedError:
             pass
     tf = None

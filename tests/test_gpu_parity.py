@@ -33,12 +33,12 @@ def torch_cuda():
 
 def _scan(score, target, template, mask, rotations, precision="fp32", plain=False, batch=16,
           template_filter=None, target_filter=None, pad=False, splits=None, callback=None,
-          callback_args=None, order=1, xpass="auto", zpass="auto"):
+          callback_args=None, order=1, xpass="auto", zpass="auto", ypass="auto"):
     import pytme_b200 as P
     from pytme_b200.analyzer import MaxScoreOverRotations
 
     P.backend.change_backend("b200", precision=precision, rotation_batch=batch, plain=plain,
-                             xpass=xpass, zpass=zpass)
+                             xpass=xpass, ypass=ypass, zpass=zpass)
     md = P.MatchingData(target.copy(), template.copy())
     if mask is not None:
         md.template_mask = mask.copy()
@@ -238,6 +238,9 @@ def test_greedy_filter_matches_reference(torch_cuda, golden):
     rng = np.random.default_rng(11)
     c = rng.integers(0, 400, size=(5000, 3)).astype(np.int64)
     assert np.array_equal(find_candidate_indices(c, 9), O.find_candidate_indices(c, 9))
+    # a negative minimum distance keeps every point (floor(sqrt(d2)) <= md never holds)
+    assert np.array_equal(find_candidate_indices(c, -3), O.find_candidate_indices(c, -3))
+    assert np.array_equal(find_candidate_indices(c[:100], -3), np.arange(100))
 
 
 def _filters_ctf_wedge(shape_t, shape_target):
@@ -526,3 +529,29 @@ def test_default_passes_odd_z_length(torch_cuda, score):
     tol = mixed_tol(ref64["scores"])
     assert np.abs(r[0] - ref["scores"]).max() <= tol
     assert np.abs(r[0] - ref64["scores"]).max() <= tol
+
+
+@pytest.mark.parametrize("shape,score", [((64, 512, 40), "FLCSphericalMask"),
+                                         ((48, 256, 33), "FLCSphericalMask"),
+                                         ((64, 512, 24), "CC")])
+def test_tensor_core_ypass(torch_cuda, shape, score):
+    """The tensor-core y pass (radix-16 and radix-n1/16 FP16 GEMM stages with twiddles
+    between them) for both supported y lengths, with a partial last launch group, against
+    the oracle in FP32 and FP64 and against the CUDA-core y pass."""
+    from pytme_b200 import synthetic as syn
+
+    rng = np.random.default_rng(sum(shape))
+    tmpl = syn.blob_template(12, rng, radius=3.5, sigma=1.2)
+    mask = syn.spherical_mask((12,) * 3, 6, center=(5.5,) * 3) if score != "CC" else None
+    target, _, _ = syn.make_tomogram(shape, tmpl, 4, rng, scale=0.5)
+    rots = syn.random_rotation_matrices(37, rng)
+    r = _scan(score, target, tmpl, mask, rots, precision="mixed", batch=32, ypass="tensor")
+    f = _scan(score, target, tmpl, mask, rots, precision="mixed", batch=32, ypass="fft")
+    ref = O.scan(target, tmpl, rots, score, template_mask=mask)
+    ref64 = O.scan(target, tmpl, rots, score, template_mask=mask, dtype=np.float64)
+    scale = max(1.0, float(np.abs(ref64["scores"]).max())) if score == "CC" else 1.0
+    tol = max(TOL * scale, mixed_tol(ref64["scores"]))
+    assert np.abs(r[0] - ref["scores"]).max() <= tol
+    assert np.abs(r[0] - ref64["scores"]).max() <= tol
+    assert np.abs(r[0] - f[0]).max() <= tol
+    assert np.count_nonzero(r[2] != ref64["rotations"]) <= max(2, int(1e-3 * r[2].size))

@@ -56,6 +56,32 @@ def test_noalloc_filter_matches_workspace_entry_point_on_consecutive_calls():
         assert np.array_equal(got, ref)
 
 
+def test_noalloc_filter_fills_its_whole_scratch():
+    """TM_NOALLOC_MAX_POINTS well-separated points (a grid of spacing 2 with minimum
+    distance 1): every point is kept, so the scratch array is written to its last
+    entry; the result must equal the workspace entry point's, on two calls in a row.
+    A negative minimum distance keeps every point, as the reference's integer rule
+    floor(sqrt(d2)) <= min_distance never holds then."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.set_device(0)
+    n = 65536
+    g = np.stack(np.meshgrid(np.arange(64), np.arange(64), np.arange(16), indexing="ij"),
+                 axis=-1).reshape(-1, 3).astype(np.int64) * 2
+    assert g.shape[0] == n
+    g = g[np.random.default_rng(5).permutation(n)]
+    for _ in range(2):
+        ref = _run("tm_find_candidate_indices", g, 1, use_workspace=True)
+        got = _run("tm_find_candidate_indices_noalloc", g, 1, use_workspace=False)
+        assert len(ref) == n
+        assert np.array_equal(got, ref)
+    close = np.random.default_rng(6).integers(0, 4, size=(3000, 3)).astype(np.int64)
+    got = _run("tm_find_candidate_indices_noalloc", close, -3, use_workspace=False)
+    assert np.array_equal(got, np.arange(3000))
+
+
 def test_noalloc_filter_rejects_sizes_beyond_its_scratch():
     from pytme_b200 import _native as N
 
