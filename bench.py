@@ -63,6 +63,8 @@ def parse():
                     help="rotations per end-to-end call (0: the whole set)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the config-2 (filtered FLC) and config-4 (uneven batch) legs")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="scoring-loop seconds of the cpu_baseline leg of this arm")
     ap.add_argument("--ref-seconds", type=float, default=60.0,
@@ -212,6 +214,59 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
                 "samples": len(self.samples)}
+
+
+CONFIG4_ANGLE = 12.0
+# 12 tomograms of mixed sizes between 128^3 and 320x320x160
+CONFIG4_SHAPES = ((128, 128, 128), (160, 160, 128), (192, 192, 128), (256, 256, 128),
+                  (256, 256, 160), (320, 320, 128), (320, 320, 160), (128, 256, 160),
+                  (192, 256, 128), (256, 192, 160), (160, 320, 128), (320, 256, 160))
+CONFIG4_TEMPLATES = (24, 32, 40)
+
+
+def make_config4_jobs(n_rotations=None, seed=2026):
+    """The uneven-batch workload: 12 tomograms (N(0,1) noise plus 6 rotated copies of each
+    of 3 blob templates, 24^3, 32^3 and 40^3, at SNR 0.1), every tomogram searched with
+    every template (36 jobs) over the 12-degree set, with a per-tomogram CTF (defocus
+    uniform in 1.5-4.5 um, 300 kV, Cs 2.7 mm, amplitude contrast 0.07, 6.8 A pixels, phase
+    flipped) times a continuous wedge (half-angle uniform in 50-65 degrees) on the
+    template and the wedge on the target. FLCSphericalMask with each template's spherical
+    mask. Returns a list of (job keyword arguments, template size, target index)."""
+    syn = _synthetic()
+    rng = np.random.default_rng(seed)
+    rots = syn.rotations_for_angle(CONFIG4_ANGLE)
+    if n_rotations is not None:
+        rots = np.ascontiguousarray(rots[:: max(1, len(rots) // n_rotations)][:n_rotations])
+    templates = []
+    for t in CONFIG4_TEMPLATES:
+        tmpl = syn.blob_template(t, rng, n_blobs=6, sigma=1.5 * t / 16, radius=5.0 * t / 16)
+        mask = syn.spherical_mask((t,) * 3, t / 2, center=((t - 1) / 2,) * 3)
+        templates.append((t, tmpl, mask))
+    jobs = []
+    for i, shape in enumerate(CONFIG4_SHAPES):
+        target = rng.normal(size=shape).astype(np.float32)
+        for t, tmpl, mask in templates:
+            sel = tmpl[mask > 0]
+            amp = float(np.sqrt(0.1 / max(float(sel.var()), 1e-30)))
+            syn.insert_copies(target, tmpl, 6, amp, rng)
+        defocus = float(rng.uniform(15000.0, 45000.0))
+        wedge = float(rng.uniform(50.0, 65.0))
+        for t, tmpl, mask in templates:
+            jobs.append((dict(target=target, template=tmpl, mask=mask, rotations=rots,
+                              score="FLCSphericalMask", interpolation_order=1,
+                              meta={"defocus": defocus, "wedge": wedge}), t, i))
+    return jobs
+
+
+def config4_filters(meta):
+    """Filter objects of a config-4 job (built on the GPU by scan_batch)."""
+    from pytme_b200.filters import Compose, CTFReconstructed, WedgeReconstructed
+
+    w = dict(angles=(meta["wedge"], meta["wedge"]), opening_axis=2, tilt_axis=0,
+             create_continuous_wedge=True)
+    ctf = dict(CONFIG2_CTF, defocus_x=meta["defocus"])
+    return (Compose([WedgeReconstructed(**w), CTFReconstructed(**ctf)]),
+            Compose([WedgeReconstructed(**w)]))
 
 
 # ------------------------------------------------------------------ CPU arms
@@ -616,6 +671,11 @@ def run_ours(args):
                          "d2h_bytes_per_step": d2h, "rotations_per_step": n_e2e,
                          "seconds_per_step": dt,
                          "call": "pytme_b200.scan_subsets on host NumPy arrays"}
+    if rank == 0 and world == 1 and not args.no_legs:
+        torch.cuda.empty_cache()
+        result["legs"] = {"config2": leg_config2(args.precision), "config4": leg_config4(
+            args.precision)}
+        torch.cuda.empty_cache()
     if rank == 0 and args.err_rotations > 0:
         # measured score error of the GPU map against the FP64 oracle on a rotation subset
         # spread over the set (the public API on the GPU, the oracle on the host cores)
@@ -654,6 +714,96 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def leg_config2(precision="mixed", batch=64):
+    """Filtered FLC at its workload (256x256x128, 32^3 template, CTF x wedge, the
+    1,992-rotation 15-degree set, 64 rotations per launch group), device-timed, with the
+    dominant stage's roofline."""
+    import torch
+
+    from pytme_b200.filters import Compose, CTFReconstructed, WedgeReconstructed
+    from pytme_b200.matching import fourier_padding, rigid_transform_matrices
+    from pytme_b200.scores import ScanPlan, _prepare_target
+
+    target, tmpl, mask, rots = make_config2_inputs()
+    tf = np.asarray(Compose([WedgeReconstructed(**CONFIG2_WEDGE), CTFReconstructed(
+        **CONFIG2_CTF)])(shape=tmpl.shape, return_real_fourier=True)["data"], np.float32)
+    gf = np.asarray(Compose([WedgeReconstructed(**CONFIG2_WEDGE)])(
+        shape=target.shape, return_real_fourier=True)["data"], np.float32)
+    conv, fast, _, _ = fourier_padding(target.shape, tmpl.shape)
+    plan = ScanPlan("FLC", fast, tmpl.shape, precision=precision, batch=batch)
+    plan.set_template(np.ascontiguousarray(tmpl[::-1, ::-1, ::-1]),
+                      np.ascontiguousarray(mask[::-1, ::-1, ::-1]), tf)
+    plan.set_target(_prepare_target(target, tuple(fast), gf))
+    mats = torch.as_tensor(rigid_transform_matrices(rots, (np.asarray(tmpl.shape) - 1) / 2),
+                           device="cuda")
+    smax = torch.zeros(fast, dtype=torch.float32, device="cuda")
+    sarg = torch.full(fast, -1, dtype=torch.int32, device="cuda")
+    for _ in range(3):
+        plan.run(mats[:batch], 0, smax, sarg)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    plan.run(mats, 0, smax, sarg)
+    e1.record()
+    torch.cuda.synchronize()
+    plan.check()
+    ms = e0.elapsed_time(e1)
+    plan.set_timing(True)
+    plan.run(mats[:4 * batch], 0, smax, sarg)
+    timing = plan.get_timing()
+    plan.set_timing(False)
+    stages = {k: v for k, v in timing.items() if k != "prepare"}
+    dom = max(stages, key=lambda k: stages[k][0])
+    avg = stages[dom][0] / max(stages[dom][1], 1)
+    alg = plan.stage_bytes(dom, batch)
+    peak, peak_kind = measured_peaks()
+    plan.close()
+    return {"workload": "FLC, 256x256x128 (40 copies, SNR 0.1), 32^3 template, dilated "
+                        "threshold mask, CTF x wedge template filter, wedge target filter, "
+                        "15-degree set (1992 rotations)",
+            "value": len(rots) / (ms / 1000.0), "unit": "rotations/s", "rotations": len(rots),
+            "rotation_batch": batch, "precision": precision,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": alg / (avg / 1000) / 1e9,
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": alg / (avg / 1000) / 1e9 / peak, "alg_bytes_per_launch": alg,
+                         "avg_launch_ms": avg},
+            "stages_ms_per_group": {k: round(v[0] / max(v[1], 1), 3) for k, v in stages.items()}}
+
+
+def leg_config4(precision="mixed"):
+    """The uneven batch (make_config4_jobs: 36 (tomogram, template) jobs, 12-degree set)
+    through scan_batch with the autotuned rotation batch and CUDA-graph replay; the timed
+    call includes every job's upload, target set-up, filters and result download."""
+    import torch
+
+    from pytme_b200.batch import MatchJob, autotune_batch, scan_batch
+
+    jobs = []
+    for kw, t, i in make_config4_jobs():
+        tfilt, gfilt = config4_filters(kw["meta"])
+        jobs.append(MatchJob(template_filter=tfilt, target_filter=gfilt, **kw))
+    t0 = time.perf_counter()
+    batches = {}
+    for job in jobs:
+        batches[(job.target.shape, job.template.shape)] = autotune_batch(job, precision)
+    tune_s = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = scan_batch(jobs, precision=precision, rotation_batch="auto", use_graph=True)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    n = sum(int(j.rotations.shape[0]) for j in jobs)
+    assert len(out) == len(jobs)
+    return {"workload": "36 jobs: 12 tomograms 128^3..320x320x160 x templates 24^3/32^3/40^3, "
+                        "per-tomogram CTF (1.5-4.5 um) x wedge (50-65 deg), 12-degree set "
+                        "(4344 rotations), FLCSphericalMask",
+            "value": n / dt, "unit": "job-rotations/s", "job_rotations": n, "seconds": dt,
+            "autotune_s": tune_s, "precision": precision,
+            "rotation_batches": sorted({int(b) for b in batches.values()}),
+            "timed": "scan_batch on host arrays: uploads, set-up, filters, graph replay, "
+                     "downloads"}
 
 
 def run_profile_case(args):

@@ -247,16 +247,17 @@ class PeakCaller:
         details = np.full((self.num_peaks,), -1, dtype=np.float32)
         return translations, rotations, scores, details
 
-    def _get_peak_mask(self, peaks: np.ndarray, scores: np.ndarray):
-        """tme/analyzer/peaks.py:241-290."""
+    def _get_peak_mask(self, peaks: np.ndarray, ps: np.ndarray, shape):
+        """tme/analyzer/peaks.py:241-290, given the candidates' scores ``ps`` (the
+        reference gathers them from the map inside; here they come gathered from the
+        device) and the map's ``shape``."""
         from .peaks import topk_indices
 
         if not len(peaks):
             return None
-        upper = np.subtract(np.asarray(scores.shape), self.min_boundary_distance)
+        upper = np.subtract(np.asarray(shape), self.min_boundary_distance)
         valid = np.multiply(peaks < upper, peaks >= self.min_boundary_distance)
         valid = np.sum(valid, axis=1) == peaks.shape[1]
-        ps = scores[tuple(peaks.T)]
         valid = np.multiply(ps == ps, valid)
         if self.min_score is not None:
             valid = np.multiply(ps >= self.min_score, valid)
@@ -274,20 +275,34 @@ class PeakCaller:
                 valid = np.multiply(ps <= self.max_score, valid)
         return valid
 
+    def call_candidates(self, scores, **kwargs):
+        """(positions, their scores, details) of this caller's candidate peaks. The
+        default gathers the scores of ``call_peaks``'s positions from the map on the
+        device; callers that produce scores with their positions override it."""
+        positions, details = self.call_peaks(scores=scores, **kwargs)
+        if positions is None or len(positions) == 0:
+            return None, None, details
+        positions = np.asarray(positions).astype(np.int64)
+        s = scores if isinstance(scores, torch.Tensor) else torch.as_tensor(np.asarray(scores))
+        s = s.to(device=torch.device("cuda", torch.cuda.current_device()))
+        idx = torch.as_tensor(positions, device=s.device)
+        ps = s[tuple(idx.T)].to(torch.float32).cpu().numpy()
+        return positions, ps, details
+
     def __call__(self, state, scores, rotation_matrix, **kwargs):
-        """tme/analyzer/peaks.py:327-384 for one score map."""
-        positions, details = self.call_peaks(scores=scores, rotation_matrix=rotation_matrix,
-                                             min_score=self.min_score, max_score=self.max_score)
+        """tme/analyzer/peaks.py:327-384 for one score map. The map stays on the device:
+        only the candidates (positions and scores) come to the host for the reference's
+        selection and greedy-filter bookkeeping."""
+        positions, ps, details = self.call_candidates(
+            scores=scores, rotation_matrix=rotation_matrix, min_score=self.min_score,
+            max_score=self.max_score)
         if positions is None or len(positions) == 0:
             return state
-        positions = np.asarray(positions).astype(np.int64)
-        host = scores.detach().cpu().numpy() if isinstance(scores, torch.Tensor) else \
-            np.asarray(scores)
-        valid = self._get_peak_mask(positions, host)
+        valid = self._get_peak_mask(positions, ps, tuple(scores.shape))
         if valid is None:
             return state
         positions = positions[valid]
-        pscores = host[tuple(positions.T)]
+        pscores = ps[valid]
         pdetails = np.full(pscores.shape, -1, dtype=np.float32) if details is None else \
             np.asarray(details)[valid]
         rot = np.asarray(be.to_numpy_array(rotation_matrix), dtype=np.float32)
@@ -373,3 +388,9 @@ class PeakCallerMaximumFilter(PeakCaller):
         from .peaks import max_filter_coordinates
 
         return max_filter_coordinates(scores, self.min_distance), None
+
+    def call_candidates(self, scores, **kwargs):
+        from .peaks import max_filter_candidates
+
+        positions, ps = max_filter_candidates(scores, self.min_distance)
+        return positions, ps, None

@@ -1086,6 +1086,11 @@ struct Scan {
   bool have_events = false;
 };
 
+// The tensor-core y pass hands H to the even/odd tensor-core z pass as 32-byte segments
+// [Re x 8 | Im x 8] per row and 8-column item; every other pass pair uses interleaved
+// complex values.
+static bool seg_layout(const Scan* s) { return s->ytc && s->ztc && s->zcfg.eo; }
+
 // Stage timing: record an event before a stage and accumulate after it.
 struct StageTimer {
   Scan* s;
@@ -1182,7 +1187,7 @@ static void launch_zpass(Scan* s, dim3 g4, HT* H, int nb, int64_t rows, float ou
   if (s->ztc && std::is_same<HT, __half2>::value) {
     zpass_tc_run(s->zcfg, H, nb, rows, s->n2, s->h2, s->hp, s->ztable, out_scale, s->inv_den,
                  first, state_max, state_rot, s->SH, s->graph_first, s->tc_err, st,
-                 s->wait_iters);
+                 s->wait_iters, seg_layout(s));
     return;
   }
   if (zpass4_supported(s->n2 / 2) && !getenv("PYTME_B200_GENERIC_FFT")) {
@@ -1301,7 +1306,7 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
   tmr.begin();
   if (s->ytc && std::is_same<HT, __half2>::value) {
     TM_TRY(ypass_tc_run(s->ycfg, H, nb, s->n0, s->hp, s->ytable, s->wait_iters, s->tc_err,
-                        stream));
+                        stream, seg_layout(s)));
   } else if (s->reg1) {
     TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, HT>(s, nb, H, stream)));
     if (flc) {

@@ -23,7 +23,9 @@
 //                 copies' addresses), kYS1 items in flight;
 //   warps 4-11    stage-1 epilogue: tensor memory -> head + tail -> twiddle -> FP16 ->
 //                 the stage-2 operand (rows (y1, k2), K position 2c);
-//   warps 12-15   stage-2 epilogue: tensor memory -> head + tail -> FP16 -> H.
+//   warps 12-15   stage-2 epilogue: tensor memory -> head + tail -> FP16 -> H, either as
+//                 interleaved complex values or, for the tensor-core z pass, as 32-byte
+//                 segments [Re x 8 | Im x 8] per row and item (full-sector stores both).
 // mbarriers hand every buffer between the roles; every wait is bounded by the plan's
 // wait budget, and a wait that runs out sets the error flag, after which all roles
 // leave, the MMAs in flight are waited for and the tensor memory is freed.
@@ -128,7 +130,8 @@ struct YLayout {
 template <int Q>
 __global__ void __launch_bounds__(kYThreads, 1)
 ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
-                const uint16_t* __restrict__ Tg, uint32_t wait_iters, int* __restrict__ err) {
+                const uint16_t* __restrict__ Tg, uint32_t wait_iters, int* __restrict__ err,
+                int seg) {
   using L = YLayout<Q>;
   extern __shared__ __align__(128) uint16_t smem_y[];
   uint16_t* T1s = smem_y;
@@ -327,6 +330,11 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
     const int q = warp & 3;
     const int y1 = 4 * q + (lane >> 3), k2 = lane & 7;
     const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16) + 256u;
+    // segment layout: word k2 of a row's 32-byte segment is (Re, Re) of columns 2k2, 2k2+1
+    // for k2 < 4 and (Im, Im) of columns 2(k2-4), 2(k2-4)+1 otherwise, gathered from the
+    // lanes of the same row
+    const int srcA = (lane & ~7) | ((2 * k2) & 7);
+    const uint32_t sel = k2 < 4 ? 0x5410u : 0x7632u;
     for (int64_t j = 0; j < mine; ++j) {
       const int p = (int)(j & 1);
       const uint32_t u = (uint32_t)(j >> 1);
@@ -353,7 +361,12 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           const int y2 = g * 16 + i;
-          const uint32_t v = pack_half2(re[i] + tr[i], im[i] + ti[i]);
+          uint32_t v = pack_half2(re[i] + tr[i], im[i] + ti[i]);
+          if (seg) {
+            const uint32_t a = __shfl_sync(0xffffffffu, v, srcA);
+            const uint32_t b = __shfl_sync(0xffffffffu, v, srcA + 1);
+            v = __byte_perm(a, b, sel);
+          }
           *reinterpret_cast<uint32_t*>(dst + (int64_t)(16 * y2) * hp) = v;
         }
       }
@@ -408,7 +421,8 @@ int ypass_tc_prepare(const YpassTcConfig& cfg, uint16_t* table, cudaStream_t str
 }
 
 int ypass_tc_run(const YpassTcConfig& cfg, void* H, int nb, int n0, int hp,
-                 const uint16_t* table, uint32_t wait_iters, int* err, cudaStream_t stream) {
+                 const uint16_t* table, uint32_t wait_iters, int* err, cudaStream_t stream,
+                 bool seg) {
   TM_REQUIRE(cfg.ok, "ypass_tc_run: unsupported configuration");
   TM_REQUIRE(H && table && err && nb >= 1 && n0 >= 1 && hp % 8 == 0,
              "ypass_tc_run: bad arguments");
@@ -416,10 +430,10 @@ int ypass_tc_run(const YpassTcConfig& cfg, void* H, int nb, int n0, int hp,
   const int grid = (int)std::min<int64_t>(nitems, cfg.sms);
   if (cfg.Q == 32)
     ypass_tc_kernel<32><<<grid, kYThreads, cfg.smem, stream>>>(
-        static_cast<__half2*>(H), nitems, hp, table, wait_iters, err);
+        static_cast<__half2*>(H), nitems, hp, table, wait_iters, err, seg ? 1 : 0);
   else
     ypass_tc_kernel<16><<<grid, kYThreads, cfg.smem, stream>>>(
-        static_cast<__half2*>(H), nitems, hp, table, wait_iters, err);
+        static_cast<__half2*>(H), nitems, hp, table, wait_iters, err, seg ? 1 : 0);
   return check_launch("ypass_tc_kernel");
 }
 

@@ -372,7 +372,10 @@ __device__ __forceinline__ int eo_loader_index(int tid) {
 }
 
 // MT: loader tasks per thread of the smaller group, ceil(256 * ceil(ceil(h2/4)/4) / 160).
-template <int MT>
+// SEG: H rows hold 32-byte segments [Re x 8 | Im x 8] of 8 consecutive k2 (the layout the
+// tensor-core y pass writes for this kernel) instead of interleaved complex values; the
+// loaders then copy each 16-byte half straight into the operand with cp.async.
+template <int MT, bool SEG>
 __global__ void __launch_bounds__(kZThreads, 1)
 zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int h2, int hp,
                 int Kp, const uint16_t* __restrict__ Ag, float scale,
@@ -441,6 +444,51 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
     if (grp == 0)
       for (int i = lt; i < (int)(4 * tab / 8); i += kEoGroup0)
         cp_async16(smem_u32(As) + 16u * i, Ag + 8 * (size_t)i, 16);
+    if constexpr (SEG) {
+      // piece i -> (operand row n = i / (2 nseg), segment c, half part = Re/Im): the
+      // lanes of a warp take 16 consecutive 16-byte pieces of one H row
+      const int nseg = hp / 8;
+      const int npiece = kEoN * nseg * 2;
+      for (int64_t j = grp; j < mine; j += 2) {
+        const int sidx = (int)(j % kEoS);
+        const uint32_t u = (uint32_t)(j / kEoS);
+        if (j >= kEoS && !mbar_wait_n(smem_u32(bempty + sidx), (u - 1) & 1u, wi)) {
+          *fail = 1;
+          break;
+        }
+        if (*fail) break;
+        const int64_t row0 = ((int64_t)blockIdx.x + j * gridDim.x) * kEoRows;
+        const uint32_t bj = smem_u32(Bs + (size_t)sidx * kEoN * K2);
+        for (int i = lt; i < npiece; i += gsz) {
+          const int part = i & 1, rest = i >> 1;
+          const int c = rest % nseg, n = rest / nseg;
+          const int r = n >> 5, b = n & (kZRot - 1);
+          const int64_t row = row0 + r;
+          const int valid = min(8, max(0, h2 - 8 * c));  // values k < h2 in the half
+          const bool live = b < nb && row < rows && valid > 0;
+          const __half2* src = live ? H + (int64_t)b * SH + row * hp + 8 * c + 4 * part : H;
+          cp_async16(bj + 2u * (uint32_t)kmajor16(n, part * Kp + 8 * c, K2), src,
+                     live ? 2u * (uint32_t)valid : 0u);
+        }
+        if (j >= kEoS && !mbar_wait_n(smem_u32(tempty + sidx), (u - 1) & 1u, wi)) {
+          *fail = 1;
+          break;
+        }
+        const int nqs = kEoRows * n2 / 4;
+        const int64_t g0 = row0 * n2;
+        const int64_t gend = rows * n2;
+        const uint32_t sd = smem_u32(sst + sidx * kEoRows * n2);
+        const uint32_t dd = smem_u32(sden + sidx * kEoRows * n2);
+        for (int q = lt; q < nqs; q += gsz) {
+          const int64_t g = g0 + 4 * q;
+          const uint32_t bytes = g + 4 <= gend ? 16u : (g < gend ? (uint32_t)(gend - g) * 4u : 0u);
+          cp_async16(sd + 16u * q, bytes ? state_max + g : state_max, bytes);
+          if (inv_den) cp_async16(dd + 16u * q, bytes ? inv_den + g : state_max, bytes);
+        }
+        mbar_track_cp_async(bfull + sidx);
+        mbar_arrive(bfull + sidx);
+      }
+    } else {
     // task i = (quad of 4-value chunks i >> 8, 8-row group (i >> 5) & 7, lane i & 31):
     // lanes 0-7 take rows 0-7 of chunk 4q, lanes 8-15 chunk 4q + 1, ...: 64 contiguous
     // bytes per H row per warp access, and 8-byte shared stores that fill two core
@@ -522,6 +570,7 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(bfull + sidx);
     }
+    }  // register-path loaders
   } else if (warp == 0) {
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
@@ -675,7 +724,8 @@ int zpass_tc_config(int n2, int h2, int hp, int nb, ZpassTcConfig* cfg) {
   cfg->sms = sms;
   // even/odd form: z <= n2/2 in one M = 128 tile
   if (n2 >= 16 && n2 / 2 + 1 <= 128 && eo_tasks(h2) <= 13 && cfg->eo_smem <= (size_t)optin) {
-    for (auto fn : {zpass_eo_kernel<12>, zpass_eo_kernel<13>})
+    for (auto fn : {zpass_eo_kernel<12, false>, zpass_eo_kernel<13, false>,
+                    zpass_eo_kernel<12, true>, zpass_eo_kernel<13, true>})
       TM_TRY(cuda_status(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               optin),
                          "zpass_tc: shared memory attribute"));
@@ -712,13 +762,16 @@ int zpass_tc_prepare(const ZpassTcConfig& cfg, uint16_t* table, int n2, int h2,
 int zpass_tc_run(const ZpassTcConfig& cfg, const void* H, int nb, int64_t rows, int n2, int h2,
                  int hp, const uint16_t* table, float scale, const float* inv_den,
                  int32_t first_index, float* state_max, int32_t* state_rot, int64_t SH,
-                 const int32_t* first_dev, int* err, cudaStream_t stream, uint32_t wait_iters) {
+                 const int32_t* first_dev, int* err, cudaStream_t stream, uint32_t wait_iters,
+                 bool seg) {
   TM_REQUIRE(cfg.ok, "zpass_tc_run: unsupported configuration");
+  TM_REQUIRE(!seg || cfg.eo, "zpass_tc_run: segment-layout rows need the even/odd kernel");
   TM_REQUIRE(nb >= 1 && nb <= kZRot, "zpass_tc_run: %d rotations per group (1..%d)", nb, kZRot);
   if (cfg.eo) {
     const int64_t nblk = (rows + kEoRows - 1) / kEoRows;
     const int grid = (int)std::min<int64_t>(nblk, cfg.sms);
-    auto fn = eo_tasks(h2) <= 12 ? zpass_eo_kernel<12> : zpass_eo_kernel<13>;
+    auto fn = eo_tasks(h2) <= 12 ? (seg ? zpass_eo_kernel<12, true> : zpass_eo_kernel<12, false>)
+                                 : (seg ? zpass_eo_kernel<13, true> : zpass_eo_kernel<13, false>);
     fn<<<grid, kZThreads, cfg.eo_smem, stream>>>(
         static_cast<const __half2*>(H), nb, rows, n2, h2, hp, cfg.Kp, table, scale, inv_den,
         first_index, state_max, state_rot, SH, first_dev, err, wait_iters);

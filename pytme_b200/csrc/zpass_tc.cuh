@@ -28,11 +28,12 @@ int zpass_tc_prepare(const ZpassTcConfig& cfg, uint16_t* table, int n2, int h2,
                      cudaStream_t stream);
 // c2r of the half-precision rows of H (pitch hp) for nb rotations, scaled by
 // scale * inv_den (inv_den may be null), strict running max / argmax into the state.
-// wait_iters bounds every data wait (0: the default budget).
+// wait_iters bounds every data wait (0: the default budget). seg: rows of H hold 32-byte
+// segments [Re x 8 | Im x 8] of 8 consecutive k2 (even/odd kernel only).
 int zpass_tc_run(const ZpassTcConfig& cfg, const void* H, int nb, int64_t rows, int n2, int h2,
                  int hp, const uint16_t* table, float scale, const float* inv_den,
                  int32_t first_index, float* state_max, int32_t* state_rot, int64_t SH,
                  const int32_t* first_dev, int* err, cudaStream_t stream,
-                 uint32_t wait_iters = 0);
+                 uint32_t wait_iters = 0, bool seg = false);
 
 }  // namespace tmb

@@ -319,10 +319,14 @@ def scan(matching_data: MatchingData, matching_setup: Callable, matching_score: 
          n_jobs: int = 1, callback_class=None, callback_class_args: Optional[Dict] = None,
          pad_target: bool = True, pad_template_filter: bool = False,
          interpolation_order: int = 3, jobs_per_callback_class: int = 8, target_slice=None,
-         template_slice=None, **kwargs):
+         template_slice=None, process_group=None, **kwargs):
     """One split of the search (tme/matching_exhaustive.py:144-295). Rotations are
     scored in one process on the current GPU; ``n_jobs`` only shapes the rotation
-    chunks handed to the scoring function, as in the reference."""
+    chunks handed to the scoring function, as in the reference. With ``process_group``
+    (a torch.distributed group of more than one rank, one process per GPU), each rank
+    scores its contiguous share of the rotations and one MAX all-reduce merges the
+    (score, rotation) states (``distributed.score_rotation_shares``); every rank then
+    holds the analyzer state of the whole scan."""
     from . import scores as _scores  # noqa: F401  (registers the default scores)
     from .analyzer import SharedAnalyzerProxy
 
@@ -358,8 +362,20 @@ def scan(matching_data: MatchingData, matching_setup: Callable, matching_score: 
     setup["template_filter"] = template_filter
 
     callback = SharedAnalyzerProxy(callback_class, default_args) if callback_class else None
-    for rotation in md._split_rotations_on_jobs(max(int(n_jobs), 1)):
-        matching_score(rotations=rotation, callback=callback, **setup)
+    sharded = False
+    if process_group is not None:
+        import torch.distributed as dist
+
+        sharded = dist.is_initialized() and dist.get_world_size(
+            None if process_group == "default" else process_group) > 1
+    if sharded:
+        from .distributed import score_rotation_shares
+
+        score_rotation_shares(matching_score, setup, md.rotations, callback,
+                              group=None if process_group == "default" else process_group)
+    else:
+        for rotation in md._split_rotations_on_jobs(max(int(n_jobs), 1)):
+            matching_score(rotations=rotation, callback=callback, **setup)
     if "plan" in setup:
         setup["plan"].close()
     if callback_class is None:
@@ -375,9 +391,11 @@ def scan_subsets(matching_data: MatchingData, matching_score: Callable,
                  pad_target_edges: bool = False, pad_template_filter: bool = False,
                  interpolation_order: int = 3, jobs_per_callback_class: int = 8,
                  backend_name: str = None, backend_args: Optional[Dict] = None,
-                 verbose: bool = False, **kwargs):
+                 verbose: bool = False, process_group=None, **kwargs):
     """tme/matching_exhaustive.py:298-465. Splits run one after another on the
-    current device; their analyzer results are merged with ``callback_class.merge``."""
+    current device; their analyzer results are merged with ``callback_class.merge``.
+    ``process_group`` ("default" or a torch.distributed group; one process per GPU)
+    shards every split's rotations over the group's ranks (see ``scan``)."""
     callback_class_args = dict(callback_class_args or {})
     template_splits = split_shape(matching_data._template.shape, splits=template_splits or {})
     target_splits = split_shape(matching_data._target.shape, splits=target_splits or {})
@@ -392,7 +410,8 @@ def scan_subsets(matching_data: MatchingData, matching_score: Callable,
             matching_setup=matching_setup, n_jobs=inner, callback_class=callback_class,
             callback_class_args=callback_class_args, interpolation_order=interpolation_order,
             pad_target=pad_target_edges, pad_template_filter=pad_template_filter,
-            target_slice=target_split, template_slice=template_split))
+            target_slice=target_split, template_slice=template_split,
+            process_group=process_group))
     if callback_class is not None:
         return callback_class.merge(results, **callback_class_args)
     return None

@@ -16,8 +16,8 @@ import torch
 
 from . import _native as N
 
-__all__ = ["max_filter_coordinates", "find_candidate_indices", "filter_points_indices",
-           "filter_bucket", "topk_indices", "topk_indices_device"]
+__all__ = ["max_filter_coordinates", "max_filter_candidates", "find_candidate_indices",
+           "filter_points_indices", "filter_bucket", "topk_indices", "topk_indices_device"]
 
 
 def _dev():
@@ -38,6 +38,29 @@ def max_filter_coordinates(scores, min_distance: int) -> np.ndarray:
     N.check(N.lib.tm_max_filter_peaks(N.ptr(s), *s.shape, int(min_distance), N.ptr(a), N.ptr(b),
                                       N.ptr(mask), N.stream_ptr()), "tm_max_filter_peaks")
     return torch.nonzero(mask).cpu().numpy().astype(np.int64)
+
+
+def max_filter_candidates(scores, min_distance: int):
+    """Peaks of the box maximum filter with their scores: (n, 3) int64 coordinates in C
+    order and their n float32 scores. The filter, the compaction and the gather of the
+    scores run on the device; only the candidates travel to the host (a few thousand
+    values for a 512x512x200 map, not the map)."""
+    s = scores if isinstance(scores, torch.Tensor) else torch.as_tensor(
+        np.ascontiguousarray(scores, dtype=np.float32))
+    s = s.to(device=_dev(), dtype=torch.float32).contiguous()
+    if s.ndim != 3:
+        raise NotImplementedError("peak calling is implemented for 3D score maps")
+    a = torch.empty_like(s)
+    b = torch.empty_like(s)
+    mask = torch.empty(s.shape, dtype=torch.uint8, device=s.device)
+    N.check(N.lib.tm_max_filter_peaks(N.ptr(s), *s.shape, int(min_distance), N.ptr(a), N.ptr(b),
+                                      N.ptr(mask), N.stream_ptr()), "tm_max_filter_peaks")
+    del a, b
+    flat = torch.nonzero(mask.reshape(-1)).reshape(-1)
+    vals = s.reshape(-1)[flat]
+    idx = flat.cpu().numpy()
+    coords = np.stack(np.unravel_index(idx, tuple(s.shape)), axis=1).astype(np.int64)
+    return coords, vals.cpu().numpy()
 
 
 def find_candidate_indices(coordinates, min_distance: int) -> np.ndarray:

@@ -193,3 +193,40 @@ def test_config2_bench_workload(torch_cuda):
     assert err32 <= tol and err64 <= tol
     ties = _check_ties("FLC", target, tmpl, mask, rots, rot, ref64, workers, tf=tf, gf=gf)
     print(f"config 2: {ties} argmax ties")
+
+
+def _oracle_job(args):
+    target, tmpl, mask, rots, tf, gf = args
+    return O.scan(target, tmpl, rots, "FLCSphericalMask", template_mask=mask,
+                  template_filter=tf, target_filter=gf)["scores"]
+
+
+def test_config4_every_job_on_a_rotation_subset(torch_cuda, tmp_path, monkeypatch):
+    """Config 4 (bench.make_config4_jobs): all 36 (tomogram, template) jobs, with their
+    per-tomogram CTF x wedge filters built on the GPU, through scan_batch with the
+    autotuned rotation batch and CUDA-graph replay, on 6 rotations of the 12-degree set,
+    against the FP32 oracle given the host filter arrays of the same filter objects."""
+    import multiprocessing as mp
+
+    import bench
+    from pytme_b200.batch import MatchJob, scan_batch
+
+    monkeypatch.setenv("PYTME_B200_CACHE", str(tmp_path / "autotune.json"))
+    jobs, oracle_args = [], []
+    for kw, t, i in bench.make_config4_jobs(n_rotations=6):
+        tfilt, gfilt = bench.config4_filters(kw["meta"])
+        jobs.append(MatchJob(template_filter=tfilt, target_filter=gfilt, **kw))
+        tf = np.asarray(tfilt(shape=kw["template"].shape, return_real_fourier=True)["data"],
+                        np.float32)
+        gf = np.asarray(gfilt(shape=kw["target"].shape, return_real_fourier=True)["data"],
+                        np.float32)
+        oracle_args.append((kw["target"], kw["template"], kw["mask"], kw["rotations"], tf, gf))
+    out = scan_batch(jobs, precision="mixed", rotation_batch="auto", use_graph=True)
+    with mp.get_context("spawn").Pool(_workers(2.0)) as pool:
+        refs = pool.map(_oracle_job, oracle_args, chunksize=1)
+    worst = 0.0
+    for (s, r), ref in zip(out, refs):
+        err = float(np.abs(s - ref).max())
+        worst = max(worst, err)
+        assert err <= _mixed_tol(ref), err
+    print(f"config 4: 36 jobs, max |gpu - fp32| = {worst:.3e}")
