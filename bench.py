@@ -83,16 +83,34 @@ def _synthetic():
     """pytme_b200/synthetic.py loaded by file path: the input generators are plain NumPy,
     and loading them this way keeps the reference arm from importing the package (and
     its CUDA library)."""
+    return _load_by_path("_pytme_b200_synthetic", os.path.join("pytme_b200", "synthetic.py"))
+
+
+def _load_by_path(name, rel):
     import importlib.util
 
-    mod = sys.modules.get("_pytme_b200_synthetic")
+    mod = sys.modules.get(name)
     if mod is None:
-        path = os.path.join(ROOT, "pytme_b200", "synthetic.py")
-        spec = importlib.util.spec_from_file_location("_pytme_b200_synthetic", path)
+        spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, rel))
         mod = importlib.util.module_from_spec(spec)
-        sys.modules["_pytme_b200_synthetic"] = mod
+        sys.modules[name] = mod
         spec.loader.exec_module(mod)
     return mod
+
+
+def rotation_set(angle):
+    """(float32 matrices, description): the reference's own quaternion set for ``angle``
+    when its data are available (pytme_b200/rotations.py finds them: an installed tme,
+    baseline/_ref), else the super-Fibonacci stand-in of the same size. Loaded by file
+    path so the reference arm does not import the package."""
+    rot = _load_by_path("_pytme_b200_rotations", os.path.join("pytme_b200", "rotations.py"))
+    try:
+        m = rot.get_rotation_matrices(angle)
+        return np.ascontiguousarray(m, dtype=np.float32), \
+            f"the reference's quaternion set for {angle} degrees ({len(m)} rotations)"
+    except FileNotFoundError:
+        m = _synthetic().rotations_for_angle(angle)
+        return m, f"super-Fibonacci stand-in of the reference set's size ({len(m)} rotations)"
 
 
 def make_inputs(small=False):
@@ -107,7 +125,7 @@ def make_inputs(small=False):
     c = (t - 1) / 2.0
     mask = syn.spherical_mask((t, t, t), t / 2, center=(c, c, c))
     target, _, _ = syn.make_tomogram(shape, tmpl, 20 if small else 300, rng, snr=0.05, mask=mask)
-    rots = syn.rotations_for_angle(ANGLE)
+    rots, _ = rotation_set(ANGLE)
     return target, tmpl, mask, rots
 
 
@@ -124,7 +142,7 @@ def make_config2_inputs():
     tmpl = syn.blob_template(32, rng, n_blobs=6, sigma=3.0, radius=10.0)
     mask = syn.dilated_threshold_mask(tmpl, 0.1, 2)
     target, _, _ = syn.make_tomogram(CONFIG2_SHAPE, tmpl, 40, rng, snr=0.1, mask=mask)
-    rots = syn.rotations_for_angle(CONFIG2_ANGLE)
+    rots, _ = rotation_set(CONFIG2_ANGLE)
     return target, tmpl, mask, rots
 
 
@@ -234,7 +252,7 @@ def make_config4_jobs(n_rotations=None, seed=2026):
     mask. Returns a list of (job keyword arguments, template size, target index)."""
     syn = _synthetic()
     rng = np.random.default_rng(seed)
-    rots = syn.rotations_for_angle(CONFIG4_ANGLE)
+    rots, _ = rotation_set(CONFIG4_ANGLE)
     if n_rotations is not None:
         rots = np.ascontiguousarray(rots[:: max(1, len(rots) // n_rotations)][:n_rotations])
     templates = []
@@ -486,6 +504,7 @@ def workload_config(small=False):
     return {"workload": WORKLOAD + (" [small]" if small else ""), "target_shape": list(shape),
             "template_shape": [t] * 3, "rotations": 27672, "score": "FLCSphericalMask",
             "analyzer": "MaxScoreOverRotations", "interpolation_order": 1,
+            "rotation_set": rotation_set(ANGLE)[1],
             "l2": "inputs larger than L2 (target spectrum 212 MB, state 420 MB)"}
 
 

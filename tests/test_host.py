@@ -158,3 +158,17 @@ def test_filter_bucket_matches_reference(golden):
         # the dispatch takes the bucket path above the cutoff
         assert np.array_equal(filter_points_indices(c, md, scores=sc, bucket_cutoff=len(c) - 1),
                               g[f"bucket{j}_idx"])
+
+
+def test_reference_rotation_set_matches_golden(golden):
+    """pytme_b200.rotations loads the reference's own quaternion set: the 30-degree set
+    equals the rotations the reference's scan used for the config-1 goldens."""
+    from pytme_b200 import rotations as R
+
+    if R.quaternion_data_dir() is None:
+        pytest.skip("the reference's quaternion data are not available")
+    g = golden("c1_flcsm.npz")
+    m = R.get_rotation_matrices(30).astype(np.float32)
+    assert np.array_equal(m, g["rotations"])
+    m7, desc = R.rotation_set(7.0)
+    assert m7.shape == (27672, 3, 3) and "reference" in desc
