@@ -692,8 +692,8 @@ def run_ours(args):
                          "call": "pytme_b200.scan_subsets on host NumPy arrays"}
     if rank == 0 and world == 1 and not args.no_legs:
         torch.cuda.empty_cache()
-        result["legs"] = {"config2": leg_config2(args.precision), "config4": leg_config4(
-            args.precision)}
+        # config 4 runs in FP32: its filtered maps exceed 1e-4 in mixed precision
+        result["legs"] = {"config2": leg_config2(args.precision), "config4": leg_config4("fp32")}
         torch.cuda.empty_cache()
     if rank == 0 and args.err_rotations > 0:
         # measured score error of the GPU map against the FP64 oracle on a rotation subset

@@ -281,9 +281,9 @@ class B200Backend:
         return torch.where(condition, *args) if args else torch.nonzero(condition, as_tuple=True)
 
     def unique(self, arr, return_index=False, return_inverse=False, return_counts=False,
-               **kwargs):
+               axis=None, **kwargs):
         out = np.unique(self.to_numpy_array(arr), return_index=return_index,
-                        return_inverse=return_inverse, return_counts=return_counts)
+                        return_inverse=return_inverse, return_counts=return_counts, axis=axis)
         if isinstance(out, tuple):
             return tuple(self.to_backend_array(x) for x in out)
         return self.to_backend_array(out)
@@ -302,6 +302,32 @@ class B200Backend:
 
     def reshape(self, arr, shape, **kw):
         return arr.reshape(shape)
+
+    def indices(self, dimensions, dtype=int, **kwargs):
+        """np.indices on the device: one index grid per axis, stacked first."""
+        grids = torch.meshgrid(*[torch.arange(int(n), device=self.device)
+                                 for n in dimensions], indexing="ij")
+        return torch.stack(grids).to(self._int_dtype if dtype is int else _tdtype(dtype))
+
+    def extract_center(self, arr, newshape):
+        """The centred box of ``newshape`` (tme/backends/npfftw_backend.py:308-315)."""
+        starts = [(int(c) - int(n)) // 2 for c, n in zip(arr.shape, newshape)]
+        return arr[tuple(slice(a, a + int(n)) for a, n in zip(starts, newshape))]
+
+    def center_of_mass(self, arr, cutoff=None):
+        """Centre of mass of the values above ``cutoff`` (all values when None), in
+        double precision (tme/backends/npfftw_backend.py:451-484)."""
+        a = self.to_backend_array(arr).to(torch.float64)
+        cutoff = float(a.min()) - 1 if cutoff is None else float(cutoff)
+        a = torch.where(a > cutoff, a, torch.zeros_like(a))
+        den = a.sum()
+        out = []
+        for axis, n in enumerate(a.shape):
+            shape = [1] * a.ndim
+            shape[axis] = n
+            grid = torch.arange(n, dtype=torch.float64, device=a.device).reshape(shape)
+            out.append(((a * grid) / den).sum())
+        return torch.stack(out)
 
     def unravel_index(self, indices, shape):
         return np.unravel_index(self.to_numpy_array(indices), shape)
@@ -392,45 +418,99 @@ class B200Backend:
                         use_geometric_center: bool = False, out=None, out_mask=None,
                         order: int = 3, cache: bool = False, batched: bool = False):
         """Rigid transform on the device; the reference's NumpyFFTWBackend.rigid_transform
-        (tme/backends/npfftw_backend.py:390-449) with SciPy's constant mode. Order 1 is
+        (tme/backends/npfftw_backend.py:357-449) with SciPy's constant mode. Order 1 is
         trilinear (tm_rigid_transform); order 3 is the cubic B-spline with the data
         prefiltered and the mask not (tm_spline_prefilter + tm_rigid_transform_cubic).
-        Only the geometric centre is supported."""
+        A square rotation matrix turns about the geometric centre or, by default as in the
+        reference, the data's centre of mass; a homogeneous matrix is used as given.
+        2D data run as one plane of a 3D volume; ``batched`` transforms every item along
+        the leading axis with the same matrix, as the reference loops over them."""
         if int(order) not in (1, 3):
             raise NotImplementedError("only order 1 (trilinear) and 3 (cubic B-spline) rigid "
                                       "transforms are supported")
-        if batched:
-            raise NotImplementedError("batched rigid transforms are not supported")
-        arr = self.to_backend_array(arr).to(torch.float32).contiguous()
-        matrix = self.to_backend_array(rotation_matrix)
-        if matrix.shape[-1] == arr.ndim:
-            if not use_geometric_center:
-                raise NotImplementedError("rotation about the centre of mass is not supported")
-            center = np.divide(np.asarray(arr.shape) - 1, 2)
-            matrix = self._rigid_transform_matrix(matrix, translation, center)
-        matrix = matrix.to(torch.float32).contiguous().reshape(1, 16)
+        arr = self.to_backend_array(arr)
         if out is None:
             out = torch.zeros_like(arr)
-        mask = None
         if arr_mask is not None:
-            mask = self.to_backend_array(arr_mask).to(torch.float32).contiguous()
+            arr_mask = self.to_backend_array(arr_mask)
             if out_mask is None:
-                out_mask = torch.zeros_like(mask)
-        o = out.shape
-        if int(order) == 3:
-            coef = torch.empty(arr.shape, dtype=torch.float64, device=arr.device)
-            N.check(N.lib.tm_spline_prefilter(N.ptr(arr), N.ptr(coef), *arr.shape, 1,
-                                              N.stream_ptr()), "tm_spline_prefilter")
-            mcoef = None if mask is None else mask.to(torch.float64).contiguous()
-            N.check(N.lib.tm_rigid_transform_cubic(
-                N.ptr(coef), N.ptr(mcoef), *arr.shape, N.ptr(matrix), 1, N.ptr(out),
-                N.ptr(out_mask) if mask is not None else None, *o, N.stream_ptr()),
-                "tm_rigid_transform_cubic")
+                out_mask = torch.zeros_like(arr_mask)
+        matrix = self.to_backend_array(rotation_matrix)
+        ndim = arr.ndim - int(bool(batched))
+        if matrix.shape[-1] == ndim:
+            if use_geometric_center:
+                center = np.divide(np.asarray(arr.shape[-ndim:]) - 1, 2)
+            else:
+                center = self.to_numpy_array(self.center_of_mass(arr, cutoff=0))[-ndim:]
+            if translation is not None and np.any(self.to_numpy_array(translation)):
+                raise NotImplementedError("rigid transforms with a translation are not "
+                                          "supported")
+            matrix = self._homogeneous(matrix, center)
+        if batched:
+            for i in range(arr.shape[0]):
+                self._transform_one(arr[i], matrix, out[i],
+                                    None if arr_mask is None else arr_mask[i],
+                                    None if arr_mask is None else out_mask[i], int(order))
             return out, out_mask
-        N.check(N.lib.tm_rigid_transform(N.ptr(arr), N.ptr(mask), *arr.shape, N.ptr(matrix), 1,
-                                         N.ptr(out), N.ptr(out_mask) if mask is not None else None,
-                                         *o, N.stream_ptr()), "tm_rigid_transform")
+        self._transform_one(arr, matrix, out, arr_mask, out_mask, int(order))
         return out, out_mask
+
+    def _homogeneous(self, rotation, center):
+        """Pull matrix of a rotation about ``center`` with the reference's float32
+        arithmetic, lifted to 3D for 2D data (an untouched leading axis)."""
+        from .matching import rigid_transform_matrices
+
+        rot = self.to_numpy_array(rotation).astype(np.float32)
+        c = np.asarray(center, dtype=np.float64)
+        if rot.shape[-1] == 2:
+            r3 = np.eye(3, dtype=np.float32)
+            r3[1:, 1:] = rot
+            rot, c = r3, np.concatenate(([0.0], c))
+        return self.to_backend_array(rigid_transform_matrices(rot[None], c)[0])
+
+    def _transform_one(self, arr, matrix, out, mask, out_mask, order):
+        """One volume (2D or 3D) through the library's kernels, into float32 scratch when
+        the output is another type or shares the input's memory."""
+        if arr.ndim not in (2, 3):
+            raise NotImplementedError("rigid transforms of 2D and 3D data only")
+        lift = (lambda t: t.reshape((1,) + tuple(t.shape))) if arr.ndim == 2 else (lambda t: t)
+        a = lift(arr.to(torch.float32).contiguous())
+        if a.data_ptr() == arr.data_ptr():
+            a = a.clone()  # the output may be this very buffer
+        m = None if mask is None else lift(mask.to(torch.float32).contiguous()).clone()
+        direct = out.dtype == torch.float32 and out.is_contiguous() and \
+            out.data_ptr() not in (arr.data_ptr(), 0 if mask is None else mask.data_ptr())
+        o = lift(out) if direct else torch.zeros(lift(out).shape, dtype=torch.float32,
+                                                  device=a.device)
+        om = None
+        if m is not None:
+            mdirect = out_mask.dtype == torch.float32 and out_mask.is_contiguous() and \
+                out_mask.data_ptr() not in (arr.data_ptr(), mask.data_ptr())
+            om = lift(out_mask) if mdirect else torch.zeros(lift(out_mask).shape,
+                                                            dtype=torch.float32,
+                                                            device=a.device)
+        mat = matrix.to(torch.float32)
+        if mat.numel() == 9:  # homogeneous matrix of 2D data: lift to 3D
+            m4 = torch.eye(4, dtype=torch.float32, device=mat.device)
+            m4[1:, 1:] = mat.reshape(3, 3)
+            mat = m4
+        mat = mat.contiguous().reshape(1, 16)
+        if order == 3:
+            coef = torch.empty(a.shape, dtype=torch.float64, device=a.device)
+            N.check(N.lib.tm_spline_prefilter(N.ptr(a), N.ptr(coef), *a.shape, 1,
+                                              N.stream_ptr()), "tm_spline_prefilter")
+            mcoef = None if m is None else m.to(torch.float64).contiguous()
+            N.check(N.lib.tm_rigid_transform_cubic(
+                N.ptr(coef), N.ptr(mcoef), *a.shape, N.ptr(mat), 1, N.ptr(o),
+                N.ptr(om), *o.shape, N.stream_ptr()), "tm_rigid_transform_cubic")
+        else:
+            N.check(N.lib.tm_rigid_transform(N.ptr(a), N.ptr(m), *a.shape, N.ptr(mat), 1,
+                                             N.ptr(o), N.ptr(om), *o.shape, N.stream_ptr()),
+                    "tm_rigid_transform")
+        if not direct:
+            out.copy_(o.reshape(out.shape))
+        if om is not None and om.data_ptr() != lift(out_mask).data_ptr():
+            out_mask.copy_(om.reshape(out_mask.shape))
 
     def norm_scores(self, arr, exp_sq, sq_exp, n_obs, eps, out):
         """tm_norm_scores: the reference's norm_scores (tme/backends/npfftw_backend.py:
@@ -467,10 +547,23 @@ class B200Backend:
 
     def max_filter_coordinates(self, score_space, min_distance):
         """Local maxima under a box maximum filter of edge ``min_distance``
-        (tme/backends/npfftw_backend.py:200-206)."""
+        (tme/backends/npfftw_backend.py:200-206): the library's kernel for 3D maps, torch's
+        max pooling over a zero-padded map (SciPy's constant mode, window
+        [i - d//2, i - d//2 + d - 1]) for 1D and 2D ones."""
         from .peaks import max_filter_coordinates
 
-        return max_filter_coordinates(score_space, min_distance)
+        s = self.to_backend_array(score_space)
+        if s.ndim == 3:
+            return max_filter_coordinates(s, min_distance)
+        if s.ndim not in (1, 2):
+            raise NotImplementedError("maximum filters of 1D, 2D and 3D maps only")
+        d = int(min_distance)
+        x = s.to(torch.float32)
+        lo, hi = d // 2, d - 1 - d // 2
+        xp = torch.nn.functional.pad(x[None, None], [lo, hi] * x.ndim, value=0.0)
+        pool = torch.nn.functional.max_pool1d if x.ndim == 1 else torch.nn.functional.max_pool2d
+        mf = pool(xp, kernel_size=d, stride=1)[0, 0]
+        return torch.nonzero(mf == x).cpu().numpy().astype(np.int64)
 
     # ------------------------------------------------------------ device handling
     def get_available_memory(self) -> int:

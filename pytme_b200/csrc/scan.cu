@@ -416,7 +416,8 @@ constexpr int kYStages = 2;
 
 template <int N, int W, typename HT>
 __global__ void __launch_bounds__(N / 8 * W, 1024 / (N / 8 * W))
-ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ tw1_g, int hp) {
+ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ tw1_g, int hp,
+                 int seg) {
   constexpr int T = N / 8;
   constexpr int NT = T * W;
   constexpr int R = colfft::stage_radix(N, colfft::num_stages(N) - 1);
@@ -455,6 +456,31 @@ ypass_reg_kernel(HT* __restrict__ H, int n0, int h2, const float2* __restrict__ 
       v[r] = valid ? Store<HT>::load(cur + (t + T * r) * W + l) : make_float2(0.f, 0.f);
     colfft::dif_stage_regs<N, 0, 1>(v, t, tw);
     dif_rest<N, W, 1>(v, sm, tw, l, t);
+    if constexpr (std::is_same<HT, __half2>::value) {
+      if (seg) {
+        // 32-byte segments [Re x 8 | Im x 8] of 8 consecutive k2 (the even/odd tensor-core
+        // z pass's input): the 8 lanes holding one row's segment exchange values so each
+        // stores one word, (Re, Re) of columns 2q, 2q+1 for q < 4, (Im, Im) after that
+        const int q = l & 7, lane = threadIdx.x & 31;
+        const int srcA = (lane & ~7) | ((2 * q) & 7);
+        const uint32_t sel = q < 4 ? 0x5410u : 0x7632u;
+        HT* h = base + (int64_t)xi * plane;
+#pragma unroll
+        for (int i = 0; i < 8 / R; ++i)
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int y = colfft::out_index<N>(t, i, r);
+            const __half2 hv = __float22half2_rn(v[i * R + r]);
+            uint32_t w = *reinterpret_cast<const uint32_t*>(&hv);
+            const uint32_t a = __shfl_sync(0xffffffffu, w, srcA);
+            const uint32_t b = __shfl_sync(0xffffffffu, w, srcA + 1);
+            w = __byte_perm(a, b, sel);
+            if (k2 < hp) *reinterpret_cast<uint32_t*>(h + (int64_t)y * hp) = w;
+          }
+        __syncthreads();  // the next plane's stage-0 stores reuse the exchange buffer
+        continue;
+      }
+    }
     if (valid) {
       HT* h = base + (int64_t)xi * plane;
 #pragma unroll
@@ -1086,10 +1112,14 @@ struct Scan {
   bool have_events = false;
 };
 
-// The tensor-core y pass hands H to the even/odd tensor-core z pass as 32-byte segments
-// [Re x 8 | Im x 8] per row and 8-column item; every other pass pair uses interleaved
-// complex values.
-static bool seg_layout(const Scan* s) { return s->ytc && s->ztc && s->zcfg.eo; }
+// The y pass hands H to the even/odd tensor-core z pass as 32-byte segments
+// [Re x 8 | Im x 8] per row and 8 consecutive k2, which its loaders copy straight into
+// the operand; the FFT z passes read interleaved complex values. (The generic
+// shared-memory y pass for lengths without a register kernel writes interleaved values,
+// so it is paired with them only.)
+static bool seg_layout(const Scan* s) {
+  return s->half && s->ztc && s->zcfg.eo && (s->ytc || s->reg1);
+}
 
 // Stage timing: record an event before a stage and accumulate after it.
 struct StageTimer {
@@ -1253,11 +1283,11 @@ static void launch_xpass_reg(Scan* s, int nb, float hs, HT* H, cudaStream_t st) 
 }
 
 template <int N, typename HT>
-static void launch_ypass_reg(Scan* s, int nb, HT* H, cudaStream_t st) {
+static void launch_ypass_reg(Scan* s, int nb, HT* H, cudaStream_t st, bool seg = false) {
   constexpr int W = reg_lines<N>();
   dim3 g(ceil_div(s->h2, W), ceil_div(s->n0, kYPlanes), nb);
   ypass_reg_kernel<N, W, HT><<<g, N / 8 * W, ypass_smem_bytes<N, HT>(), st>>>(
-      H, s->n0, s->h2, s->tw1, s->hp);
+      H, s->n0, s->h2, s->tw1, s->hp, seg ? 1 : 0);
 }
 
 #define TM_DISPATCH_N(n, CALL)      \
@@ -1308,7 +1338,7 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
     TM_TRY(ypass_tc_run(s->ycfg, H, nb, s->n0, s->hp, s->ytable, s->wait_iters, s->tc_err,
                         stream, seg_layout(s)));
   } else if (s->reg1) {
-    TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, HT>(s, nb, H, stream)));
+    TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, HT>(s, nb, H, stream, seg_layout(s))));
     if (flc) {
       TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, float2>(s, nb, s->Hm, stream)));
       TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, float2>(s, nb, s->Hm2, stream)));

@@ -1,35 +1,38 @@
-// y pass of the fused CC / FLCSphericalMask scan on the tensor cores.
+// y pass of the fused CC / FLCSphericalMask scan with its long stage on the tensor cores.
 //
 // For every rotation, x' plane and k2 column of the half-precision intermediate spectra
 // H[b][x'][k1][k2] (row pitch hp), the unnormalised inverse DFT along y,
 //     Y[y'] = sum_{k1 < n1} X[k1] w^(k1 y'),   w = exp(+2 pi i / n1),  n1 = 16 Q,
-// runs as two GEMM stages with k1 = Q a + c and y' = y1 + 16 y2 (a, y1 < 16; c, y2 < Q):
-//     Z[y1][c]      = sum_{a < 16} X[Q a + c] w16^(a y1)       (stage 1, radix 16)
+// runs in two stages with k1 = Q a + c and y' = y1 + 16 y2 (a, y1 < 16; c, y2 < Q):
+//     Z[y1][c]      = sum_{a < 16} X[Q a + c] w16^(a y1)       (radix 16, CUDA cores)
 //     Z'[y1][c]     = Z[y1][c] w^(c y1)                        (twiddle, CUDA cores)
-//     Y[y1 + 16 y2] = sum_{c < Q} Z'[y1][c] wQ^(c y2)          (stage 2, radix Q)
-// Complex products are real GEMMs over interleaved (Re, Im) K positions: the data are the
-// M operand (rows = independent transforms), a fixed DFT operator the N operand, with
-// output columns [Re | Im] of the operator's FP16 head and then of its FP16 rounded
-// remainder (the tail), so one MMA pass gives head and tail products side by side and the
-// epilogue adds them (the operators keep about 22 significant bits). The only added
-// rounding is that of Z' to FP16 between the stages.
+//     Y[y1 + 16 y2] = sum_{c < Q} Z'[y1][c] wQ^(c y2)          (radix Q, tensor cores)
+// The radix-16 stage is a 4 x 4 register FFT in FP32 per (c, k2) column; the radix-Q stage
+// is a real GEMM over interleaved (Re, Im) K positions: rows (y1, k2) of Z' are the M
+// operand, a fixed DFT operator the N operand, with output columns [Re | Im] of the
+// operator's FP16 head and then of its FP16 rounded remainder (the tail), so one MMA pass
+// gives both products and the epilogue adds them (about 22 significant bits). Z' enters
+// the GEMM as an FP16 head plus its FP16 rounded remainder (two K blocks against the same
+// operator), so the only rounding of the pass is that of its FP16 output, as in the FFT y
+// pass.
 //
 // A work item is one rotation, one x' plane and 8 consecutive k2 columns: n1 rows of
 // 32 bytes (one sector each), read and written in place. Roles of the persistent
 // 512-thread CTA:
-//   warp 0        one thread issues the MMAs of both stages;
-//   warps 1-3     load items straight into the stage-1 operand with 4-byte cp.async
-//                 (the gather k1 = Q a + c -> row (c, k2), K position 2a is done by the
-//                 copies' addresses), kYS1 items in flight;
-//   warps 4-11    stage-1 epilogue: tensor memory -> head + tail -> twiddle -> FP16 ->
-//                 the stage-2 operand (rows (y1, k2), K position 2c);
-//   warps 12-15   stage-2 epilogue: tensor memory -> head + tail -> FP16 -> H, either as
-//                 interleaved complex values or, for the tensor-core z pass, as 32-byte
-//                 segments [Re x 8 | Im x 8] per row and item (full-sector stores both).
+//   warp 0         one thread issues the stage-2 MMAs;
+//   warps 1-3      copy items row by row into a dense staging buffer with 16-byte
+//                  cp.async (kYS items in flight), and the operator once;
+//   warps 4-11     stage 1: one thread per (c, k2) column reads its 16 values from the
+//                  staging buffer (bank-conflict-free), runs the radix-16 FFT and the
+//                  twiddle, and writes Z' (head and tail) into the stage-2 operand;
+//   warps 12-15    stage-2 epilogue: tensor memory -> head + tail -> FP16 -> H, either as
+//                  interleaved complex values or, for the tensor-core z pass, as 32-byte
+//                  segments [Re x 8 | Im x 8] per row and item (full-sector stores both).
 // mbarriers hand every buffer between the roles; every wait is bounded by the plan's
 // wait budget, and a wait that runs out sets the error flag, after which all roles
 // leave, the MMAs in flight are waited for and the tensor memory is freed.
 #include "common.cuh"
+#include "fft_smem.cuh"
 #include "tc_common.cuh"
 #include "ypass_tc.cuh"
 
@@ -44,35 +47,28 @@ namespace {
 using namespace tc;
 
 constexpr int kYThreads = 512;
-constexpr int kYS1 = 4;         // stage-1 operand buffers (items whose loads are in flight)
+constexpr int kYS = 4;          // staging buffers (items whose loads are in flight)
 constexpr int kYLoaders = 96;   // warps 1-3
 
-// Operator tables, canonical K-major FP16 (head rows, then tail rows):
-//   T1: 64 rows x 32 K, rows [Re Z | Im Z] x 16 outputs, K = 2a + (0: Re X, 1: Im X);
-//   T2: 4Q rows x 2Q K, rows [Re Y | Im Y] x Q outputs, K = 2c + (0: Re Z', 1: Im Z').
-__host__ __device__ constexpr int t1_halves() { return 64 * 32; }
-__host__ __device__ constexpr int t2_halves(int Q) { return 4 * Q * 2 * Q; }
+// Stage-2 operator, canonical K-major FP16: 4Q rows [Re Y | Im Y] x Q outputs (head rows,
+// then tail rows) by 4Q K positions: 2c + (0: Re Z', 1: Im Z') for the FP16 head of Z',
+// and again from K = 2Q for its FP16 rounded remainder.
+__host__ __device__ constexpr int t2_halves(int Q) { return 4 * Q * 4 * Q; }
 
 __global__ void ydft_table_kernel(uint16_t* __restrict__ T, int Q) {
-  const int n1 = t1_halves(), total = n1 + t2_halves(Q);
+  const int K = 4 * Q, total = t2_halves(Q);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-    const int R = i < n1 ? 16 : Q;            // radix of the stage
-    const int K = 2 * R;
-    const int idx = i < n1 ? i : i - n1;
-    const int n = idx / K, k = idx - n * K;
-    const int part = n / (2 * R), comp = (n / R) & 1, o = n % R;
-    const int a = k >> 1, ri = k & 1;
+    const int n = i / K, k = i - n * K;
+    const int part = n / (2 * Q), comp = (n / Q) & 1, o = n % Q;
+    const int c = (k % (2 * Q)) >> 1, ri = k & 1;
     double sn, cs;
-    sincospi(2.0 * (double)((a * o) % R) / (double)R, &sn, &cs);
-    // (Re, Im) of X w^(a o): Re = Re X cos - Im X sin, Im = Re X sin + Im X cos
+    sincospi(2.0 * (double)((c * o) % Q) / (double)Q, &sn, &cs);
+    // (Re, Im) of Z' wQ^(c o): Re = Re Z' cos - Im Z' sin, Im = Re Z' sin + Im Z' cos
     const double v = comp == 0 ? (ri == 0 ? cs : -sn) : (ri == 0 ? sn : cs);
     const float vf = (float)v;
     const __half hd = __float2half_rn(vf);
     const __half tl = __float2half_rn(vf - __half2float(hd));
-    const int rows = 2 * R;  // rows per part
-    const int nn = comp * R + o;
-    const int base = i < n1 ? 0 : n1;
-    T[base + kmajor16(part * rows + nn, k, K)] = __half_as_ushort(part == 0 ? hd : tl);
+    T[kmajor16(part * 2 * Q + comp * Q + o, k, K)] = __half_as_ushort(part == 0 ? hd : tl);
   }
 }
 
@@ -87,9 +83,6 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 __device__ __forceinline__ void mbar_arrive_cp_async(uint64_t* bar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" : : "r"(smem_u32(bar))
                : "memory");
-}
-__device__ __forceinline__ void cp_async4(uint32_t smem, const void* gmem) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem), "l"(gmem));
 }
 __device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
   uint32_t r[16];
@@ -111,19 +104,14 @@ __device__ __forceinline__ uint32_t pack_half2(float re, float im) {
 template <int Q>
 struct YLayout {
   static constexpr int N1 = 16 * Q;        // transform length
-  static constexpr int R1 = 8 * Q;         // stage-1 rows (c, k2)
-  static constexpr int NT1 = R1 / 128;     // stage-1 M tiles
-  static constexpr int K1 = 32;            // stage-1 K: 16 complex inputs
-  static constexpr int NC1 = 64;           // stage-1 N: [Re | Im] x 16, head then tail
-  static constexpr int K2 = 2 * Q;         // stage-2 K: Q complex inputs
+  static constexpr int K2 = 4 * Q;         // stage-2 K: Q complex inputs, Z' head and tail
   static constexpr int NC2 = 4 * Q;        // stage-2 N: [Re | Im] x Q, head then tail
-  static constexpr int A1 = R1 * K1;       // halves per stage-1 operand buffer
+  static constexpr int S = N1 * 16;        // halves per staging buffer (n1 rows of 32 B)
   static constexpr int A2 = 128 * K2;      // halves per stage-2 operand buffer
-  static constexpr int EPI1 = 128 * NT1;   // stage-1 epilogue threads
+  static constexpr int EPI1 = 8 * Q;       // stage-1 threads: one per (c, k2)
   static constexpr int EPI2 = 128;
   static constexpr size_t smem_bytes() {
-    return (size_t)(t1_halves() + t2_halves(Q) + kYS1 * A1 + 2 * A2) * 2 +
-           (size_t)(2 * kYS1 + 9) * 8 + 16;
+    return (size_t)(t2_halves(Q) + kYS * S + 2 * A2) * 2 + (size_t)(2 * kYS + 8) * 8 + 16;
   }
 };
 
@@ -134,18 +122,17 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
                 int seg) {
   using L = YLayout<Q>;
   extern __shared__ __align__(128) uint16_t smem_y[];
-  uint16_t* T1s = smem_y;
-  uint16_t* T2s = T1s + t1_halves();
-  uint16_t* A1s = T2s + t2_halves(Q);
-  uint16_t* A2s = A1s + kYS1 * L::A1;
+  uint16_t* T2s = smem_y;
+  uint16_t* Ss = T2s + t2_halves(Q);                // kYS staging buffers
+  uint16_t* A2s = Ss + kYS * L::S;                  // 2 stage-2 operand buffers
   uint64_t* bar = reinterpret_cast<uint64_t*>(A2s + 2 * L::A2);
-  uint64_t* a1full = bar;              // [kYS1] item loaded (loader threads, async)
-  uint64_t* a1empty = bar + kYS1;      // [kYS1] stage-1 MMAs done with the operand (commit)
-  uint64_t* d1full = bar + 2 * kYS1;   // [2] stage-1 accumulators written (commit)
-  uint64_t* e1done = d1full + 2;       // [2] stage-1 epilogue: D1 read, A2 written
-  uint64_t* s2done = e1done + 2;       // [2] stage-2 MMAs done: A2 free, D2 written (commit)
+  uint64_t* sfull = bar;               // [kYS] item staged (loader threads, async)
+  uint64_t* sempty = bar + kYS;        // [kYS] stage 1 read the item (stage-1 threads)
+  uint64_t* e1done = bar + 2 * kYS;    // [2] stage 1 wrote the operand (stage-1 threads)
+  uint64_t* s2done = e1done + 2;       // [2] stage-2 MMAs done: operand free, D2 written
   uint64_t* d2empty = s2done + 2;      // [2] stage-2 epilogue read D2
-  uint64_t* mdone = d2empty + 2;
+  uint64_t* tfull = d2empty + 2;       // the operator landed (loader threads, async)
+  uint64_t* mdone = tfull + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mdone + 1);
   volatile int* fail = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -153,20 +140,20 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  :
-                 : "r"(smem_u32(tmem_slot)), "r"(512));
+                 : "r"(smem_u32(tmem_slot)), "r"(256));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    for (int s = 0; s < kYS1; ++s) {
-      mbar_init(a1full + s, kYLoaders);
-      mbar_init(a1empty + s, 1);
+    for (int s = 0; s < kYS; ++s) {
+      mbar_init(sfull + s, kYLoaders);
+      mbar_init(sempty + s, L::EPI1);
     }
     for (int p = 0; p < 2; ++p) {
-      mbar_init(d1full + p, 1);
       mbar_init(e1done + p, L::EPI1);
       mbar_init(s2done + p, 1);
       mbar_init(d2empty + p, L::EPI2);
     }
+    mbar_init(tfull, kYLoaders);
     mbar_init(mdone, 1);
     asm volatile("fence.mbarrier_init.release.cluster;");
     *fail = 0;
@@ -175,8 +162,7 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tmem_slot;
-  // tensor memory: D1 (stage-1 accumulators) in columns [0, 256), two buffers of 128;
-  // D2 in [256, 512), two buffers of 128
+  // tensor memory: D2 (stage-2 accumulators) in two buffers of 128 columns
   const int64_t mine = nitems > blockIdx.x ? (nitems - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const int nc = hp / 8;  // items per (rotation, x') plane
   auto item_base = [&](int64_t j) -> int64_t {
@@ -187,89 +173,54 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
   if (warp >= 1 && warp <= 3) {
     // ---------------------------------------------------------------- loaders
     const int lt = tid - 32;
-    constexpr int tpieces = (t1_halves() + t2_halves(Q)) / 8;
+    constexpr int tpieces = t2_halves(Q) / 8;
     for (int i = lt; i < tpieces; i += kYLoaders)
-      cp_async16(smem_u32(T1s) + 16u * i, Tg + 8 * (size_t)i, 16);
-    // lane -> (j4 = lane >> 3, k2 = lane & 7); warp task t -> (am = t & 3, c = t >> 2),
-    // a = 4 am + j4: element X[Q a + c][k2] goes to row 8c + k2, K position 2a, i.e. byte
-    // 512 c + 128 am + 16 k2 + 4 j4 of the operand (32 distinct banks per warp access)
-    const int wl = warp - 1, j4 = lane >> 3, k2 = lane & 7;
+      cp_async16(smem_u32(T2s) + 16u * i, Tg + 8 * (size_t)i, 16);
+    mbar_arrive_cp_async(tfull);
+    // 16-byte piece i: row i >> 1, half i & 1 of the row's 32 bytes (dense rows)
     for (int64_t j = 0; j < mine; ++j) {
-      const int s = (int)(j % kYS1);
-      const uint32_t u = (uint32_t)(j / kYS1);
-      if (j >= kYS1 && !mbar_wait_n(smem_u32(a1empty + s), (u - 1) & 1u, wait_iters)) {
+      const int s = (int)(j % kYS);
+      const uint32_t u = (uint32_t)(j / kYS);
+      if (j >= kYS && !mbar_wait_n(smem_u32(sempty + s), (u - 1) & 1u, wait_iters)) {
         *fail = 1;
         break;
       }
       if (*fail) break;
-      const __half2* src0 = H + item_base(j) + k2;
-      const uint32_t dst0 = smem_u32(A1s + (size_t)s * L::A1) + 16u * k2 + 4u * j4;
+      const __half2* src = H + item_base(j);
+      const uint32_t dst = smem_u32(Ss + (size_t)s * L::S);
 #pragma unroll 4
-      for (int t = wl; t < 4 * Q; t += 3) {
-        const int am = t & 3, c = t >> 2;
-        cp_async4(dst0 + 512u * c + 128u * am, src0 + (int64_t)(Q * (4 * am + j4) + c) * hp);
-      }
-      mbar_arrive_cp_async(a1full + s);
+      for (int i = lt; i < 2 * L::N1; i += kYLoaders)
+        cp_async16(dst + 16u * (uint32_t)i, src + (int64_t)(i >> 1) * hp + 4 * (i & 1), 16);
+      mbar_arrive_cp_async(sfull + s);
     }
   } else if (warp == 0) {
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
-      const uint32_t id1 = idesc_f16(128, L::NC1), id2 = idesc_f16(128, L::NC2);
-      const uint32_t t1 = smem_u32(T1s), t2 = smem_u32(T2s);
-      const uint32_t a1 = smem_u32(A1s), a2 = smem_u32(A2s);
-      bool ok = true;
-      for (int64_t j = 0; j <= mine && ok; ++j) {
-        if (j < mine) {
-          // stage 1 of item j into D1[j & 1]
-          const int s = (int)(j % kYS1), p = (int)(j & 1);
-          const uint32_t u = (uint32_t)(j / kYS1);
-          if (!mbar_wait_n(smem_u32(a1full + s), u & 1u, wait_iters)) { ok = false; break; }
-          if (j >= 2 &&
-              !mbar_wait_n(smem_u32(e1done + p), (uint32_t)((j - 2) >> 1) & 1u, wait_iters)) {
-            ok = false;
-            break;
-          }
-          if (*fail) { ok = false; break; }
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          asm volatile("tcgen05.fence::after_thread_sync;");
-          const uint32_t ab = a1 + (uint32_t)s * (uint32_t)L::A1 * 2u;
-#pragma unroll
-          for (int m = 0; m < L::NT1; ++m)
-#pragma unroll
-            for (int st = 0; st < L::K1 / 16; ++st)
-              mma_f16(tmem + (uint32_t)(p * 128 + m * 64),
-                      smem_desc(ab + (uint32_t)(m * 128 * L::K1 * 2 + st * 256), 128u,
-                                (uint32_t)L::K1 * 16u),
-                      smem_desc(t1 + (uint32_t)(st * 256), 128u, (uint32_t)L::K1 * 16u), id1,
-                      st > 0);
-          mma_commit(smem_u32(a1empty + s));
-          mma_commit(smem_u32(d1full + p));
+      const uint32_t id2 = idesc_f16(128, L::NC2);
+      const uint32_t t2 = smem_u32(T2s), a2 = smem_u32(A2s);
+      bool ok = mbar_wait_n(smem_u32(tfull), 0u, wait_iters);
+      for (int64_t j = 0; j < mine && ok; ++j) {
+        const int p = (int)(j & 1);
+        if (!mbar_wait_n(smem_u32(e1done + p), (uint32_t)(j >> 1) & 1u, wait_iters)) {
+          ok = false;
+          break;
         }
-        if (j >= 1) {
-          // stage 2 of item j - 1 into D2[(j - 1) & 1]
-          const int64_t jj = j - 1;
-          const int p = (int)(jj & 1);
-          if (!mbar_wait_n(smem_u32(e1done + p), (uint32_t)(jj >> 1) & 1u, wait_iters)) {
-            ok = false;
-            break;
-          }
-          if (jj >= 2 &&
-              !mbar_wait_n(smem_u32(d2empty + p), (uint32_t)((jj - 2) >> 1) & 1u, wait_iters)) {
-            ok = false;
-            break;
-          }
-          if (*fail) { ok = false; break; }
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          asm volatile("tcgen05.fence::after_thread_sync;");
-          const uint32_t ab = a2 + (uint32_t)p * (uint32_t)L::A2 * 2u;
-#pragma unroll
-          for (int st = 0; st < L::K2 / 16; ++st)
-            mma_f16(tmem + 256u + (uint32_t)(p * 128),
-                    smem_desc(ab + (uint32_t)(st * 256), 128u, (uint32_t)L::K2 * 16u),
-                    smem_desc(t2 + (uint32_t)(st * 256), 128u, (uint32_t)L::K2 * 16u), id2,
-                    st > 0);
-          mma_commit(smem_u32(s2done + p));
+        if (j >= 2 &&
+            !mbar_wait_n(smem_u32(d2empty + p), (uint32_t)((j - 2) >> 1) & 1u, wait_iters)) {
+          ok = false;
+          break;
         }
+        if (*fail) { ok = false; break; }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t ab = a2 + (uint32_t)p * (uint32_t)L::A2 * 2u;
+#pragma unroll
+        for (int st = 0; st < L::K2 / 16; ++st)
+          mma_f16(tmem + (uint32_t)(p * 128),
+                  smem_desc(ab + (uint32_t)(st * 256), 128u, (uint32_t)L::K2 * 16u),
+                  smem_desc(t2 + (uint32_t)(st * 256), 128u, (uint32_t)L::K2 * 16u), id2,
+                  st > 0);
+        mma_commit(smem_u32(s2done + p));
       }
       if (!ok) *fail = 1;
       // nothing may free tensor memory or shared memory under a running MMA: this wait
@@ -277,59 +228,82 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
       mma_commit(smem_u32(mdone));
       if (!mbar_wait(smem_u32(mdone), 0u)) *fail = 1;
     }
-  } else if (warp < 4 + 4 * L::NT1) {
-    // ---------------------------------------------------------------- stage-1 epilogue
-    const int m = (warp - 4) >> 2, q = warp & 3;
-    const int c = 16 * m + 4 * q + (lane >> 3), k2 = lane & 7;
-    float wr[16], wi[16];
+  } else if (warp < 4 + L::EPI1 / 32) {
+    // ---------------------------------------------------------------- stage 1
+    const int t = tid - 128;
+    const int c = t >> 3, k2 = t & 7;
+    // twiddles w^(c y1) of the column and w16^k, k <= 9, of the radix-16 FFT
+    float wr[16], wi[16], tr16[10], ti16[10];
 #pragma unroll
-    for (int y1 = 0; y1 < 16; ++y1) sincospif(2.0f * (float)(c * y1) / (float)L::N1, &wi[y1], &wr[y1]);
-    const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(m * 64);
-    // row (y1, k2), K position 2c of the stage-2 operand: byte
-    // y1 * 32Q + 128 (c >> 2) + 16 k2 + 4 (c & 3)
+    for (int y1 = 0; y1 < 16; ++y1)
+      sincospif(2.0f * (float)(c * y1) / (float)L::N1, &wi[y1], &wr[y1]);
+#pragma unroll
+    for (int k = 0; k < 10; ++k) sincospif((float)k / 8.0f, &ti16[k], &tr16[k]);
+    // staging: X[k1][k2] at byte 32 k1 + 4 k2 (banks 8c + k2: conflict-free per warp);
+    // operand: row (y1, k2), K position 2c (head) at byte
+    // y1 * 64Q + 128 (c >> 2) + 16 k2 + 4 (c & 3), the tail 32Q bytes further
+    const uint32_t src0 = 32u * (uint32_t)c + 4u * (uint32_t)k2;
     const uint32_t a2t = smem_u32(A2s) + 128u * (uint32_t)(c >> 2) + 16u * (uint32_t)k2 +
                          4u * (uint32_t)(c & 3);
     for (int64_t j = 0; j < mine; ++j) {
-      const int p = (int)(j & 1);
-      const uint32_t u = (uint32_t)(j >> 1);
-      bool got = mbar_wait_n(smem_u32(d1full + p), u & 1u, wait_iters);
-      if (got && j >= 2) got = mbar_wait_n(smem_u32(s2done + p), (u - 1) & 1u, wait_iters);
-      __syncwarp();
-      if (!__all_sync(0xffffffffu, got)) { *fail = 1; break; }
-      if (__any_sync(0xffffffffu, *fail)) break;
-      asm volatile("tcgen05.fence::after_thread_sync;");
-      float re[16], im[16];
-      {
-        float hr[16], hi[16];
-        tmem_ld16(tl + (uint32_t)(p * 128), hr);
-        tmem_ld16(tl + (uint32_t)(p * 128 + 32), re);
-        tmem_ld16(tl + (uint32_t)(p * 128 + 16), hi);
-        tmem_ld16(tl + (uint32_t)(p * 128 + 48), im);
-        asm volatile("tcgen05.wait::ld.sync.aligned;");
+      const int s = (int)(j % kYS), p = (int)(j & 1);
+      if (!mbar_wait_n(smem_u32(sfull + s), (uint32_t)(j / kYS) & 1u, wait_iters)) {
+        *fail = 1;
+        break;
+      }
+      if (*fail) break;
+      float2 x[16];
+      const uint32_t sb = smem_u32(Ss + (size_t)s * L::S) + src0;
 #pragma unroll
-        for (int y1 = 0; y1 < 16; ++y1) {
-          re[y1] += hr[y1];
-          im[y1] += hi[y1];
+      for (int a = 0; a < 16; ++a) {
+        uint32_t w;
+        asm volatile("ld.shared.b32 %0, [%1];" : "=r"(w) : "r"(sb + (uint32_t)(a * 32 * Q)));
+        x[a] = __half22float2(*reinterpret_cast<const __half2*>(&w));
+      }
+      mbar_arrive(sempty + s);
+      // radix 16 = 4 x 4: DFT4 over a1 (a = 4 a1 + a0), twiddle w16^(a0 y0), DFT4 over a0;
+      // Z[y0 + 4 y1] ends in v[y0][y1]
+      float2 v[4][4];
+#pragma unroll
+      for (int a0 = 0; a0 < 4; ++a0) {
+        float2 u[4] = {x[a0], x[a0 + 4], x[a0 + 8], x[a0 + 12]};
+        fft::dft4<1>(u);
+#pragma unroll
+        for (int y0 = 0; y0 < 4; ++y0) {
+          const int k = a0 * y0;
+          v[y0][a0] = k == 0 ? u[y0] : fft::cmul(u[y0], make_float2(tr16[k], ti16[k]));
         }
+      }
+#pragma unroll
+      for (int y0 = 0; y0 < 4; ++y0) fft::dft4<1>(v[y0]);
+      if (j >= 2 && !mbar_wait_n(smem_u32(s2done + p), (uint32_t)((j - 2) >> 1) & 1u,
+                                 wait_iters)) {
+        *fail = 1;
+        break;
       }
       const uint32_t dst = a2t + (uint32_t)p * (uint32_t)L::A2 * 2u;
 #pragma unroll
       for (int y1 = 0; y1 < 16; ++y1) {
-        const float orr = re[y1] * wr[y1] - im[y1] * wi[y1];
-        const float oi = re[y1] * wi[y1] + im[y1] * wr[y1];
-        asm volatile("st.shared.b32 [%0], %1;" ::"r"(dst + (uint32_t)(y1 * 32 * Q)),
-                     "r"(pack_half2(orr, oi))
+        const float2 z = v[y1 & 3][y1 >> 2];
+        const float orr = z.x * wr[y1] - z.y * wi[y1];
+        const float oi = z.x * wi[y1] + z.y * wr[y1];
+        const __half2 hd = __floats2half2_rn(orr, oi);
+        const float2 hf = __half22float2(hd);
+        const uint32_t head = *reinterpret_cast<const uint32_t*>(&hd);
+        asm volatile("st.shared.b32 [%0], %1;" ::"r"(dst + (uint32_t)(y1 * 64 * Q)), "r"(head)
+                     : "memory");
+        asm volatile("st.shared.b32 [%0], %1;" ::"r"(dst + (uint32_t)(y1 * 64 * Q + 32 * Q)),
+                     "r"(pack_half2(orr - hf.x, oi - hf.y))
                      : "memory");
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;");
       mbar_arrive(e1done + p);
     }
   } else if (warp >= 12) {
     // ---------------------------------------------------------------- stage-2 epilogue
     const int q = warp & 3;
     const int y1 = 4 * q + (lane >> 3), k2 = lane & 7;
-    const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16) + 256u;
+    const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16);
     // segment layout: word k2 of a row's 32-byte segment is (Re, Re) of columns 2k2, 2k2+1
     // for k2 < 4 and (Im, Im) of columns 2(k2-4), 2(k2-4)+1 otherwise, gathered from the
     // lanes of the same row
@@ -378,7 +352,7 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
   asm volatile("tcgen05.fence::after_thread_sync;");
   if (warp == 0) {
     __syncwarp();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(tmem), "r"(512));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(tmem), "r"(256));
   }
   if (tid == 0 && *fail) atomicExch(err, 1);
 }
@@ -411,7 +385,7 @@ int ypass_tc_config(int n1, int hp, YpassTcConfig* cfg) {
 }
 
 size_t ypass_tc_table_bytes(const YpassTcConfig& cfg) {
-  return (size_t)(t1_halves() + t2_halves(cfg.Q)) * 2;
+  return (size_t)t2_halves(cfg.Q) * 2;
 }
 
 int ypass_tc_prepare(const YpassTcConfig& cfg, uint16_t* table, cudaStream_t stream) {

@@ -111,7 +111,10 @@ def test_tme_scan_subsets_flcsm(tme_b200, golden, run_counter, precision):
                                 score_threshold=-np.inf, probe=mism)["probe"]
         best = g["scores64"][tuple(mism.T)]
         for j, (v, p) in enumerate(zip(mism, rot[tuple(mism.T)])):
-            assert p >= 0 and best[j] - probe[p, j] <= 2 * TOL, (v, p)
+            if p < 0:  # no rotation above the zero threshold here: the best is a tie with it
+                assert best[j] <= 2 * TOL, (v, best[j])
+            else:
+                assert best[j] - probe[p, j] <= 2 * TOL, (v, p)
     # tme's result() inverts the mapping: index -> the rotation matrix scored under it
     rmap = res[3]
     assert len(rmap) == n
