@@ -8,7 +8,27 @@ is imported, under a subclass that constructs it on the current CUDA device what
 device the suite names (the B200 backend has no CPU mode), and keeps only the tests
 parametrised with it. Loaded with ``-p ref_backend_suite`` by
 tests/test_gpu_tme_dropin.py.
+
+A few of the suite's checks hand backend arrays straight to NumPy (``np.allclose(arr,
+arr_b)`` in test_rigid_transform_batch), which works for the reference's backends because
+the suite builds them on the CPU. The B200 backend's arrays are CUDA tensors, which
+``torch.Tensor.__array__`` refuses to convert; in the suite's own process (and only there)
+the conversion copies a CUDA tensor to the host first, so those checks compare values as
+they do for the reference's backends.
 """
+
+
+def _host_array_conversion():
+    import torch
+
+    orig = torch.Tensor.__array__
+
+    def __array__(self, dtype=None):
+        if self.is_cuda:
+            self = self.detach().cpu()
+        return orig(self, dtype)
+
+    torch.Tensor.__array__ = __array__
 
 
 def pytest_configure(config):
@@ -16,6 +36,7 @@ def pytest_configure(config):
 
     from pytme_b200.tme_plugin import register
 
+    _host_array_conversion()
     register(strict=True)
     base = tme_be._BACKEND_REGISTRY["b200"]
 

@@ -87,19 +87,38 @@ def _check_ties(score, target, tmpl, mask, rots, gpu_rot, ref64, workers, tf=Non
     return len(mism)
 
 
+def _window_max(score, p, size):
+    """Maximum of the maximum filter's box around ``p`` (SciPy's box of an even ``size``
+    covers offsets -size/2 .. size/2 - 1; outside the map counts as 0, mode "constant")."""
+    lo = [max(0, int(x) - size // 2) for x in p]
+    hi = [min(n, int(x) - size // 2 + size) for x, n in zip(p, score.shape)]
+    box = score[tuple(slice(a, b) for a, b in zip(lo, hi))]
+    full = all(int(x) - size // 2 >= 0 and int(x) - size // 2 + size <= n
+               for x, n in zip(p, score.shape))
+    return float(box.max()) if full else max(float(box.max()), 0.0)
+
+
 def _explained(diff, other, score_a, score_b, cutoff, min_distance):
-    """Peaks present in one set only: each sits within 2e-4 of the score cutoff (rank at
-    the boundary) or within the minimum distance of another such peak (a greedy choice
-    between near-equal neighbours, and what it cascades into)."""
+    """Peaks present in one set only. Each must be explained by a near-tie (within 2e-4,
+    twice the map's error bound): its score sits at the cutoff (rank at the boundary); or
+    in the map where it is not a local maximum, a neighbour inside the maximum filter's
+    box beats it by no more than that (which voxel is the local maximum is a tie); or it
+    lies within the minimum distance of another differing peak (a greedy choice between
+    near-equal neighbours, and what it cascades into). Returns the unexplained ones with
+    their scores and box maxima in both maps."""
     bad = []
     for p in diff:
-        near_cut = min(abs(score_a[tuple(p)] - cutoff), abs(score_b[tuple(p)] - cutoff)) <= 2 * TOL
-        if near_cut:
+        t = tuple(int(x) for x in p)
+        sa, sb = float(score_a[t]), float(score_b[t])
+        if min(abs(sa - cutoff), abs(sb - cutoff)) <= 2 * TOL:
+            continue
+        wa, wb = _window_max(score_a, t, min_distance), _window_max(score_b, t, min_distance)
+        if (sa >= wa and wb - sb <= 2 * TOL) or (sb >= wb and wa - sa <= 2 * TOL):
             continue
         d = np.sqrt(((other - p) ** 2).sum(1)) if len(other) else np.array([np.inf])
         if np.any((d > 0) & (d <= min_distance + 1)):
             continue
-        bad.append(tuple(int(x) for x in p))
+        bad.append((t, sa, sb, wa, wb))
     return bad
 
 

@@ -554,4 +554,18 @@ def test_tensor_core_ypass(torch_cuda, shape, score):
     assert np.abs(r[0] - ref["scores"]).max() <= tol
     assert np.abs(r[0] - ref64["scores"]).max() <= tol
     assert np.abs(r[0] - f[0]).max() <= tol
-    assert np.count_nonzero(r[2] != ref64["rotations"]) <= max(2, int(1e-3 * r[2].size))
+    # a blob template makes many rotations score alike: every voxel whose rotation differs
+    # from the FP64 oracle's must be a tie within the path's error bound
+    for rot in (r[2], f[2]):
+        mism = np.argwhere(rot != ref64["rotations"])
+        print(f"{shape} {score}: {len(mism)} argmax differences of {rot.size}")
+        assert len(mism) <= 0.02 * rot.size
+        if len(mism) == 0:
+            continue
+        probe = O.scan_parallel(target, tmpl, rots, score, template_mask=mask,
+                                dtype=np.float64, n_workers=4, score_threshold=-np.inf,
+                                probe=mism)["probe"]
+        best = ref64["scores"][tuple(mism.T)]
+        picks = rot[tuple(mism.T)]
+        gaps = np.where(picks < 0, best, best - probe[np.maximum(picks, 0), np.arange(len(mism))])
+        assert gaps.max() <= 2 * tol, float(gaps.max())
