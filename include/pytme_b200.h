@@ -192,8 +192,9 @@ int tm_scan_zpass_mode(const tm_scan* plan);
 /* y pass of the fused CC / FLCSphericalMask scan (the inverse transform along axis 1 of
  * corr_scoring's irfftn, tme/matching_scores.py:618-620): mode 0 runs it on the tensor
  * cores as two FP16 DFT GEMM stages (radix 16, then radix n1/16, twiddles between them;
- * mixed-precision plans with n1 of 256 or 512), mode 1 as CUDA-core FFTs, mode 2 restores
- * the default. TM_E_UNSUPPORTED when mode 0 is not available. */
+ * mixed-precision plans with n1 of 256 or 512; the default where available), mode 1 as
+ * CUDA-core FFTs, mode 2 restores the default. TM_E_UNSUPPORTED when mode 0 is not
+ * available. */
 int tm_scan_set_ypass(tm_scan* plan, int mode);
 int tm_scan_ypass_mode(const tm_scan* plan);
 /* Bound of every data wait inside the plan's tensor-core kernels, in mbarrier polls

@@ -1469,7 +1469,7 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     if (s->ztc_avail) o_zt = take(zpass_tc_table_bytes(s->zcfg));
     TM_TRY(ypass_tc_config(s->n1, s->hp, &s->ycfg));
     s->ytc_avail = s->ycfg.ok;
-    s->ytc = false;  // opt-in through tm_scan_set_ypass
+    s->ytc = s->ytc_avail;
     if (s->ytc_avail) o_yt = take(ypass_tc_table_bytes(s->ycfg));
   }
   if (s->fused && d.score != TM_SCORE_FLC) {
@@ -1737,13 +1737,13 @@ int scan_set_zpass(Scan* s, int mode) {
 int scan_zpass_mode(const Scan* s) { return s && s->ztc ? 0 : 1; }
 
 // y pass on the tensor cores (mode 0: two FP16 GEMM stages, half-precision CC /
-// FLCSphericalMask plans with n1 in {256, 512}) or as FFTs on the CUDA cores (mode 1);
-// mode 2 restores the default.
+// FLCSphericalMask plans with n1 in {256, 512}; the default where available) or as FFTs on
+// the CUDA cores (mode 1); mode 2 restores the default.
 int scan_set_ypass(Scan* s, int mode) {
   TM_REQUIRE(s, "scan_set_ypass: null plan");
   TM_REQUIRE(mode >= 0 && mode <= 2,
              "scan_set_ypass: mode must be 0 (tensor cores), 1 (FFT) or 2 (default)");
-  const bool want = mode == 0;
+  const bool want = mode == 0 || (mode == 2 && s->ytc_avail);
   if (want && !s->ytc_avail) {
     set_error("scan_set_ypass: the tensor-core y pass does not support this plan");
     return TM_E_UNSUPPORTED;

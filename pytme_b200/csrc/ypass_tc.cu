@@ -9,12 +9,10 @@
 //     Y[y1 + 16 y2] = sum_{c < Q} Z'[y1][c] wQ^(c y2)          (radix Q, tensor cores)
 // The radix-16 stage is a 4 x 4 register FFT in FP32 per (c, k2) column; the radix-Q stage
 // is a real GEMM over interleaved (Re, Im) K positions: rows (y1, k2) of Z' are the M
-// operand, a fixed DFT operator the N operand, with output columns [Re | Im] of the
-// operator's FP16 head and then of its FP16 rounded remainder (the tail), so one MMA pass
-// gives both products and the epilogue adds them (about 22 significant bits). Z' enters
-// the GEMM as an FP16 head plus its FP16 rounded remainder (two K blocks against the same
-// operator), so the only rounding of the pass is that of its FP16 output, as in the FFT y
-// pass.
+// operand, a fixed DFT operator the N operand (output columns [Re | Im]). Both enter as an
+// FP16 head plus its FP16 rounded remainder (the tail), and three MMAs per K step
+// accumulate Zh Th + Zt Th + Zh Tt in one FP32 accumulator (about 22 significant bits),
+// so the only rounding of the pass is that of its FP16 output, as in the FFT y pass.
 //
 // A work item is one rotation, one x' plane and 8 consecutive k2 columns: n1 rows of
 // 32 bytes (one sector each), read and written in place. Roles of the persistent
@@ -25,9 +23,10 @@
 //   warps 4-11     stage 1: one thread per (c, k2) column reads its 16 values from the
 //                  staging buffer (bank-conflict-free), runs the radix-16 FFT and the
 //                  twiddle, and writes Z' (head and tail) into the stage-2 operand;
-//   warps 12-15    stage-2 epilogue: tensor memory -> head + tail -> FP16 -> H, either as
-//                  interleaved complex values or, for the tensor-core z pass, as 32-byte
-//                  segments [Re x 8 | Im x 8] per row and item (full-sector stores both).
+//   warps 12-15    stage-2 epilogue: tensor memory -> FP16 -> a staging buffer holding
+//                  the item's rows, either as interleaved complex values or, for the
+//                  tensor-core z pass, as 32-byte segments [Re x 8 | Im x 8] -> H with
+//                  16-byte stores of whole rows.
 // mbarriers hand every buffer between the roles; every wait is bounded by the plan's
 // wait budget, and a wait that runs out sets the error flag, after which all roles
 // leave, the MMAs in flight are waited for and the tensor memory is freed.
@@ -50,17 +49,18 @@ constexpr int kYThreads = 512;
 constexpr int kYS = 4;          // staging buffers (items whose loads are in flight)
 constexpr int kYLoaders = 96;   // warps 1-3
 
-// Stage-2 operator, canonical K-major FP16: 4Q rows [Re Y | Im Y] x Q outputs (head rows,
-// then tail rows) by 4Q K positions: 2c + (0: Re Z', 1: Im Z') for the FP16 head of Z',
-// and again from K = 2Q for its FP16 rounded remainder.
-__host__ __device__ constexpr int t2_halves(int Q) { return 4 * Q * 4 * Q; }
+// Stage-2 operator, canonical K-major FP16, two tables (the FP16 head, then the FP16
+// rounded remainder) of 2Q rows [Re Y | Im Y] x Q outputs by 2Q K positions
+// 2c + (0: Re Z', 1: Im Z').
+__host__ __device__ constexpr int t2_halves(int Q) { return 2 * (2 * Q) * (2 * Q); }
 
 __global__ void ydft_table_kernel(uint16_t* __restrict__ T, int Q) {
-  const int K = 4 * Q, total = t2_halves(Q);
+  const int K = 2 * Q, total = t2_halves(Q);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-    const int n = i / K, k = i - n * K;
-    const int part = n / (2 * Q), comp = (n / Q) & 1, o = n % Q;
-    const int c = (k % (2 * Q)) >> 1, ri = k & 1;
+    const int part = i / (K * K), e = i - part * K * K;
+    const int n = e / K, k = e - n * K;
+    const int comp = n / Q, o = n % Q;
+    const int c = k >> 1, ri = k & 1;
     double sn, cs;
     sincospi(2.0 * (double)((c * o) % Q) / (double)Q, &sn, &cs);
     // (Re, Im) of Z' wQ^(c o): Re = Re Z' cos - Im Z' sin, Im = Re Z' sin + Im Z' cos
@@ -68,7 +68,7 @@ __global__ void ydft_table_kernel(uint16_t* __restrict__ T, int Q) {
     const float vf = (float)v;
     const __half hd = __float2half_rn(vf);
     const __half tl = __float2half_rn(vf - __half2float(hd));
-    T[kmajor16(part * 2 * Q + comp * Q + o, k, K)] = __half_as_ushort(part == 0 ? hd : tl);
+    T[part * K * K + kmajor16(n, k, K)] = __half_as_ushort(part == 0 ? hd : tl);
   }
 }
 
@@ -104,16 +104,36 @@ __device__ __forceinline__ uint32_t pack_half2(float re, float im) {
 template <int Q>
 struct YLayout {
   static constexpr int N1 = 16 * Q;        // transform length
-  static constexpr int K2 = 4 * Q;         // stage-2 K: Q complex inputs, Z' head and tail
-  static constexpr int NC2 = 4 * Q;        // stage-2 N: [Re | Im] x Q, head then tail
+  static constexpr int K2 = 4 * Q;         // stage-2 operand K: Z' head (2Q), Z' tail (2Q)
+  static constexpr int KT = 2 * Q;         // operator K: Q complex inputs
+  static constexpr int NC2 = 2 * Q;        // stage-2 N: [Re | Im] x Q
   static constexpr int S = N1 * 16;        // halves per staging buffer (n1 rows of 32 B)
   static constexpr int A2 = 128 * K2;      // halves per stage-2 operand buffer
   static constexpr int EPI1 = 8 * Q;       // stage-1 threads: one per (c, k2)
   static constexpr int EPI2 = 128;
   static constexpr size_t smem_bytes() {
-    return (size_t)(t2_halves(Q) + kYS * S + 2 * A2) * 2 + (size_t)(2 * kYS + 8) * 8 + 16;
+    return (size_t)(t2_halves(Q) + kYS * S + 2 * A2 + 2 * S) * 2 + (size_t)(2 * kYS + 8) * 8 +
+           16;
   }
 };
+
+// barrier of the 128 stage-2 epilogue threads (warps 12-15) that returns the OR of `pred`
+// over them, so all four warps take the same branch after it
+__device__ __forceinline__ bool epi_any(bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)pred)
+      : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ void epi_sync() {
+  asm volatile("bar.sync 2, 128;" ::: "memory");
+}
 
 template <int Q>
 __global__ void __launch_bounds__(kYThreads, 1)
@@ -125,7 +145,8 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
   uint16_t* T2s = smem_y;
   uint16_t* Ss = T2s + t2_halves(Q);                // kYS staging buffers
   uint16_t* A2s = Ss + kYS * L::S;                  // 2 stage-2 operand buffers
-  uint64_t* bar = reinterpret_cast<uint64_t*>(A2s + 2 * L::A2);
+  uint16_t* Es = A2s + 2 * L::A2;                   // 2 output staging buffers
+  uint64_t* bar = reinterpret_cast<uint64_t*>(Es + 2 * L::S);
   uint64_t* sfull = bar;               // [kYS] item staged (loader threads, async)
   uint64_t* sempty = bar + kYS;        // [kYS] stage 1 read the item (stage-1 threads)
   uint64_t* e1done = bar + 2 * kYS;    // [2] stage 1 wrote the operand (stage-1 threads)
@@ -140,7 +161,7 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  :
-                 : "r"(smem_u32(tmem_slot)), "r"(256));
+                 : "r"(smem_u32(tmem_slot)), "r"(128));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
@@ -162,7 +183,7 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tmem_slot;
-  // tensor memory: D2 (stage-2 accumulators) in two buffers of 128 columns
+  // tensor memory: D2 (stage-2 accumulators) in two buffers of 64 columns
   const int64_t mine = nitems > blockIdx.x ? (nitems - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const int nc = hp / 8;  // items per (rotation, x') plane
   auto item_base = [&](int64_t j) -> int64_t {
@@ -214,12 +235,20 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::after_thread_sync;");
         const uint32_t ab = a2 + (uint32_t)p * (uint32_t)L::A2 * 2u;
+        const uint32_t dt = tmem + (uint32_t)(p * L::NC2);
+        // D = Zh Th + Zt Th + Zh Tt, K step by K step (16 positions, 256 bytes)
 #pragma unroll
-        for (int st = 0; st < L::K2 / 16; ++st)
-          mma_f16(tmem + (uint32_t)(p * 128),
-                  smem_desc(ab + (uint32_t)(st * 256), 128u, (uint32_t)L::K2 * 16u),
-                  smem_desc(t2 + (uint32_t)(st * 256), 128u, (uint32_t)L::K2 * 16u), id2,
-                  st > 0);
+        for (int st = 0; st < L::KT / 16; ++st) {
+          const uint64_t zh = smem_desc(ab + (uint32_t)(st * 256), 128u, (uint32_t)L::K2 * 16u);
+          const uint64_t zt = smem_desc(ab + (uint32_t)((L::KT / 16 + st) * 256), 128u,
+                                        (uint32_t)L::K2 * 16u);
+          const uint64_t th = smem_desc(t2 + (uint32_t)(st * 256), 128u, (uint32_t)L::KT * 16u);
+          const uint64_t tt = smem_desc(t2 + (uint32_t)(L::KT * L::KT * 2 + st * 256), 128u,
+                                        (uint32_t)L::KT * 16u);
+          mma_f16(dt, zh, th, id2, st > 0);
+          mma_f16(dt, zt, th, id2, 1);
+          mma_f16(dt, zh, tt, id2, 1);
+        }
         mma_commit(smem_u32(s2done + p));
       }
       if (!ok) *fail = 1;
@@ -301,32 +330,31 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
     }
   } else if (warp >= 12) {
     // ---------------------------------------------------------------- stage-2 epilogue
-    const int q = warp & 3;
+    // tensor memory -> FP16 -> output staging (row y' of 32 bytes, interleaved complex or
+    // the segment [Re x 8 | Im x 8]) -> 16-byte stores of whole rows
+    const int q = warp & 3, te = tid - 384;
     const int y1 = 4 * q + (lane >> 3), k2 = lane & 7;
     const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16);
-    // segment layout: word k2 of a row's 32-byte segment is (Re, Re) of columns 2k2, 2k2+1
-    // for k2 < 4 and (Im, Im) of columns 2(k2-4), 2(k2-4)+1 otherwise, gathered from the
-    // lanes of the same row
-    const int srcA = (lane & ~7) | ((2 * k2) & 7);
-    const uint32_t sel = k2 < 4 ? 0x5410u : 0x7632u;
     for (int64_t j = 0; j < mine; ++j) {
       const int p = (int)(j & 1);
       const uint32_t u = (uint32_t)(j >> 1);
       const bool got = mbar_wait_n(smem_u32(s2done + p), u & 1u, wait_iters);
-      __syncwarp();
-      if (!__all_sync(0xffffffffu, got)) { *fail = 1; break; }
-      if (__any_sync(0xffffffffu, *fail)) break;
+      // one decision for all four warps (and the barrier that frees staging buffer p:
+      // every epilogue thread finished item j - 1, so item j - 2's reads are done)
+      if (epi_any(!got || *fail)) {
+        *fail = 1;
+        break;
+      }
+      __syncwarp();  // tcgen05.ld needs the whole warp, converged
       asm volatile("tcgen05.fence::after_thread_sync;");
-      __half2* dst = H + item_base(j) + k2 + (int64_t)y1 * hp;
-      const uint32_t tb = tl + (uint32_t)(p * 128);
-      // D2 columns [Re head | Im head | Re tail | Im tail], Q each
+      const uint32_t tb = tl + (uint32_t)(p * L::NC2);
+      const uint32_t es = smem_u32(Es + (size_t)p * L::S);
+      // D2 columns [Re | Im], Q each: output y' = y1 + 16 y2
 #pragma unroll
       for (int g = 0; g < Q / 16; ++g) {
-        float re[16], im[16], tr[16], ti[16];
+        float re[16], im[16];
         tmem_ld16(tb + (uint32_t)(g * 16), re);
         tmem_ld16(tb + (uint32_t)(Q + g * 16), im);
-        tmem_ld16(tb + (uint32_t)(2 * Q + g * 16), tr);
-        tmem_ld16(tb + (uint32_t)(3 * Q + g * 16), ti);
         asm volatile("tcgen05.wait::ld.sync.aligned;");
         if (g == Q / 16 - 1) {
           asm volatile("tcgen05.fence::before_thread_sync;");
@@ -334,15 +362,30 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
         }
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
-          const int y2 = g * 16 + i;
-          uint32_t v = pack_half2(re[i] + tr[i], im[i] + ti[i]);
+          const uint32_t row = es + 32u * (uint32_t)(y1 + 16 * (g * 16 + i));
+          const uint32_t v = pack_half2(re[i], im[i]);
           if (seg) {
-            const uint32_t a = __shfl_sync(0xffffffffu, v, srcA);
-            const uint32_t b = __shfl_sync(0xffffffffu, v, srcA + 1);
-            v = __byte_perm(a, b, sel);
+            asm volatile("st.shared.b16 [%0], %1;" ::"r"(row + 2u * k2), "h"((uint16_t)(v & 0xffffu))
+                         : "memory");
+            asm volatile("st.shared.b16 [%0], %1;" ::"r"(row + 16u + 2u * k2), "h"((uint16_t)(v >> 16))
+                         : "memory");
+          } else {
+            asm volatile("st.shared.b32 [%0], %1;" ::"r"(row + 4u * k2), "r"(v) : "memory");
           }
-          *reinterpret_cast<uint32_t*>(dst + (int64_t)(16 * y2) * hp) = v;
         }
+      }
+      epi_sync();
+      // 16-byte piece i: row i >> 1, half i & 1
+      __half2* dst = H + item_base(j);
+#pragma unroll
+      for (int m = 0; m < 2 * L::N1 / L::EPI2; ++m) {
+        const int i = te + L::EPI2 * m;
+        uint32_t a, b, c, d;
+        asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
+                     : "=r"(a), "=r"(b), "=r"(c), "=r"(d)
+                     : "r"(es + 16u * (uint32_t)i));
+        uint4* g = reinterpret_cast<uint4*>(dst + (int64_t)(i >> 1) * hp + 4 * (i & 1));
+        *g = make_uint4(a, b, c, d);
       }
     }
   }
@@ -352,7 +395,7 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
   asm volatile("tcgen05.fence::after_thread_sync;");
   if (warp == 0) {
     __syncwarp();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(tmem), "r"(256));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(tmem), "r"(128));
   }
   if (tid == 0 && *fail) atomicExch(err, 1);
 }
