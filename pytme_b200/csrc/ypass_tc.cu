@@ -15,26 +15,31 @@
 // so the only rounding of the pass is that of its FP16 output, as in the FFT y pass.
 //
 // A work item is one rotation, one x' plane and 8 consecutive k2 columns: n1 rows of
-// 32 bytes (one sector each), read and written in place. Roles of the persistent
-// 512-thread CTA:
+// 32 bytes, read and written in place. The rows of an item move between H and shared
+// memory as tiles of the tensor memory accelerator (TMA): H is a 2D tensor of 4-byte
+// words (hp columns, nb n0 n1 rows) and an item is n1 / 256 boxes of 8 x 256 words, so
+// no thread issues per-row loads or stores. Roles of the persistent 512-thread CTA:
 //   warp 0         one thread issues the stage-2 MMAs;
-//   warps 1-3      copy items row by row into a dense staging buffer with 16-byte
-//                  cp.async (kYS items in flight), and the operator once;
+//   warp 1         one thread issues the TMA loads of the items (kYS in flight) and the
+//                  bulk copy of the operator;
+//   warp 2         one thread issues the TMA stores of the finished items;
 //   warps 4-11     stage 1: one thread per (c, k2) column reads its 16 values from the
 //                  staging buffer (bank-conflict-free), runs the radix-16 FFT and the
 //                  twiddle, and writes Z' (head and tail) into the stage-2 operand;
-//   warps 12-15    stage-2 epilogue: tensor memory -> FP16 -> a staging buffer holding
-//                  the item's rows, either as interleaved complex values or, for the
-//                  tensor-core z pass, as 32-byte segments [Re x 8 | Im x 8] -> H with
-//                  16-byte stores of whole rows.
+//   warps 12-15    stage-2 epilogue: tensor memory -> FP16 -> an output staging buffer
+//                  holding the item's rows, either as interleaved complex values or, for
+//                  the tensor-core z pass, as 32-byte segments [Re x 8 | Im x 8].
 // mbarriers hand every buffer between the roles; every wait is bounded by the plan's
 // wait budget, and a wait that runs out sets the error flag, after which all roles
-// leave, the MMAs in flight are waited for and the tensor memory is freed.
+// leave, the copies and MMAs in flight are waited for and the tensor memory is freed.
+// No load here uses cluster multicast.
 #include "common.cuh"
 #include "fft_smem.cuh"
 #include "tc_common.cuh"
 #include "ypass_tc.cuh"
 
+#include <cuda.h>  // CUtensorMap and the encoder's types; the encoder itself is reached
+                   // through cudaGetDriverEntryPointByVersion
 #include <cuda_fp16.h>
 
 #include <algorithm>
@@ -46,8 +51,8 @@ namespace {
 using namespace tc;
 
 constexpr int kYThreads = 512;
-constexpr int kYS = 4;          // staging buffers (items whose loads are in flight)
-constexpr int kYLoaders = 96;   // warps 1-3
+constexpr int kYS = 4;          // input staging buffers (items whose loads are in flight)
+constexpr int kBoxRows = 256;   // rows per TMA box (the box-dimension limit)
 
 // Stage-2 operator, canonical K-major FP16, two tables (the FP16 head, then the FP16
 // rounded remainder) of 2Q rows [Re Y | Im Y] x Q outputs by 2Q K positions
@@ -78,11 +83,39 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(smem_u32(bar)) : "memory");
 }
-// arrival once this thread's earlier cp.async copies have landed (counted in the
-// barrier's expected arrivals)
-__device__ __forceinline__ void mbar_arrive_cp_async(uint64_t* bar) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" : : "r"(smem_u32(bar))
+// one arrival that also announces `bytes` of asynchronous copies completing on the barrier
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+               :
+               : "r"(smem_u32(bar)), "r"(bytes)
                : "memory");
+}
+// TMA load of one 8 x 256-word box at (x, y) of the tensor into shared memory
+__device__ __forceinline__ void tma_load_box(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                             uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];"
+      :
+      : "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+// TMA store of one box from shared memory to (x, y) of the tensor
+__device__ __forceinline__ void tma_store_box(const CUtensorMap* map, int x, int y,
+                                              uint32_t src) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"
+               :
+               : "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(src)
+               : "memory");
+}
+// contiguous bulk copy global -> shared (bytes a multiple of 16, both addresses aligned)
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :
+      : "r"(dst), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
 }
 __device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
   uint32_t r[16];
@@ -107,52 +140,40 @@ struct YLayout {
   static constexpr int K2 = 4 * Q;         // stage-2 operand K: Z' head (2Q), Z' tail (2Q)
   static constexpr int KT = 2 * Q;         // operator K: Q complex inputs
   static constexpr int NC2 = 2 * Q;        // stage-2 N: [Re | Im] x Q
-  static constexpr int S = N1 * 16;        // halves per staging buffer (n1 rows of 32 B)
+  static constexpr int S = N1 * 16;        // halves per item buffer (n1 rows of 32 B)
   static constexpr int A2 = 128 * K2;      // halves per stage-2 operand buffer
   static constexpr int EPI1 = 8 * Q;       // stage-1 threads: one per (c, k2)
   static constexpr int EPI2 = 128;
+  static constexpr int NBOX = N1 / kBoxRows;  // TMA boxes per item
+  static constexpr uint32_t ITEM_BYTES = (uint32_t)N1 * 32u;
+  static constexpr int NBAR = 2 * kYS + 10 + 2;
   static constexpr size_t smem_bytes() {
-    return (size_t)(t2_halves(Q) + kYS * S + 2 * A2 + 2 * S) * 2 + (size_t)(2 * kYS + 8) * 8 +
-           16;
+    return (size_t)(t2_halves(Q) + kYS * S + 2 * A2 + 2 * S) * 2 + (size_t)NBAR * 8 + 16;
   }
 };
-
-// barrier of the 128 stage-2 epilogue threads (warps 12-15) that returns the OR of `pred`
-// over them, so all four warps take the same branch after it
-__device__ __forceinline__ bool epi_any(bool pred) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.u32 p, %1, 0;\n\t"
-      "bar.red.or.pred q, 1, 128, p;\n\t"
-      "selp.u32 %0, 1, 0, q;\n\t}\n"
-      : "=r"(r)
-      : "r"((uint32_t)pred)
-      : "memory");
-  return r != 0;
-}
-__device__ __forceinline__ void epi_sync() {
-  asm volatile("bar.sync 2, 128;" ::: "memory");
-}
+static_assert(YLayout<16>::N1 % kBoxRows == 0 && YLayout<32>::N1 % kBoxRows == 0,
+              "items are whole TMA boxes");
 
 template <int Q>
 __global__ void __launch_bounds__(kYThreads, 1)
-ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
+ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc,
                 const uint16_t* __restrict__ Tg, uint32_t wait_iters, int* __restrict__ err,
                 int seg) {
   using L = YLayout<Q>;
-  extern __shared__ __align__(128) uint16_t smem_y[];
+  extern __shared__ __align__(1024) uint16_t smem_y[];
   uint16_t* T2s = smem_y;
-  uint16_t* Ss = T2s + t2_halves(Q);                // kYS staging buffers
+  uint16_t* Ss = T2s + t2_halves(Q);                // kYS input staging buffers
   uint16_t* A2s = Ss + kYS * L::S;                  // 2 stage-2 operand buffers
   uint16_t* Es = A2s + 2 * L::A2;                   // 2 output staging buffers
   uint64_t* bar = reinterpret_cast<uint64_t*>(Es + 2 * L::S);
-  uint64_t* sfull = bar;               // [kYS] item staged (loader threads, async)
+  uint64_t* sfull = bar;               // [kYS] item landed (loader arrival + TMA bytes)
   uint64_t* sempty = bar + kYS;        // [kYS] stage 1 read the item (stage-1 threads)
   uint64_t* e1done = bar + 2 * kYS;    // [2] stage 1 wrote the operand (stage-1 threads)
   uint64_t* s2done = e1done + 2;       // [2] stage-2 MMAs done: operand free, D2 written
   uint64_t* d2empty = s2done + 2;      // [2] stage-2 epilogue read D2
-  uint64_t* tfull = d2empty + 2;       // the operator landed (loader threads, async)
+  uint64_t* estaged = d2empty + 2;     // [2] output rows staged (epilogue threads)
+  uint64_t* efree = estaged + 2;       // [2] TMA stores finished reading the staging
+  uint64_t* tfull = efree + 2;         // the operator landed (loader arrival + bytes)
   uint64_t* mdone = tfull + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mdone + 1);
   volatile int* fail = reinterpret_cast<volatile int*>(tmem_slot + 1);
@@ -166,15 +187,17 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
   }
   if (tid == 0) {
     for (int s = 0; s < kYS; ++s) {
-      mbar_init(sfull + s, kYLoaders);
+      mbar_init(sfull + s, 1);
       mbar_init(sempty + s, L::EPI1);
     }
     for (int p = 0; p < 2; ++p) {
       mbar_init(e1done + p, L::EPI1);
       mbar_init(s2done + p, 1);
       mbar_init(d2empty + p, L::EPI2);
+      mbar_init(estaged + p, L::EPI2);
+      mbar_init(efree + p, 1);
     }
-    mbar_init(tfull, kYLoaders);
+    mbar_init(tfull, 1);
     mbar_init(mdone, 1);
     asm volatile("fence.mbarrier_init.release.cluster;");
     *fail = 0;
@@ -185,34 +208,65 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
   const uint32_t tmem = *tmem_slot;
   // tensor memory: D2 (stage-2 accumulators) in two buffers of 64 columns
   const int64_t mine = nitems > blockIdx.x ? (nitems - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  const int nc = hp / 8;  // items per (rotation, x') plane
-  auto item_base = [&](int64_t j) -> int64_t {
+  // item id -> (tensor row of its first row, tensor column of its first word)
+  auto item_xy = [&](int64_t j, int& x, int& y) {
     const int64_t id = (int64_t)blockIdx.x + j * gridDim.x;
-    return (id / nc) * (int64_t)L::N1 * hp + (id % nc) * 8;
+    x = (int)(id % nc) * 8;
+    y = (int)(id / nc) * L::N1;
   };
 
-  if (warp >= 1 && warp <= 3) {
-    // ---------------------------------------------------------------- loaders
-    const int lt = tid - 32;
-    constexpr int tpieces = t2_halves(Q) / 8;
-    for (int i = lt; i < tpieces; i += kYLoaders)
-      cp_async16(smem_u32(T2s) + 16u * i, Tg + 8 * (size_t)i, 16);
-    mbar_arrive_cp_async(tfull);
-    // 16-byte piece i: row i >> 1, half i & 1 of the row's 32 bytes (dense rows)
-    for (int64_t j = 0; j < mine; ++j) {
-      const int s = (int)(j % kYS);
-      const uint32_t u = (uint32_t)(j / kYS);
-      if (j >= kYS && !mbar_wait_n(smem_u32(sempty + s), (u - 1) & 1u, wait_iters)) {
-        *fail = 1;
-        break;
+  if (warp == 1) {
+    // ---------------------------------------------------------------- TMA loader
+    if (lane == 0) {
+      mbar_arrive_tx(tfull, (uint32_t)t2_halves(Q) * 2u);
+      bulk_load(smem_u32(T2s), Tg, (uint32_t)t2_halves(Q) * 2u, tfull);
+      int64_t issued = 0;
+      for (int64_t j = 0; j < mine; ++j) {
+        const int s = (int)(j % kYS);
+        if (j >= kYS &&
+            !mbar_wait_n(smem_u32(sempty + s), (uint32_t)(j / kYS - 1) & 1u, wait_iters)) {
+          *fail = 1;
+          break;
+        }
+        if (*fail) break;
+        int x, y;
+        item_xy(j, x, y);
+        const uint32_t dst = smem_u32(Ss + (size_t)s * L::S);
+        mbar_arrive_tx(sfull + s, L::ITEM_BYTES);
+#pragma unroll
+        for (int b = 0; b < L::NBOX; ++b)
+          tma_load_box(dst + (uint32_t)(b * kBoxRows * 32), &hmap, x, y + b * kBoxRows,
+                       sfull + s);
+        issued = j + 1;
       }
-      if (*fail) break;
-      const __half2* src = H + item_base(j);
-      const uint32_t dst = smem_u32(Ss + (size_t)s * L::S);
-#pragma unroll 4
-      for (int i = lt; i < 2 * L::N1; i += kYLoaders)
-        cp_async16(dst + 16u * (uint32_t)i, src + (int64_t)(i >> 1) * hp + 4 * (i & 1), 16);
-      mbar_arrive_cp_async(sfull + s);
+      // nothing may leave while a load still writes into shared memory: wait (with the
+      // full default budget) for the loads of every item stage 1 did not consume
+      for (int64_t j = issued > kYS ? issued - kYS : 0; j < issued; ++j)
+        mbar_wait(smem_u32(sfull + (int)(j % kYS)), (uint32_t)(j / kYS) & 1u);
+      mbar_wait(smem_u32(tfull), 0u);
+    }
+  } else if (warp == 2) {
+    // ---------------------------------------------------------------- TMA storer
+    if (lane == 0) {
+      for (int64_t j = 0; j < mine; ++j) {
+        const int p = (int)(j & 1);
+        if (!mbar_wait_n(smem_u32(estaged + p), (uint32_t)(j >> 1) & 1u, wait_iters)) {
+          *fail = 1;
+          break;
+        }
+        if (*fail) break;
+        int x, y;
+        item_xy(j, x, y);
+        const uint32_t src = smem_u32(Es + (size_t)p * L::S);
+#pragma unroll
+        for (int b = 0; b < L::NBOX; ++b)
+          tma_store_box(&hmap, x, y + b * kBoxRows, src + (uint32_t)(b * kBoxRows * 32));
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        // the staging buffer is free once the stores have read it
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+        mbar_arrive(efree + p);
+      }
+      asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
   } else if (warp == 0) {
     // ---------------------------------------------------------------- MMA issuer
@@ -257,7 +311,7 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
       mma_commit(smem_u32(mdone));
       if (!mbar_wait(smem_u32(mdone), 0u)) *fail = 1;
     }
-  } else if (warp < 4 + L::EPI1 / 32) {
+  } else if (warp >= 4 && warp < 4 + L::EPI1 / 32) {
     // ---------------------------------------------------------------- stage 1
     const int t = tid - 128;
     const int c = t >> 3, k2 = t & 7;
@@ -331,21 +385,19 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
   } else if (warp >= 12) {
     // ---------------------------------------------------------------- stage-2 epilogue
     // tensor memory -> FP16 -> output staging (row y' of 32 bytes, interleaved complex or
-    // the segment [Re x 8 | Im x 8]) -> 16-byte stores of whole rows
-    const int q = warp & 3, te = tid - 384;
+    // the segment [Re x 8 | Im x 8]), then handed to the TMA storer
+    const int q = warp & 3;
     const int y1 = 4 * q + (lane >> 3), k2 = lane & 7;
     const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16);
     for (int64_t j = 0; j < mine; ++j) {
       const int p = (int)(j & 1);
-      const uint32_t u = (uint32_t)(j >> 1);
-      const bool got = mbar_wait_n(smem_u32(s2done + p), u & 1u, wait_iters);
-      // one decision for all four warps (and the barrier that frees staging buffer p:
-      // every epilogue thread finished item j - 1, so item j - 2's reads are done)
-      if (epi_any(!got || *fail)) {
-        *fail = 1;
-        break;
-      }
+      const bool got = mbar_wait_n(smem_u32(s2done + p), (uint32_t)(j >> 1) & 1u, wait_iters);
+      // staging buffer p is free once the stores of item j - 2 have read it
+      const bool freed = got && (j < 2 || mbar_wait_n(smem_u32(efree + p),
+                                                      (uint32_t)((j - 2) >> 1) & 1u, wait_iters));
       __syncwarp();  // tcgen05.ld needs the whole warp, converged
+      if (!__all_sync(0xffffffffu, freed)) { *fail = 1; break; }
+      if (__any_sync(0xffffffffu, *fail)) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
       const uint32_t tb = tl + (uint32_t)(p * L::NC2);
       const uint32_t es = smem_u32(Es + (size_t)p * L::S);
@@ -365,31 +417,22 @@ ypass_tc_kernel(__half2* __restrict__ H, int64_t nitems, int hp,
           const uint32_t row = es + 32u * (uint32_t)(y1 + 16 * (g * 16 + i));
           const uint32_t v = pack_half2(re[i], im[i]);
           if (seg) {
-            asm volatile("st.shared.b16 [%0], %1;" ::"r"(row + 2u * k2), "h"((uint16_t)(v & 0xffffu))
+            asm volatile("st.shared.b16 [%0], %1;" ::"r"(row + 2u * k2),
+                         "h"((uint16_t)(v & 0xffffu))
                          : "memory");
-            asm volatile("st.shared.b16 [%0], %1;" ::"r"(row + 16u + 2u * k2), "h"((uint16_t)(v >> 16))
+            asm volatile("st.shared.b16 [%0], %1;" ::"r"(row + 16u + 2u * k2),
+                         "h"((uint16_t)(v >> 16))
                          : "memory");
           } else {
             asm volatile("st.shared.b32 [%0], %1;" ::"r"(row + 4u * k2), "r"(v) : "memory");
           }
         }
       }
-      epi_sync();
-      // 16-byte piece i: row i >> 1, half i & 1
-      __half2* dst = H + item_base(j);
-#pragma unroll
-      for (int m = 0; m < 2 * L::N1 / L::EPI2; ++m) {
-        const int i = te + L::EPI2 * m;
-        uint32_t a, b, c, d;
-        asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
-                     : "=r"(a), "=r"(b), "=r"(c), "=r"(d)
-                     : "r"(es + 16u * (uint32_t)i));
-        uint4* g = reinterpret_cast<uint4*>(dst + (int64_t)(i >> 1) * hp + 4 * (i & 1));
-        *g = make_uint4(a, b, c, d);
-      }
+      // the TMA stores read the staging through the async proxy
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(estaged + p);
     }
   }
-  asm volatile("cp.async.wait_all;\n" ::);
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
@@ -407,6 +450,44 @@ int set_attrs(int optin) {
                      "ypass_tc: shared memory attribute");
 }
 
+using TensorMapEncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                            const cuuint64_t*, const cuuint64_t*,
+                                            const cuuint32_t*, const cuuint32_t*,
+                                            CUtensorMapInterleave, CUtensorMapSwizzle,
+                                            CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+TensorMapEncodeTiledFn tensor_map_encoder() {
+  static const TensorMapEncodeTiledFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault,
+                                         &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (TensorMapEncodeTiledFn) nullptr;
+    }
+    return reinterpret_cast<TensorMapEncodeTiledFn>(f);
+  }();
+  return fn;
+}
+
+// H as a 2D tensor of 4-byte words: hp columns, rows rows (row stride hp words); boxes of
+// 8 columns x 256 rows, no swizzle, no out-of-range fill (every box lies inside).
+int encode_h_map(CUtensorMap* map, void* H, int64_t rows, int hp) {
+  const TensorMapEncodeTiledFn enc = tensor_map_encoder();
+  TM_REQUIRE(enc, "ypass_tc: the driver has no cuTensorMapEncodeTiled");
+  const cuuint64_t dims[2] = {(cuuint64_t)hp, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)hp * 4u};
+  const cuuint32_t box[2] = {8u, (cuuint32_t)kBoxRows};
+  const cuuint32_t estr[2] = {1u, 1u};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, H, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  TM_REQUIRE(r == CUDA_SUCCESS, "ypass_tc: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return TM_OK;
+}
+
 }  // namespace
 
 int ypass_tc_config(int n1, int hp, YpassTcConfig* cfg) {
@@ -414,6 +495,7 @@ int ypass_tc_config(int n1, int hp, YpassTcConfig* cfg) {
   cfg->n1 = n1;
   cfg->Q = n1 / 16;
   if ((n1 != 256 && n1 != 512) || hp % 8 != 0 || hp <= 0) return TM_OK;
+  if (!tensor_map_encoder()) return TM_OK;
   int dev = 0, optin = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -441,16 +523,23 @@ int ypass_tc_run(const YpassTcConfig& cfg, void* H, int nb, int n0, int hp,
                  const uint16_t* table, uint32_t wait_iters, int* err, cudaStream_t stream,
                  bool seg) {
   TM_REQUIRE(cfg.ok, "ypass_tc_run: unsupported configuration");
-  TM_REQUIRE(H && table && err && nb >= 1 && n0 >= 1 && hp % 8 == 0,
+  TM_REQUIRE(H && table && err && nb >= 1 && n0 >= 1 && hp % 8 == 0 && wait_iters > 0,
              "ypass_tc_run: bad arguments");
+  TM_REQUIRE(reinterpret_cast<uintptr_t>(H) % 16 == 0 &&
+                 reinterpret_cast<uintptr_t>(table) % 16 == 0,
+             "ypass_tc_run: H and the operator table must be 16-byte aligned");
+  const int64_t rows = (int64_t)nb * n0 * cfg.n1;
+  TM_REQUIRE(rows < ((int64_t)1 << 31), "ypass_tc_run: more than 2^31 rows");
+  CUtensorMap map;
+  TM_TRY(encode_h_map(&map, H, rows, hp));
   const int64_t nitems = (int64_t)nb * n0 * (hp / 8);
   const int grid = (int)std::min<int64_t>(nitems, cfg.sms);
   if (cfg.Q == 32)
-    ypass_tc_kernel<32><<<grid, kYThreads, cfg.smem, stream>>>(
-        static_cast<__half2*>(H), nitems, hp, table, wait_iters, err, seg ? 1 : 0);
+    ypass_tc_kernel<32><<<grid, kYThreads, cfg.smem, stream>>>(map, nitems, hp / 8, table,
+                                                                wait_iters, err, seg ? 1 : 0);
   else
-    ypass_tc_kernel<16><<<grid, kYThreads, cfg.smem, stream>>>(
-        static_cast<__half2*>(H), nitems, hp, table, wait_iters, err, seg ? 1 : 0);
+    ypass_tc_kernel<16><<<grid, kYThreads, cfg.smem, stream>>>(map, nitems, hp / 8, table,
+                                                                wait_iters, err, seg ? 1 : 0);
   return check_launch("ypass_tc_kernel");
 }
 
