@@ -7,9 +7,11 @@ its target and template. Full launch groups replay one captured CUDA graph per p
 Results come back per job in the reference's ``MaxScoreOverRotations.result``
 layout.
 
-``autotune_batch`` times candidate rotations-per-launch-group values on the real
-target and caches the fastest per (GPU, score, shapes, precision) in a JSON file
-(``$PYTME_B200_CACHE`` or ``~/.cache/pytme_b200/autotune.json``).
+``autotune_plan`` times the plan's configurations on the real target: candidate
+rotations-per-launch-group values, and for each the form of every pass (tensor cores or
+FFTs for the x, y and z passes, a coordinate search from the plan's default), and caches
+the fastest per (GPU, score, shapes, precision) in a JSON file (``$PYTME_B200_CACHE`` or
+``~/.cache/pytme_b200/autotune.json``). ``autotune_batch`` returns its rotation batch.
 """
 from __future__ import annotations
 
@@ -25,7 +27,9 @@ from .matching import (TargetSpectrum, _evaluate_filter, apply_convolution_mode,
                        fourier_padding, rigid_transform_matrices)
 from .scores import ScanPlan, _prepare_target
 
-__all__ = ["MatchJob", "scan_batch", "autotune_batch"]
+__all__ = ["MatchJob", "scan_batch", "autotune_batch", "autotune_plan"]
+
+_PASSES = ("xpass", "ypass", "zpass")
 
 
 @dataclass
@@ -77,15 +81,37 @@ def _key(score, fast, tshape, precision) -> str:
     return f"{name}|{score}|{'x'.join(map(str, fast))}|{'x'.join(map(str, tshape))}|{precision}"
 
 
-def autotune_batch(job: MatchJob, precision: str = "mixed",
-                   candidates: Sequence[int] = (8, 16, 32, 64), groups: int = 2,
-                   use_cache: bool = True) -> int:
-    """Fastest rotations-per-launch-group for this job's shapes (device-timed)."""
+def _time_groups(plan, mats, b, groups, smax, sarg) -> float:
+    """Rotations per second of ``groups`` launch groups after one warm-up group."""
+    n = b * (groups + 1)
+    plan.run(mats[:b], 0, smax, sarg)  # warm-up group
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    plan.run(mats[b:n], b, smax, sarg)
+    e1.record()
+    torch.cuda.synchronize()
+    return (n - b) / (e0.elapsed_time(e1) / 1000.0)
+
+
+def _apply_passes(plan, config: Dict) -> None:
+    for name in _PASSES:
+        getattr(plan, "set_" + name)(config.get(name, "auto"))
+
+
+def autotune_plan(job: MatchJob, precision: str = "mixed",
+                  candidates: Sequence[int] = (8, 16, 32, 64), groups: int = 2,
+                  use_cache: bool = True) -> Dict:
+    """Fastest plan configuration for this job's shapes (device-timed): the rotation
+    batch and, per batch, the x, y and z pass forms found by a coordinate search from the
+    plan's defaults (each pass's other form is kept when it is faster). Returns
+    ``{"batch": B, "xpass": ..., "ypass": ..., "zpass": ..., "rate": rotations/s}``."""
     conv, fast, fast_ft, shift = fourier_padding(job.target.shape, job.template.shape)
     key = _key(job.score, fast, job.template.shape, precision)
     cache = _cache_load() if use_cache else {}
-    if key in cache:
-        return int(cache[key])
+    hit = cache.get(key)
+    if isinstance(hit, dict) and "batch" in hit:
+        return dict(hit)
     t_rev = np.ascontiguousarray(job.template[::-1, ::-1, ::-1], dtype=np.float32)
     m_rev = None if job.mask is None else np.ascontiguousarray(job.mask[::-1, ::-1, ::-1],
                                                                    dtype=np.float32)
@@ -96,41 +122,57 @@ def autotune_batch(job: MatchJob, precision: str = "mixed",
     target = _prepare_target(job.target, tuple(fast), gf)
     center = np.divide(np.asarray(job.template.shape) - 1, 2)
     dev = target.device
-    best, best_rate = None, -1.0
+    best: Optional[Dict] = None
     for b in candidates:
         try:
             plan = ScanPlan(job.score, fast, job.template.shape, precision=precision, batch=b)
         except MemoryError:
             continue
-        if plan.plain:
+        try:
+            if plan.plain:
+                return {"batch": int(candidates[0]), "rate": 0.0}
+            plan.set_template(t_rev, m_rev, tf)
+            plan.set_interpolation(job.interpolation_order)
+            plan.set_target(target)
+            n = b * (groups + 1)
+            rots = np.resize(np.asarray(job.rotations, dtype=np.float32).reshape(-1, 3, 3),
+                             (n, 3, 3))
+            mats = torch.as_tensor(rigid_transform_matrices(rots, center), device=dev)
+            smax = torch.zeros(tuple(fast), dtype=torch.float32, device=dev)
+            sarg = torch.full(tuple(fast), -1, dtype=torch.int32, device=dev)
+            config = {name: getattr(plan, name) for name in _PASSES}
+            rate = _time_groups(plan, mats, b, groups, smax, sarg)
+            for name in _PASSES:
+                other = "fft" if config[name] == "tensor" else "tensor"
+                trial = dict(config, **{name: other})
+                try:
+                    _apply_passes(plan, trial)
+                except (NotImplementedError, ValueError):
+                    _apply_passes(plan, config)
+                    continue
+                r = _time_groups(plan, mats, b, groups, smax, sarg)
+                if r > rate:
+                    config, rate = trial, r
+                _apply_passes(plan, config)
+            del smax, sarg
+        finally:
             plan.close()
-            return int(candidates[0])
-        plan.set_template(t_rev, m_rev, tf)
-        plan.set_interpolation(job.interpolation_order)
-        plan.set_target(target)
-        n = b * (groups + 1)
-        rots = np.resize(np.asarray(job.rotations, dtype=np.float32).reshape(-1, 3, 3), (n, 3, 3))
-        mats = torch.as_tensor(rigid_transform_matrices(rots, center), device=dev)
-        smax = torch.zeros(tuple(fast), dtype=torch.float32, device=dev)
-        sarg = torch.full(tuple(fast), -1, dtype=torch.int32, device=dev)
-        plan.run(mats[:b], 0, smax, sarg)  # warm-up group
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record()
-        plan.run(mats[b:], b, smax, sarg)
-        e1.record()
-        torch.cuda.synchronize()
-        rate = (n - b) / (e0.elapsed_time(e1) / 1000.0)
-        plan.close()
-        del smax, sarg
-        if rate > best_rate:
-            best, best_rate = b, rate
-    best = int(best if best is not None else candidates[0])
+        if best is None or rate > best["rate"]:
+            best = dict(config, batch=int(b), rate=float(rate))
+    if best is None:
+        best = {"batch": int(candidates[0]), "rate": 0.0}
     if use_cache:
         cache = _cache_load()
         cache[key] = best
         _cache_store(cache)
-    return best
+    return dict(best)
+
+
+def autotune_batch(job: MatchJob, precision: str = "mixed",
+                   candidates: Sequence[int] = (8, 16, 32, 64), groups: int = 2,
+                   use_cache: bool = True) -> int:
+    """Fastest rotations-per-launch-group for this job's shapes (``autotune_plan``)."""
+    return int(autotune_plan(job, precision, candidates, groups, use_cache)["batch"])
 
 
 def scan_batch(jobs: List[MatchJob], precision: str = "mixed", rotation_batch="auto",
@@ -147,10 +189,13 @@ def scan_batch(jobs: List[MatchJob], precision: str = "mixed", rotation_batch="a
             key = (job.score, tuple(fast), tmpl.shape, has_filter)
             plan = plans.get(key)
             if plan is None:
-                b = rotation_batch
+                b, config = rotation_batch, {}
                 if b == "auto":
-                    b = autotune_batch(job, precision=precision)
+                    config = autotune_plan(job, precision=precision)
+                    b = config["batch"]
                 plan = ScanPlan(job.score, fast, tmpl.shape, precision=precision, batch=int(b))
+                if not plan.plain:
+                    _apply_passes(plan, config)
                 if use_graph:
                     plan.set_graph(True)
                 plans[key] = plan

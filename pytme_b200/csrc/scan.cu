@@ -1335,7 +1335,7 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
   tmr.end(TM_STAGE_XPASS);
   tmr.begin();
   if (s->ytc && std::is_same<HT, __half2>::value) {
-    TM_TRY(ypass_tc_run(s->ycfg, H, nb, s->n0, s->hp, s->ytable, s->wait_iters, s->tc_err,
+    TM_TRY(ypass_tc_run(s->ycfg, H, nb, s->n0, s->hp, s->h2, s->ytable, s->wait_iters, s->tc_err,
                         stream, seg_layout(s)));
   } else if (s->reg1) {
     TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, HT>(s, nb, H, stream, seg_layout(s))));

@@ -38,8 +38,8 @@
 #include "tc_common.cuh"
 #include "ypass_tc.cuh"
 
-#include <cuda.h>  // CUtensorMap and the encoder's types; the encoder itself is reached
-                   // through cudaGetDriverEntryPointByVersion
+#include "tma.cuh"
+
 #include <cuda_fp16.h>
 
 #include <algorithm>
@@ -51,7 +51,12 @@ namespace {
 using namespace tc;
 
 constexpr int kYThreads = 512;
+// Buffer counts of the pipeline. Deeper rings (3 operand and 4 accumulator buffers, or 3
+// output staging buffers) measured no faster.
 constexpr int kYS = 4;          // input staging buffers (items whose loads are in flight)
+constexpr int kNA = 2;          // stage-2 operand buffers
+constexpr int kND = 2;          // stage-2 accumulator buffers in tensor memory
+constexpr int kNE = 2;          // output staging buffers
 constexpr int kBoxRows = 256;   // rows per TMA box (the box-dimension limit)
 
 // Stage-2 operator, canonical K-major FP16, two tables (the FP16 head, then the FP16
@@ -83,40 +88,6 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" : : "r"(smem_u32(bar)) : "memory");
 }
-// one arrival that also announces `bytes` of asynchronous copies completing on the barrier
-__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-               :
-               : "r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-// TMA load of one 8 x 256-word box at (x, y) of the tensor into shared memory
-__device__ __forceinline__ void tma_load_box(uint32_t dst, const CUtensorMap* map, int x, int y,
-                                             uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3}], [%4];"
-      :
-      : "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
-// TMA store of one box from shared memory to (x, y) of the tensor
-__device__ __forceinline__ void tma_store_box(const CUtensorMap* map, int x, int y,
-                                              uint32_t src) {
-  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"
-               :
-               : "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(src)
-               : "memory");
-}
-// contiguous bulk copy global -> shared (bytes a multiple of 16, both addresses aligned)
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes,
-                                          uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-      :
-      : "r"(dst), "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
 __device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
   uint32_t r[16];
   asm volatile(
@@ -146,34 +117,39 @@ struct YLayout {
   static constexpr int EPI2 = 128;
   static constexpr int NBOX = N1 / kBoxRows;  // TMA boxes per item
   static constexpr uint32_t ITEM_BYTES = (uint32_t)N1 * 32u;
-  static constexpr int NBAR = 2 * kYS + 10 + 2;
+  static constexpr int NBAR = 2 * (kYS + kNA + kND + kNE) + 2;
+  // tensor-memory columns: kND accumulators of NC2 columns, allocated as a power of two
+  static constexpr uint32_t TMEM = kND * NC2 <= 32 ? 32u : kND * NC2 <= 64 ? 64u
+                                 : kND * NC2 <= 128 ? 128u : kND * NC2 <= 256 ? 256u : 512u;
   static constexpr size_t smem_bytes() {
-    return (size_t)(t2_halves(Q) + kYS * S + 2 * A2 + 2 * S) * 2 + (size_t)NBAR * 8 + 16;
+    return (size_t)(t2_halves(Q) + kYS * S + kNA * A2 + kNE * S) * 2 + (size_t)NBAR * 8 + 16;
   }
 };
 static_assert(YLayout<16>::N1 % kBoxRows == 0 && YLayout<32>::N1 % kBoxRows == 0,
               "items are whole TMA boxes");
+static_assert(kND * YLayout<32>::NC2 <= 512, "accumulators fit in tensor memory");
 
 template <int Q>
 __global__ void __launch_bounds__(kYThreads, 1)
-ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc,
+ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc, int h2,
                 const uint16_t* __restrict__ Tg, uint32_t wait_iters, int* __restrict__ err,
                 int seg) {
   using L = YLayout<Q>;
   extern __shared__ __align__(1024) uint16_t smem_y[];
   uint16_t* T2s = smem_y;
   uint16_t* Ss = T2s + t2_halves(Q);                // kYS input staging buffers
-  uint16_t* A2s = Ss + kYS * L::S;                  // 2 stage-2 operand buffers
-  uint16_t* Es = A2s + 2 * L::A2;                   // 2 output staging buffers
-  uint64_t* bar = reinterpret_cast<uint64_t*>(Es + 2 * L::S);
+  uint16_t* A2s = Ss + kYS * L::S;                  // kNA stage-2 operand buffers
+  uint16_t* Es = A2s + kNA * L::A2;                 // kNE output staging buffers
+  uint64_t* bar = reinterpret_cast<uint64_t*>(Es + kNE * L::S);
   uint64_t* sfull = bar;               // [kYS] item landed (loader arrival + TMA bytes)
   uint64_t* sempty = bar + kYS;        // [kYS] stage 1 read the item (stage-1 threads)
-  uint64_t* e1done = bar + 2 * kYS;    // [2] stage 1 wrote the operand (stage-1 threads)
-  uint64_t* s2done = e1done + 2;       // [2] stage-2 MMAs done: operand free, D2 written
-  uint64_t* d2empty = s2done + 2;      // [2] stage-2 epilogue read D2
-  uint64_t* estaged = d2empty + 2;     // [2] output rows staged (epilogue threads)
-  uint64_t* efree = estaged + 2;       // [2] TMA stores finished reading the staging
-  uint64_t* tfull = efree + 2;         // the operator landed (loader arrival + bytes)
+  uint64_t* e1done = bar + 2 * kYS;    // [kNA] stage 1 wrote the operand (stage-1 threads)
+  uint64_t* a2free = e1done + kNA;     // [kNA] the MMAs that read the operand are done
+  uint64_t* d2full = a2free + kNA;     // [kND] the MMAs that write the accumulator are done
+  uint64_t* d2empty = d2full + kND;    // [kND] stage-2 epilogue read the accumulator
+  uint64_t* estaged = d2empty + kND;   // [kNE] output rows staged (epilogue threads)
+  uint64_t* efree = estaged + kNE;     // [kNE] TMA stores finished reading the staging
+  uint64_t* tfull = efree + kNE;       // the operator landed (loader arrival + bytes)
   uint64_t* mdone = tfull + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mdone + 1);
   volatile int* fail = reinterpret_cast<volatile int*>(tmem_slot + 1);
@@ -182,7 +158,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                  :
-                 : "r"(smem_u32(tmem_slot)), "r"(128));
+                 : "r"(smem_u32(tmem_slot)), "r"(L::TMEM));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
@@ -190,10 +166,15 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
       mbar_init(sfull + s, 1);
       mbar_init(sempty + s, L::EPI1);
     }
-    for (int p = 0; p < 2; ++p) {
+    for (int p = 0; p < kNA; ++p) {
       mbar_init(e1done + p, L::EPI1);
-      mbar_init(s2done + p, 1);
+      mbar_init(a2free + p, 1);
+    }
+    for (int p = 0; p < kND; ++p) {
+      mbar_init(d2full + p, 1);
       mbar_init(d2empty + p, L::EPI2);
+    }
+    for (int p = 0; p < kNE; ++p) {
       mbar_init(estaged + p, L::EPI2);
       mbar_init(efree + p, 1);
     }
@@ -206,7 +187,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tmem_slot;
-  // tensor memory: D2 (stage-2 accumulators) in two buffers of 64 columns
+  // tensor memory: D2 (stage-2 accumulators) in kND buffers of NC2 columns
   const int64_t mine = nitems > blockIdx.x ? (nitems - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   // item id -> (tensor row of its first row, tensor column of its first word)
   auto item_xy = [&](int64_t j, int& x, int& y) {
@@ -218,8 +199,8 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
   if (warp == 1) {
     // ---------------------------------------------------------------- TMA loader
     if (lane == 0) {
-      mbar_arrive_tx(tfull, (uint32_t)t2_halves(Q) * 2u);
-      bulk_load(smem_u32(T2s), Tg, (uint32_t)t2_halves(Q) * 2u, tfull);
+      tma::arrive_expect_tx(tfull, (uint32_t)t2_halves(Q) * 2u);
+      tma::bulk_load(smem_u32(T2s), Tg, (uint32_t)t2_halves(Q) * 2u, tfull);
       int64_t issued = 0;
       for (int64_t j = 0; j < mine; ++j) {
         const int s = (int)(j % kYS);
@@ -232,10 +213,10 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
         int x, y;
         item_xy(j, x, y);
         const uint32_t dst = smem_u32(Ss + (size_t)s * L::S);
-        mbar_arrive_tx(sfull + s, L::ITEM_BYTES);
+        tma::arrive_expect_tx(sfull + s, L::ITEM_BYTES);
 #pragma unroll
         for (int b = 0; b < L::NBOX; ++b)
-          tma_load_box(dst + (uint32_t)(b * kBoxRows * 32), &hmap, x, y + b * kBoxRows,
+          tma::load_2d(dst + (uint32_t)(b * kBoxRows * 32), &hmap, x, y + b * kBoxRows,
                        sfull + s);
         issued = j + 1;
       }
@@ -249,8 +230,8 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
     // ---------------------------------------------------------------- TMA storer
     if (lane == 0) {
       for (int64_t j = 0; j < mine; ++j) {
-        const int p = (int)(j & 1);
-        if (!mbar_wait_n(smem_u32(estaged + p), (uint32_t)(j >> 1) & 1u, wait_iters)) {
+        const int p = (int)(j % kNE);
+        if (!mbar_wait_n(smem_u32(estaged + p), (uint32_t)(j / kNE) & 1u, wait_iters)) {
           *fail = 1;
           break;
         }
@@ -260,7 +241,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
         const uint32_t src = smem_u32(Es + (size_t)p * L::S);
 #pragma unroll
         for (int b = 0; b < L::NBOX; ++b)
-          tma_store_box(&hmap, x, y + b * kBoxRows, src + (uint32_t)(b * kBoxRows * 32));
+          tma::store_2d(&hmap, x, y + b * kBoxRows, src + (uint32_t)(b * kBoxRows * 32));
         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
         // the staging buffer is free once the stores have read it
         asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
@@ -275,21 +256,21 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
       const uint32_t t2 = smem_u32(T2s), a2 = smem_u32(A2s);
       bool ok = mbar_wait_n(smem_u32(tfull), 0u, wait_iters);
       for (int64_t j = 0; j < mine && ok; ++j) {
-        const int p = (int)(j & 1);
-        if (!mbar_wait_n(smem_u32(e1done + p), (uint32_t)(j >> 1) & 1u, wait_iters)) {
+        const int pa = (int)(j % kNA), pd = (int)(j % kND);
+        if (!mbar_wait_n(smem_u32(e1done + pa), (uint32_t)(j / kNA) & 1u, wait_iters)) {
           ok = false;
           break;
         }
-        if (j >= 2 &&
-            !mbar_wait_n(smem_u32(d2empty + p), (uint32_t)((j - 2) >> 1) & 1u, wait_iters)) {
+        if (j >= kND &&
+            !mbar_wait_n(smem_u32(d2empty + pd), (uint32_t)(j / kND - 1) & 1u, wait_iters)) {
           ok = false;
           break;
         }
         if (*fail) { ok = false; break; }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::after_thread_sync;");
-        const uint32_t ab = a2 + (uint32_t)p * (uint32_t)L::A2 * 2u;
-        const uint32_t dt = tmem + (uint32_t)(p * L::NC2);
+        const uint32_t ab = a2 + (uint32_t)pa * (uint32_t)L::A2 * 2u;
+        const uint32_t dt = tmem + (uint32_t)(pd * L::NC2);
         // D = Zh Th + Zt Th + Zh Tt, K step by K step (16 positions, 256 bytes)
 #pragma unroll
         for (int st = 0; st < L::KT / 16; ++st) {
@@ -303,7 +284,8 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
           mma_f16(dt, zt, th, id2, 1);
           mma_f16(dt, zh, tt, id2, 1);
         }
-        mma_commit(smem_u32(s2done + p));
+        mma_commit(smem_u32(a2free + pa));
+        mma_commit(smem_u32(d2full + pd));
       }
       if (!ok) *fail = 1;
       // nothing may free tensor memory or shared memory under a running MMA: this wait
@@ -329,7 +311,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
     const uint32_t a2t = smem_u32(A2s) + 128u * (uint32_t)(c >> 2) + 16u * (uint32_t)k2 +
                          4u * (uint32_t)(c & 3);
     for (int64_t j = 0; j < mine; ++j) {
-      const int s = (int)(j % kYS), p = (int)(j & 1);
+      const int s = (int)(j % kYS), pa = (int)(j % kNA);
       if (!mbar_wait_n(smem_u32(sfull + s), (uint32_t)(j / kYS) & 1u, wait_iters)) {
         *fail = 1;
         break;
@@ -359,12 +341,12 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
       }
 #pragma unroll
       for (int y0 = 0; y0 < 4; ++y0) fft::dft4<1>(v[y0]);
-      if (j >= 2 && !mbar_wait_n(smem_u32(s2done + p), (uint32_t)((j - 2) >> 1) & 1u,
-                                 wait_iters)) {
+      if (j >= kNA && !mbar_wait_n(smem_u32(a2free + pa), (uint32_t)(j / kNA - 1) & 1u,
+                                   wait_iters)) {
         *fail = 1;
         break;
       }
-      const uint32_t dst = a2t + (uint32_t)p * (uint32_t)L::A2 * 2u;
+      const uint32_t dst = a2t + (uint32_t)pa * (uint32_t)L::A2 * 2u;
 #pragma unroll
       for (int y1 = 0; y1 < 16; ++y1) {
         const float2 z = v[y1 & 3][y1 >> 2];
@@ -380,7 +362,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
                      : "memory");
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(e1done + p);
+      mbar_arrive(e1done + pa);
     }
   } else if (warp >= 12) {
     // ---------------------------------------------------------------- stage-2 epilogue
@@ -390,17 +372,22 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
     const int y1 = 4 * q + (lane >> 3), k2 = lane & 7;
     const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16);
     for (int64_t j = 0; j < mine; ++j) {
-      const int p = (int)(j & 1);
-      const bool got = mbar_wait_n(smem_u32(s2done + p), (uint32_t)(j >> 1) & 1u, wait_iters);
-      // staging buffer p is free once the stores of item j - 2 have read it
-      const bool freed = got && (j < 2 || mbar_wait_n(smem_u32(efree + p),
-                                                      (uint32_t)((j - 2) >> 1) & 1u, wait_iters));
+      const int pd = (int)(j % kND), pe = (int)(j % kNE);
+      const bool got = mbar_wait_n(smem_u32(d2full + pd), (uint32_t)(j / kND) & 1u, wait_iters);
+      // staging buffer pe is free once the stores of item j - kNE have read it
+      const bool freed = got && (j < kNE || mbar_wait_n(smem_u32(efree + pe),
+                                                        (uint32_t)(j / kNE - 1) & 1u,
+                                                        wait_iters));
       __syncwarp();  // tcgen05.ld needs the whole warp, converged
       if (!__all_sync(0xffffffffu, freed)) { *fail = 1; break; }
       if (__any_sync(0xffffffffu, *fail)) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
-      const uint32_t tb = tl + (uint32_t)(p * L::NC2);
-      const uint32_t es = smem_u32(Es + (size_t)p * L::S);
+      const uint32_t tb = tl + (uint32_t)(pd * L::NC2);
+      const uint32_t es = smem_u32(Es + (size_t)pe * L::S);
+      // columns k2 >= h2 (the row padding) are written as zeros
+      int xcol, yrow;
+      item_xy(j, xcol, yrow);
+      const bool pad = xcol + k2 >= h2;
       // D2 columns [Re | Im], Q each: output y' = y1 + 16 y2
 #pragma unroll
       for (int g = 0; g < Q / 16; ++g) {
@@ -410,12 +397,12 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
         asm volatile("tcgen05.wait::ld.sync.aligned;");
         if (g == Q / 16 - 1) {
           asm volatile("tcgen05.fence::before_thread_sync;");
-          mbar_arrive(d2empty + p);
+          mbar_arrive(d2empty + pd);
         }
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           const uint32_t row = es + 32u * (uint32_t)(y1 + 16 * (g * 16 + i));
-          const uint32_t v = pack_half2(re[i], im[i]);
+          const uint32_t v = pad ? 0u : pack_half2(re[i], im[i]);
           if (seg) {
             asm volatile("st.shared.b16 [%0], %1;" ::"r"(row + 2u * k2),
                          "h"((uint16_t)(v & 0xffffu))
@@ -430,7 +417,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
       }
       // the TMA stores read the staging through the async proxy
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(estaged + p);
+      mbar_arrive(estaged + pe);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -438,7 +425,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
   asm volatile("tcgen05.fence::after_thread_sync;");
   if (warp == 0) {
     __syncwarp();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(tmem), "r"(128));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(tmem), "r"(L::TMEM));
   }
   if (tid == 0 && *fail) atomicExch(err, 1);
 }
@@ -450,44 +437,6 @@ int set_attrs(int optin) {
                      "ypass_tc: shared memory attribute");
 }
 
-using TensorMapEncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                            const cuuint64_t*, const cuuint64_t*,
-                                            const cuuint32_t*, const cuuint32_t*,
-                                            CUtensorMapInterleave, CUtensorMapSwizzle,
-                                            CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-TensorMapEncodeTiledFn tensor_map_encoder() {
-  static const TensorMapEncodeTiledFn fn = [] {
-    void* f = nullptr;
-    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault,
-                                         &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess) {
-      cudaGetLastError();
-      return (TensorMapEncodeTiledFn) nullptr;
-    }
-    return reinterpret_cast<TensorMapEncodeTiledFn>(f);
-  }();
-  return fn;
-}
-
-// H as a 2D tensor of 4-byte words: hp columns, rows rows (row stride hp words); boxes of
-// 8 columns x 256 rows, no swizzle, no out-of-range fill (every box lies inside).
-int encode_h_map(CUtensorMap* map, void* H, int64_t rows, int hp) {
-  const TensorMapEncodeTiledFn enc = tensor_map_encoder();
-  TM_REQUIRE(enc, "ypass_tc: the driver has no cuTensorMapEncodeTiled");
-  const cuuint64_t dims[2] = {(cuuint64_t)hp, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)hp * 4u};
-  const cuuint32_t box[2] = {8u, (cuuint32_t)kBoxRows};
-  const cuuint32_t estr[2] = {1u, 1u};
-  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, H, dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  TM_REQUIRE(r == CUDA_SUCCESS, "ypass_tc: cuTensorMapEncodeTiled failed (%d)", (int)r);
-  return TM_OK;
-}
-
 }  // namespace
 
 int ypass_tc_config(int n1, int hp, YpassTcConfig* cfg) {
@@ -495,7 +444,7 @@ int ypass_tc_config(int n1, int hp, YpassTcConfig* cfg) {
   cfg->n1 = n1;
   cfg->Q = n1 / 16;
   if ((n1 != 256 && n1 != 512) || hp % 8 != 0 || hp <= 0) return TM_OK;
-  if (!tensor_map_encoder()) return TM_OK;
+  if (!tensor_maps_available()) return TM_OK;
   int dev = 0, optin = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -519,26 +468,31 @@ int ypass_tc_prepare(const YpassTcConfig& cfg, uint16_t* table, cudaStream_t str
   return check_launch("ydft_table_kernel");
 }
 
-int ypass_tc_run(const YpassTcConfig& cfg, void* H, int nb, int n0, int hp,
+int ypass_tc_run(const YpassTcConfig& cfg, void* H, int nb, int n0, int hp, int h2,
                  const uint16_t* table, uint32_t wait_iters, int* err, cudaStream_t stream,
                  bool seg) {
   TM_REQUIRE(cfg.ok, "ypass_tc_run: unsupported configuration");
-  TM_REQUIRE(H && table && err && nb >= 1 && n0 >= 1 && hp % 8 == 0 && wait_iters > 0,
+  TM_REQUIRE(H && table && err && nb >= 1 && n0 >= 1 && hp % 8 == 0 && h2 >= 1 && h2 <= hp &&
+                 wait_iters > 0,
              "ypass_tc_run: bad arguments");
   TM_REQUIRE(reinterpret_cast<uintptr_t>(H) % 16 == 0 &&
                  reinterpret_cast<uintptr_t>(table) % 16 == 0,
              "ypass_tc_run: H and the operator table must be 16-byte aligned");
   const int64_t rows = (int64_t)nb * n0 * cfg.n1;
   TM_REQUIRE(rows < ((int64_t)1 << 31), "ypass_tc_run: more than 2^31 rows");
+  // H as a 2D tensor of 4-byte words: hp columns, rows rows; boxes of 8 x 256 words
   CUtensorMap map;
-  TM_TRY(encode_h_map(&map, H, rows, hp));
+  const uint64_t dims[2] = {(uint64_t)hp, (uint64_t)rows};
+  const uint64_t strides[1] = {(uint64_t)hp * 4u};
+  const uint32_t box[2] = {8u, (uint32_t)kBoxRows};
+  TM_TRY(encode_tensor_map_u32(&map, H, 2, dims, strides, box));
   const int64_t nitems = (int64_t)nb * n0 * (hp / 8);
   const int grid = (int)std::min<int64_t>(nitems, cfg.sms);
   if (cfg.Q == 32)
-    ypass_tc_kernel<32><<<grid, kYThreads, cfg.smem, stream>>>(map, nitems, hp / 8, table,
+    ypass_tc_kernel<32><<<grid, kYThreads, cfg.smem, stream>>>(map, nitems, hp / 8, h2, table,
                                                                 wait_iters, err, seg ? 1 : 0);
   else
-    ypass_tc_kernel<16><<<grid, kYThreads, cfg.smem, stream>>>(map, nitems, hp / 8, table,
+    ypass_tc_kernel<16><<<grid, kYThreads, cfg.smem, stream>>>(map, nitems, hp / 8, h2, table,
                                                                 wait_iters, err, seg ? 1 : 0);
   return check_launch("ypass_tc_kernel");
 }

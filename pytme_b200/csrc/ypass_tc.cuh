@@ -22,11 +22,12 @@ size_t ypass_tc_table_bytes(const YpassTcConfig& cfg);
 // ypass_tc_table_bytes.
 int ypass_tc_prepare(const YpassTcConfig& cfg, uint16_t* table, cudaStream_t stream);
 // Unnormalised inverse DFT along axis 1 of the half-precision spectra
-// H[nb][n0][n1][hp], in place. wait_iters bounds every mbarrier wait; a wait that runs
-// out sets *err and the kernel returns early (its output is then invalid).
+// H[nb][n0][n1][hp], in place; columns h2 .. hp - 1 of every row are written as zeros.
+// wait_iters bounds every mbarrier wait; a wait that runs out sets *err and the kernel
+// returns early (its output is then invalid).
 // seg: write each row's 8-column item as a segment [Re x 8 | Im x 8] (the layout the
 // even/odd tensor-core z pass reads with plain 16-byte copies) instead of interleaved.
-int ypass_tc_run(const YpassTcConfig& cfg, void* H, int nb, int n0, int hp,
+int ypass_tc_run(const YpassTcConfig& cfg, void* H, int nb, int n0, int hp, int h2,
                  const uint16_t* table, uint32_t wait_iters, int* err, cudaStream_t stream,
                  bool seg = false);
 
