@@ -450,8 +450,10 @@ def time_cpu_loop(loop, rots, steps, warmup, min_seconds):
         t0 = time.perf_counter()
         loop.step(chunks(1))
         t_warm.append(time.perf_counter() - t0)
-    per_rot = min(t_warm)
-    r = int(min(8, max(1, np.ceil(min_seconds / max(steps, 1) / per_rot))))
+    # the last warm-up step is the closest to steady state (the first ones also plan the
+    # FFTs and fault in the workers' memory); 15 % margin on the target duration
+    per_rot = t_warm[-1]
+    r = int(min(16, max(1, np.ceil(1.15 * min_seconds / max(steps, 1) / per_rot))))
     times = []
     for _ in range(steps):
         t0 = time.perf_counter()
