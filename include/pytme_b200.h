@@ -191,10 +191,12 @@ int tm_scan_set_zpass(tm_scan* plan, int mode);
 int tm_scan_zpass_mode(const tm_scan* plan);
 /* y pass of the fused CC / FLCSphericalMask scan (the inverse transform along axis 1 of
  * corr_scoring's irfftn, tme/matching_scores.py:618-620): mode 0 runs it on the tensor
- * cores as two FP16 DFT GEMM stages (radix 16, then radix n1/16, twiddles between them;
- * mixed-precision plans with n1 of 256 or 512; the default where available), mode 1 as
- * CUDA-core FFTs, mode 2 restores the default. TM_E_UNSUPPORTED when mode 0 is not
- * available. */
+ * cores (radix 16 in FP32 registers, then radix n1/16 as an FP16 DFT GEMM, twiddles
+ * between them; mixed-precision plans with n1 of 256 or 512; the default where
+ * available), mode 1 as CUDA-core FFTs, mode 2 restores the default, mode 3 runs both
+ * DFT stages on the tensor cores (needs the warp-specialised tensor-core x pass, which
+ * then writes the y pass's input layout). tm_scan_ypass_mode reports 0, 1 or 3.
+ * TM_E_UNSUPPORTED when the requested form is not available. */
 int tm_scan_set_ypass(tm_scan* plan, int mode);
 int tm_scan_ypass_mode(const tm_scan* plan);
 /* Bound of every data wait inside the plan's tensor-core kernels, in mbarrier polls

@@ -44,8 +44,9 @@ def _set_options(**kwargs):
     if _OPTIONS["precision"] not in ("fp32", "mixed"):
         raise ValueError("precision must be 'fp32' or 'mixed'")
     for key in ("xpass", "ypass", "zpass"):
-        if _OPTIONS[key] not in ("auto", "fft", "tensor"):
-            raise ValueError(f"{key} must be 'auto', 'fft' or 'tensor'")
+        allowed = ("auto", "fft", "tensor") + (("tensor2",) if key == "ypass" else ())
+        if _OPTIONS[key] not in allowed:
+            raise ValueError(f"{key} must be one of {', '.join(allowed)}")
     _OPTIONS["rotation_batch"] = int(_OPTIONS["rotation_batch"])
     if not 1 <= _OPTIONS["rotation_batch"] <= 4096:
         raise ValueError("rotation_batch must be in [1, 4096]")

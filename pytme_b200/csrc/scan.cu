@@ -1066,6 +1066,7 @@ struct Scan {
   // tensor-core y pass (CC / FLCSphericalMask, half-precision H, n1 in {256, 512}): the
   // two DFT operators
   bool ytc_avail = false, ytc = false;
+  bool ys1 = false;  // radix-16 stage on the tensor cores too (tm_scan_set_ypass mode 3)
   YpassTcConfig ycfg{};
   uint16_t* ytable = nullptr;
   // polls of every data wait of the tensor-core kernels before they give up
@@ -1120,6 +1121,16 @@ struct Scan {
 static bool seg_layout(const Scan* s) {
   return s->half && s->ztc && s->zcfg.eo && (s->ytc || s->reg1);
 }
+
+// Whether the warp-specialised tensor-core x pass writes every launch group, so it can store
+// H rows as segments in the y pass's stage-1 order.
+static bool x_writes_stage1(const Scan* s) {
+  return s->half && s->xtc && s->xcfg.ws && s->B <= s->xcfg.ws_NB && s->hp % 8 == 0 &&
+         s->d.score != TM_SCORE_FLC;
+}
+// The tensor-core y pass runs its radix-16 stage on the tensor cores too (opt-in: measured
+// slower than the radix-16 stage on the CUDA cores).
+static bool y_stage1_tc(const Scan* s) { return s->ytc && s->ys1 && x_writes_stage1(s); }
 
 // Stage timing: record an event before a stage and accumulate after it.
 struct StageTimer {
@@ -1320,9 +1331,10 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
   if (flc) {
     TM_DISPATCH_N(s->n0, (launch_xpass_flc_reg<NN, HT>(s, nb, hs, H, stream)));
   } else if (s->xtc) {
+    const bool s1 = y_stage1_tc(s);
     TM_TRY(xcorr_tc_run(s->xcfg, s->G, s->ctarget, nb, s->t0, s->n0, s->n1, s->h2, s->hp, hs,
                         H, std::is_same<HT, __half2>::value, s->tc_err, stream,
-                        s->wait_iters));
+                        s->wait_iters, s1, s1 ? s->n1 / 16 : 0));
   } else if (s->reg0) {
     TM_DISPATCH_N(s->n0, (launch_xpass_reg<NN, HT>(s, nb, hs, H, stream)));
   } else {
@@ -1336,7 +1348,7 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
   tmr.begin();
   if (s->ytc && std::is_same<HT, __half2>::value) {
     TM_TRY(ypass_tc_run(s->ycfg, H, nb, s->n0, s->hp, s->h2, s->ytable, s->wait_iters, s->tc_err,
-                        stream, seg_layout(s)));
+                        stream, seg_layout(s), y_stage1_tc(s)));
   } else if (s->reg1) {
     TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, HT>(s, nb, H, stream, seg_layout(s))));
     if (flc) {
@@ -1736,14 +1748,25 @@ int scan_set_zpass(Scan* s, int mode) {
 
 int scan_zpass_mode(const Scan* s) { return s && s->ztc ? 0 : 1; }
 
-// y pass on the tensor cores (mode 0: two FP16 GEMM stages, half-precision CC /
-// FLCSphericalMask plans with n1 in {256, 512}; the default where available) or as FFTs on
-// the CUDA cores (mode 1); mode 2 restores the default.
+// y pass on the tensor cores (mode 0: radix 16 in FP32 registers, radix n1/16 as an FP16
+// GEMM; half-precision CC / FLCSphericalMask plans with n1 in {256, 512}; the default
+// where available), as FFTs on the CUDA cores (mode 1), the default (mode 2), or with both
+// DFT stages on the tensor cores (mode 3: needs the warp-specialised tensor-core x pass,
+// which then writes the y pass's stage-1 layout).
 int scan_set_ypass(Scan* s, int mode) {
   TM_REQUIRE(s, "scan_set_ypass: null plan");
-  TM_REQUIRE(mode >= 0 && mode <= 2,
-             "scan_set_ypass: mode must be 0 (tensor cores), 1 (FFT) or 2 (default)");
-  const bool want = mode == 0 || (mode == 2 && s->ytc_avail);
+  TM_REQUIRE(mode >= 0 && mode <= 3,
+             "scan_set_ypass: mode must be 0 (tensor cores), 1 (FFT), 2 (default) or 3 "
+             "(both DFT stages on the tensor cores)");
+  if (mode == 3 && !(s->ytc_avail && x_writes_stage1(s))) {
+    set_error("scan_set_ypass: both y stages on the tensor cores need the tensor-core y pass "
+              "and the warp-specialised tensor-core x pass");
+    return TM_E_UNSUPPORTED;
+  }
+  const bool want = mode == 0 || mode == 3 || (mode == 2 && s->ytc_avail);
+  const bool s1 = mode == 3;
+  if (s1 != s->ys1 && s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+  s->ys1 = s1;
   if (want && !s->ytc_avail) {
     set_error("scan_set_ypass: the tensor-core y pass does not support this plan");
     return TM_E_UNSUPPORTED;
@@ -1753,7 +1776,10 @@ int scan_set_ypass(Scan* s, int mode) {
   return TM_OK;
 }
 
-int scan_ypass_mode(const Scan* s) { return s && s->ytc ? 0 : 1; }
+int scan_ypass_mode(const Scan* s) {
+  if (!s || !s->ytc) return 1;
+  return y_stage1_tc(s) ? 3 : 0;
+}
 
 // Polls of every data wait in the plan's tensor-core kernels (0 restores the default).
 int scan_set_wait_budget(Scan* s, uint32_t iters) {

@@ -167,7 +167,8 @@ template <int NXC, int R>
 __global__ void __launch_bounds__(kWsThreads, 1)
 xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int nb, int NB,
                 int t0, int n0, int n1, int h2, int hp, float scale,
-                __half2* __restrict__ H, int* __restrict__ err, uint32_t wait_iters) {
+                __half2* __restrict__ H, int* __restrict__ err, uint32_t wait_iters,
+                int seg, int rowq) {
   constexpr int t0p = 8 * NXC;
   const uint32_t wi = wait_iters ? wait_iters : kWaitIters;  // data waits
   constexpr uint32_t kAccCols = 16u * R;               // one fill
@@ -394,7 +395,10 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
     for (int64_t j = 0; j < mine && ok; ++j) {
       const int64_t item = (int64_t)blockIdx.x + j * gridDim.x;
       const int k1 = (int)(item / ncg), k20 = (int)(item - (int64_t)k1 * ncg) * kWsW;
-      const int64_t colH = (int64_t)k1 * hp + k20;
+      // row k1 = rowq a + c goes to position 16 c + a when rowq > 0 (the y pass's stage-1
+      // order), to position k1 otherwise
+      const int krow = rowq > 0 ? (k1 % rowq) * 16 + k1 / rowq : k1;
+      const int64_t colH = (int64_t)krow * hp + k20;
       for (int t = 0; t < ntile && ok; ++t) {
         const int64_t tau = j * ntile + t;
         const int xp = t * kWsRows + kWsRows - 1 - r;
@@ -424,10 +428,23 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
               const int b = R * h + bl + q;
               if (b >= nb) break;
               uint32_t pk[kWsW];
+              if (seg) {
+                // segment [Re x 8 | Im x 8]: words 0-3 Re of column pairs, 4-7 Im
 #pragma unroll
-              for (int w = 0; w < kWsW; ++w) {
-                const __half2 hv = __floats2half2_rn(v[2 * w][q] * inv, v[2 * w + 1][q] * inv);
-                pk[w] = *reinterpret_cast<const uint32_t*>(&hv);
+                for (int w = 0; w < kWsW / 2; ++w) {
+                  const __half2 re = __floats2half2_rn(v[4 * w][q] * inv, v[4 * w + 2][q] * inv);
+                  const __half2 im =
+                      __floats2half2_rn(v[4 * w + 1][q] * inv, v[4 * w + 3][q] * inv);
+                  pk[w] = *reinterpret_cast<const uint32_t*>(&re);
+                  pk[kWsW / 2 + w] = *reinterpret_cast<const uint32_t*>(&im);
+                }
+              } else {
+#pragma unroll
+                for (int w = 0; w < kWsW; ++w) {
+                  const __half2 hv =
+                      __floats2half2_rn(v[2 * w][q] * inv, v[2 * w + 1][q] * inv);
+                  pk[w] = *reinterpret_cast<const uint32_t*>(&hv);
+                }
               }
               st_global_v8(hrow + (int64_t)b * SH, pk);
             }
@@ -478,10 +495,11 @@ int xcorr_ws_config(int n0, int t0, int nb, XcorrTcConfig* cfg) {
 
 int xcorr_ws_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int nb, int t0,
                  int n0, int n1, int h2, int hp, float scale, __half2* H, int* err,
-                 cudaStream_t stream, uint32_t wait_iters) {
+                 cudaStream_t stream, uint32_t wait_iters, bool seg, int rowq) {
   // 32-byte row segments: pitch a multiple of 8 complex values, aligned base
   TM_REQUIRE(cfg.ws && nb <= cfg.ws_NB && hp % 8 == 0 && hp >= h2 &&
-                 reinterpret_cast<uintptr_t>(H) % 32 == 0,
+                 reinterpret_cast<uintptr_t>(H) % 32 == 0 &&
+                 (rowq == 0 || (rowq > 0 && n1 == 16 * rowq)),
              "xcorr_ws_run: unsupported configuration");
   const int64_t nitems = (int64_t)n1 * ((h2 + kWsW - 1) / kWsW);
   const int grid = (int)std::min<int64_t>(nitems, cfg.sms);
@@ -496,7 +514,7 @@ int xcorr_ws_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int
     default: TM_REQUIRE(false, "xcorr_ws_run: t0p %d", cfg.ws_t0p);
   }
   fn<<<grid, kWsThreads, cfg.ws_smem, stream>>>(G, C, nb, cfg.ws_NB, t0, n0, n1, h2, hp, scale,
-                                               H, err, wait_iters);
+                                               H, err, wait_iters, seg ? 1 : 0, rowq);
   return check_launch("xcorr_ws_kernel");
 }
 

@@ -82,6 +82,27 @@ __global__ void ydft_table_kernel(uint16_t* __restrict__ T, int Q) {
   }
 }
 
+// Stage-1 operator (radix 16 on the tensor cores), canonical K-major FP16, two tables (head,
+// then the FP16 rounded remainder) of 32 rows [Re Z | Im Z] x 16 outputs y1 by 32 K
+// positions 2a + (0: Re X, 1: Im X): the inverse DFT w16^(a y1).
+constexpr int kF1Halves = 2 * 32 * 32;
+
+__global__ void ydft16_table_kernel(uint16_t* __restrict__ T) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kF1Halves; i += gridDim.x * blockDim.x) {
+    const int part = i / 1024, e = i - part * 1024;
+    const int n = e / 32, k = e - n * 32;
+    const int comp = n / 16, y1 = n % 16;
+    const int a = k >> 1, ri = k & 1;
+    double sn, cs;
+    sincospi(2.0 * (double)((a * y1) % 16) / 16.0, &sn, &cs);
+    const double v = comp == 0 ? (ri == 0 ? cs : -sn) : (ri == 0 ? sn : cs);
+    const float vf = (float)v;
+    const __half hd = __float2half_rn(vf);
+    const __half tl = __float2half_rn(vf - __half2float(hd));
+    T[part * 1024 + kmajor16(n, k, 32)] = __half_as_ushort(part == 0 ? hd : tl);
+  }
+}
+
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" : : "r"(smem_u32(bar)), "r"(count));
 }
@@ -117,19 +138,30 @@ struct YLayout {
   static constexpr int EPI2 = 128;
   static constexpr int NBOX = N1 / kBoxRows;  // TMA boxes per item
   static constexpr uint32_t ITEM_BYTES = (uint32_t)N1 * 32u;
-  static constexpr int NBAR = 2 * (kYS + kNA + kND + kNE) + 2;
+  static constexpr int NBAR = 2 * (kYS + kNA + kND + kNE) + 2 + 4;  // + d1full, d1empty
   // tensor-memory columns: kND accumulators of NC2 columns, allocated as a power of two
-  static constexpr uint32_t TMEM = kND * NC2 <= 32 ? 32u : kND * NC2 <= 64 ? 64u
-                                 : kND * NC2 <= 128 ? 128u : kND * NC2 <= 256 ? 256u : 512u;
+  // with stage 1 on the tensor cores, two more buffers of Q/16 tiles x 32 columns (D1)
+  static constexpr int D1COLS = (Q / 16) * 32;
+  static constexpr int TCOLS = kND * NC2 + 2 * D1COLS;
+  static constexpr uint32_t TMEM = TCOLS <= 32 ? 32u : TCOLS <= 64 ? 64u
+                                 : TCOLS <= 128 ? 128u : TCOLS <= 256 ? 256u : 512u;
   static constexpr size_t smem_bytes() {
-    return (size_t)(t2_halves(Q) + kYS * S + kNA * A2 + kNE * S) * 2 + (size_t)NBAR * 8 + 16;
+    return (size_t)(t2_halves(Q) + kF1Halves + kYS * S + kNA * A2 + kNE * S) * 2 +
+           (size_t)NBAR * 8 + 16;
   }
 };
 static_assert(YLayout<16>::N1 % kBoxRows == 0 && YLayout<32>::N1 % kBoxRows == 0,
               "items are whole TMA boxes");
-static_assert(kND * YLayout<32>::NC2 <= 512, "accumulators fit in tensor memory");
+static_assert(YLayout<32>::TCOLS <= 512, "accumulators fit in tensor memory");
 
-template <int Q>
+// Shared-memory descriptor strides of the stage-1 X operand, which is M-major (8 k2 values
+// of one row half per 16 bytes): M groups (one c each) 512 bytes apart, K groups (four
+// rows a) 128 bytes apart. As for K-major operands, the descriptor's leading-dimension
+// offset is the stride between core matrices along K and the stride-dimension offset the
+// stride along M (checked against a known product on a B200).
+constexpr uint32_t kS1MStride = 512, kS1KStride = 128;
+
+template <int Q, bool S1>
 __global__ void __launch_bounds__(kYThreads, 1)
 ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc, int h2,
                 const uint16_t* __restrict__ Tg, uint32_t wait_iters, int* __restrict__ err,
@@ -137,7 +169,8 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
   using L = YLayout<Q>;
   extern __shared__ __align__(1024) uint16_t smem_y[];
   uint16_t* T2s = smem_y;
-  uint16_t* Ss = T2s + t2_halves(Q);                // kYS input staging buffers
+  uint16_t* F1s = T2s + t2_halves(Q);               // stage-1 operator (S1)
+  uint16_t* Ss = F1s + kF1Halves;                   // kYS input staging buffers
   uint16_t* A2s = Ss + kYS * L::S;                  // kNA stage-2 operand buffers
   uint16_t* Es = A2s + kNA * L::A2;                 // kNE output staging buffers
   uint64_t* bar = reinterpret_cast<uint64_t*>(Es + kNE * L::S);
@@ -151,7 +184,9 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
   uint64_t* efree = estaged + kNE;     // [kNE] TMA stores finished reading the staging
   uint64_t* tfull = efree + kNE;       // the operator landed (loader arrival + bytes)
   uint64_t* mdone = tfull + 1;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mdone + 1);
+  uint64_t* d1full = mdone + 1;        // [2] stage-1 MMAs done (S1; commit)
+  uint64_t* d1empty = d1full + 2;      // [2] stage-1 accumulators read (S1; stage-1 threads)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(d1empty + 2);
   volatile int* fail = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -164,7 +199,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
   if (tid == 0) {
     for (int s = 0; s < kYS; ++s) {
       mbar_init(sfull + s, 1);
-      mbar_init(sempty + s, L::EPI1);
+      mbar_init(sempty + s, S1 ? 1 : L::EPI1);
     }
     for (int p = 0; p < kNA; ++p) {
       mbar_init(e1done + p, L::EPI1);
@@ -180,6 +215,10 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
     }
     mbar_init(tfull, 1);
     mbar_init(mdone, 1);
+    for (int p = 0; p < 2; ++p) {
+      mbar_init(d1full + p, 1);
+      mbar_init(d1empty + p, L::EPI1);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;");
     *fail = 0;
   }
@@ -199,8 +238,8 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
   if (warp == 1) {
     // ---------------------------------------------------------------- TMA loader
     if (lane == 0) {
-      tma::arrive_expect_tx(tfull, (uint32_t)t2_halves(Q) * 2u);
-      tma::bulk_load(smem_u32(T2s), Tg, (uint32_t)t2_halves(Q) * 2u, tfull);
+      tma::arrive_expect_tx(tfull, (uint32_t)(t2_halves(Q) + kF1Halves) * 2u);
+      tma::bulk_load(smem_u32(T2s), Tg, (uint32_t)(t2_halves(Q) + kF1Halves) * 2u, tfull);
       int64_t issued = 0;
       for (int64_t j = 0; j < mine; ++j) {
         const int s = (int)(j % kYS);
@@ -253,20 +292,45 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
     // ---------------------------------------------------------------- MMA issuer
     if (lane == 0) {
       const uint32_t id2 = idesc_f16(128, L::NC2);
-      const uint32_t t2 = smem_u32(T2s), a2 = smem_u32(A2s);
-      bool ok = mbar_wait_n(smem_u32(tfull), 0u, wait_iters);
-      for (int64_t j = 0; j < mine && ok; ++j) {
+      const uint32_t id1 = idesc_f16(128, 32) | (1u << 15);  // stage 1: X is M-major
+      const uint32_t t2 = smem_u32(T2s), a2 = smem_u32(A2s), f1 = smem_u32(F1s);
+      const uint32_t d1base = tmem + (uint32_t)(kND * L::NC2);
+      // stage 1 of item j (S1): X (staging, rows (c, a)) times the radix-16 operator
+      auto stage1 = [&](int64_t j) -> bool {
+        const int s = (int)(j % kYS), p1 = (int)(j & 1);
+        if (!mbar_wait_n(smem_u32(sfull + s), (uint32_t)(j / kYS) & 1u, wait_iters)) return false;
+        if (j >= 2 &&
+            !mbar_wait_n(smem_u32(d1empty + p1), (uint32_t)((j - 2) >> 1) & 1u, wait_iters))
+          return false;
+        if (*fail) return false;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t xs = smem_u32(Ss + (size_t)s * L::S);
+#pragma unroll
+        for (int tt = 0; tt < Q / 16; ++tt) {
+          const uint32_t d1 = d1base + (uint32_t)(p1 * L::D1COLS + tt * 32);
+#pragma unroll
+          for (int st = 0; st < 2; ++st) {
+            const uint64_t xd = smem_desc(xs + (uint32_t)(tt * 16 * 512 + st * 256), kS1KStride,
+                                          kS1MStride);
+            const uint64_t fh = smem_desc(f1 + (uint32_t)(st * 256), 128u, 512u);
+            const uint64_t ft = smem_desc(f1 + 2048u + (uint32_t)(st * 256), 128u, 512u);
+            mma_f16(d1, xd, fh, id1, st > 0);
+            mma_f16(d1, xd, ft, id1, 1);
+          }
+        }
+        mma_commit(smem_u32(d1full + p1));
+        mma_commit(smem_u32(sempty + s));  // the staging buffer is free once read
+        return true;
+      };
+      // stage 2 of item j: Z' (operand buffer) times the radix-Q operator
+      auto stage2 = [&](int64_t j) -> bool {
         const int pa = (int)(j % kNA), pd = (int)(j % kND);
-        if (!mbar_wait_n(smem_u32(e1done + pa), (uint32_t)(j / kNA) & 1u, wait_iters)) {
-          ok = false;
-          break;
-        }
+        if (!mbar_wait_n(smem_u32(e1done + pa), (uint32_t)(j / kNA) & 1u, wait_iters))
+          return false;
         if (j >= kND &&
-            !mbar_wait_n(smem_u32(d2empty + pd), (uint32_t)(j / kND - 1) & 1u, wait_iters)) {
-          ok = false;
-          break;
-        }
-        if (*fail) { ok = false; break; }
+            !mbar_wait_n(smem_u32(d2empty + pd), (uint32_t)(j / kND - 1) & 1u, wait_iters))
+          return false;
+        if (*fail) return false;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::after_thread_sync;");
         const uint32_t ab = a2 + (uint32_t)pa * (uint32_t)L::A2 * 2u;
@@ -286,6 +350,17 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
         }
         mma_commit(smem_u32(a2free + pa));
         mma_commit(smem_u32(d2full + pd));
+        return true;
+      };
+      bool ok = mbar_wait_n(smem_u32(tfull), 0u, wait_iters);
+      if constexpr (S1) {
+        // stage 1 of item j runs ahead of stage 2 of item j - 1
+        for (int64_t j = 0; j <= mine && ok; ++j) {
+          if (j < mine) ok = stage1(j);
+          if (ok && j >= 1) ok = stage2(j - 1);
+        }
+      } else {
+        for (int64_t j = 0; j < mine && ok; ++j) ok = stage2(j);
       }
       if (!ok) *fail = 1;
       // nothing may free tensor memory or shared memory under a running MMA: this wait
@@ -295,6 +370,56 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
     }
   } else if (warp >= 4 && warp < 4 + L::EPI1 / 32) {
     // ---------------------------------------------------------------- stage 1
+    if constexpr (S1) {
+      // radix 16 came from the tensor cores: read Z[y1] of this (c, k2) row from tensor
+      // memory, apply the twiddle w^(c y1) and write Z' (head and tail) as below
+      const int t = tid - 128;
+      const int c = t >> 3, k2 = t & 7;
+      float wr[16], wi[16];
+#pragma unroll
+      for (int y1 = 0; y1 < 16; ++y1)
+        sincospif(2.0f * (float)(c * y1) / (float)L::N1, &wi[y1], &wr[y1]);
+      const uint32_t a2t = smem_u32(A2s) + 128u * (uint32_t)(c >> 2) + 16u * (uint32_t)k2 +
+                           4u * (uint32_t)(c & 3);
+      // lanes 32 q .. 32 q + 31 of tile (warp - 4) / 4: rows (c mod 16, k2)
+      const uint32_t tl1 = tmem + ((uint32_t)((warp & 3) * 32) << 16) +
+                           (uint32_t)(kND * L::NC2 + ((warp - 4) >> 2) * 32);
+      for (int64_t j = 0; j < mine; ++j) {
+        const int p1 = (int)(j & 1), pa = (int)(j % kNA);
+        const bool got = mbar_wait_n(smem_u32(d1full + p1), (uint32_t)(j >> 1) & 1u, wait_iters);
+        __syncwarp();  // tcgen05.ld needs the whole warp, converged
+        if (!__all_sync(0xffffffffu, got)) { *fail = 1; break; }
+        if (__any_sync(0xffffffffu, *fail)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        float re[16], im[16];
+        tmem_ld16(tl1 + (uint32_t)(p1 * L::D1COLS), re);
+        tmem_ld16(tl1 + (uint32_t)(p1 * L::D1COLS + 16), im);
+        asm volatile("tcgen05.wait::ld.sync.aligned;");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        mbar_arrive(d1empty + p1);
+        if (j >= kNA && !mbar_wait_n(smem_u32(a2free + pa), (uint32_t)(j / kNA - 1) & 1u,
+                                     wait_iters)) {
+          *fail = 1;
+          break;
+        }
+        const uint32_t dst = a2t + (uint32_t)pa * (uint32_t)L::A2 * 2u;
+#pragma unroll
+        for (int y1 = 0; y1 < 16; ++y1) {
+          const float orr = re[y1] * wr[y1] - im[y1] * wi[y1];
+          const float oi = re[y1] * wi[y1] + im[y1] * wr[y1];
+          const __half2 hd = __floats2half2_rn(orr, oi);
+          const float2 hf = __half22float2(hd);
+          const uint32_t head = *reinterpret_cast<const uint32_t*>(&hd);
+          asm volatile("st.shared.b32 [%0], %1;" ::"r"(dst + (uint32_t)(y1 * 64 * Q)), "r"(head)
+                       : "memory");
+          asm volatile("st.shared.b32 [%0], %1;" ::"r"(dst + (uint32_t)(y1 * 64 * Q + 32 * Q)),
+                       "r"(pack_half2(orr - hf.x, oi - hf.y))
+                       : "memory");
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive(e1done + pa);
+      }
+    } else {
     const int t = tid - 128;
     const int c = t >> 3, k2 = t & 7;
     // twiddles w^(c y1) of the column and w16^k, k <= 9, of the radix-16 FFT
@@ -364,6 +489,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(e1done + pa);
     }
+    }
   } else if (warp >= 12) {
     // ---------------------------------------------------------------- stage-2 epilogue
     // tensor memory -> FP16 -> output staging (row y' of 32 bytes, interleaved complex or
@@ -432,7 +558,10 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
 
 template <int Q>
 int set_attrs(int optin) {
-  return cuda_status(cudaFuncSetAttribute(ypass_tc_kernel<Q>,
+  TM_TRY(cuda_status(cudaFuncSetAttribute(ypass_tc_kernel<Q, false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, optin),
+                     "ypass_tc: shared memory attribute"));
+  return cuda_status(cudaFuncSetAttribute(ypass_tc_kernel<Q, true>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, optin),
                      "ypass_tc: shared memory attribute");
 }
@@ -459,18 +588,20 @@ int ypass_tc_config(int n1, int hp, YpassTcConfig* cfg) {
 }
 
 size_t ypass_tc_table_bytes(const YpassTcConfig& cfg) {
-  return (size_t)t2_halves(cfg.Q) * 2;
+  return (size_t)(t2_halves(cfg.Q) + kF1Halves) * 2;
 }
 
 int ypass_tc_prepare(const YpassTcConfig& cfg, uint16_t* table, cudaStream_t stream) {
   TM_REQUIRE(cfg.ok && table, "ypass_tc_prepare: unsupported configuration");
   ydft_table_kernel<<<32, 256, 0, stream>>>(table, cfg.Q);
-  return check_launch("ydft_table_kernel");
+  TM_TRY(check_launch("ydft_table_kernel"));
+  ydft16_table_kernel<<<8, 256, 0, stream>>>(table + t2_halves(cfg.Q));
+  return check_launch("ydft16_table_kernel");
 }
 
 int ypass_tc_run(const YpassTcConfig& cfg, void* H, int nb, int n0, int hp, int h2,
                  const uint16_t* table, uint32_t wait_iters, int* err, cudaStream_t stream,
-                 bool seg) {
+                 bool seg, bool s1) {
   TM_REQUIRE(cfg.ok, "ypass_tc_run: unsupported configuration");
   TM_REQUIRE(H && table && err && nb >= 1 && n0 >= 1 && hp % 8 == 0 && h2 >= 1 && h2 <= hp &&
                  wait_iters > 0,
@@ -488,12 +619,10 @@ int ypass_tc_run(const YpassTcConfig& cfg, void* H, int nb, int n0, int hp, int 
   TM_TRY(encode_tensor_map_u32(&map, H, 2, dims, strides, box));
   const int64_t nitems = (int64_t)nb * n0 * (hp / 8);
   const int grid = (int)std::min<int64_t>(nitems, cfg.sms);
-  if (cfg.Q == 32)
-    ypass_tc_kernel<32><<<grid, kYThreads, cfg.smem, stream>>>(map, nitems, hp / 8, h2, table,
-                                                                wait_iters, err, seg ? 1 : 0);
-  else
-    ypass_tc_kernel<16><<<grid, kYThreads, cfg.smem, stream>>>(map, nitems, hp / 8, h2, table,
-                                                                wait_iters, err, seg ? 1 : 0);
+  auto fn = cfg.Q == 32 ? (s1 ? ypass_tc_kernel<32, true> : ypass_tc_kernel<32, false>)
+                        : (s1 ? ypass_tc_kernel<16, true> : ypass_tc_kernel<16, false>);
+  fn<<<grid, kYThreads, cfg.smem, stream>>>(map, nitems, hp / 8, h2, table, wait_iters, err,
+                                            seg ? 1 : 0);
   return check_launch("ypass_tc_kernel");
 }
 

@@ -27,8 +27,11 @@ int ypass_tc_prepare(const YpassTcConfig& cfg, uint16_t* table, cudaStream_t str
 // returns early (its output is then invalid).
 // seg: write each row's 8-column item as a segment [Re x 8 | Im x 8] (the layout the
 // even/odd tensor-core z pass reads with plain 16-byte copies) instead of interleaved.
+// s1: the input rows are segments too, stored in the stage-1 order (row k1 = Q a + c of
+// a plane at position 16 c + a, the order the tensor-core x pass writes with rowq = Q), and
+// the radix-16 stage runs on the tensor cores; the output rows are in natural order.
 int ypass_tc_run(const YpassTcConfig& cfg, void* H, int nb, int n0, int hp, int h2,
                  const uint16_t* table, uint32_t wait_iters, int* err, cudaStream_t stream,
-                 bool seg = false);
+                 bool seg = false, bool s1 = false);
 
 }  // namespace tmb

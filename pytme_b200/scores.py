@@ -147,15 +147,17 @@ class ScanPlan:
         N.check(N.lib.tm_scan_set_zpass(self._h, code), "tm_scan_set_zpass")
 
     def set_ypass(self, mode: str = "auto"):
-        """y pass on the tensor cores ("tensor"), as FFTs on the CUDA cores ("fft"), or
-        the plan's default ("auto")."""
-        code = {"tensor": 0, "fft": 1, "auto": 2}[mode]
+        """y pass on the tensor cores ("tensor": radix 16 in FP32 registers, radix n1/16 on
+        the tensor cores), with both DFT stages on the tensor cores ("tensor2"; needs the
+        tensor-core x pass), as FFTs on the CUDA cores ("fft"), or the plan's default
+        ("auto")."""
+        code = {"tensor": 0, "fft": 1, "auto": 2, "tensor2": 3}[mode]
         N.check(N.lib.tm_scan_set_ypass(self._h, code), "tm_scan_set_ypass")
 
     @property
     def ypass(self) -> str:
-        """The y pass this plan runs: "tensor" or "fft"."""
-        return "tensor" if N.lib.tm_scan_ypass_mode(self._h) == 0 else "fft"
+        """The y pass this plan runs: "tensor", "tensor2" or "fft"."""
+        return {0: "tensor", 1: "fft", 3: "tensor2"}[N.lib.tm_scan_ypass_mode(self._h)]
 
     def set_wait_budget(self, iters: int = 0):
         """Polls of every data wait in the tensor-core kernels (0: the default). A wait

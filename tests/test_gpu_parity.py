@@ -536,8 +536,9 @@ def test_default_passes_odd_z_length(torch_cuda, score):
                                          ((64, 512, 24), "CC")])
 def test_tensor_core_ypass(torch_cuda, shape, score):
     """The tensor-core y pass (radix-16 and radix-n1/16 FP16 GEMM stages with twiddles
-    between them) for both supported y lengths, with a partial last launch group, against
-    the oracle in FP32 and FP64 and against the CUDA-core y pass."""
+    between them; "tensor": the radix-16 stage in FP32 registers, "tensor2": both stages on
+    the tensor cores) for both supported y lengths, with a partial last launch
+    group, against the oracle in FP32 and FP64 and against the CUDA-core y pass."""
     from pytme_b200 import synthetic as syn
 
     rng = np.random.default_rng(sum(shape))
@@ -546,6 +547,7 @@ def test_tensor_core_ypass(torch_cuda, shape, score):
     target, _, _ = syn.make_tomogram(shape, tmpl, 4, rng, scale=0.5)
     rots = syn.random_rotation_matrices(37, rng)
     r = _scan(score, target, tmpl, mask, rots, precision="mixed", batch=32, ypass="tensor")
+    c = _scan(score, target, tmpl, mask, rots, precision="mixed", batch=32, ypass="tensor2")
     f = _scan(score, target, tmpl, mask, rots, precision="mixed", batch=32, ypass="fft")
     ref = O.scan(target, tmpl, rots, score, template_mask=mask)
     ref64 = O.scan(target, tmpl, rots, score, template_mask=mask, dtype=np.float64)
@@ -554,9 +556,11 @@ def test_tensor_core_ypass(torch_cuda, shape, score):
     assert np.abs(r[0] - ref["scores"]).max() <= tol
     assert np.abs(r[0] - ref64["scores"]).max() <= tol
     assert np.abs(r[0] - f[0]).max() <= tol
+    assert np.abs(c[0] - ref64["scores"]).max() <= tol
+    assert np.abs(c[0] - f[0]).max() <= tol
     # a blob template makes many rotations score alike: every voxel whose rotation differs
     # from the FP64 oracle's must be a tie within the path's error bound
-    for rot in (r[2], f[2]):
+    for rot in (r[2], c[2], f[2]):
         mism = np.argwhere(rot != ref64["rotations"])
         print(f"{shape} {score}: {len(mism)} argmax differences of {rot.size}")
         assert len(mism) <= 0.02 * rot.size
