@@ -76,6 +76,10 @@ def parse():
                     help="run --groups launch groups of the fused scan on a target of this "
                          "shape and exit (a small case for ncu captures; no timing, no JSON)")
     ap.add_argument("--groups", type=int, default=2)
+    ap.add_argument("--profile-score", choices=("FLCSphericalMask", "FLC", "CC"),
+                    default="FLCSphericalMask", help="score of --profile-case")
+    ap.add_argument("--profile-template", type=int, default=None,
+                    help="template edge of --profile-case (default: the bench's 48)")
     return ap.parse_args()
 
 
@@ -661,6 +665,8 @@ def run_ours(args):
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
+    if rank == 0:
+        result["peak_calling"] = time_peak_calling(smax)
     # end-to-end through the public API with host arrays (rank 0)
     if rank == 0 and not args.no_e2e:
         n_e2e = args.e2e_rotations or n_rot
@@ -695,7 +701,8 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_legs:
         torch.cuda.empty_cache()
         # config 4 runs in FP32: its filtered maps exceed 1e-4 in mixed precision
-        result["legs"] = {"config2": leg_config2(args.precision), "config4": leg_config4("fp32")}
+        result["legs"] = {"config2": leg_config2(args.precision, cpu=not args.no_cpu),
+                          "config4": leg_config4("fp32", cpu=not args.no_cpu)}
         torch.cuda.empty_cache()
     if rank == 0 and args.err_rotations > 0:
         # measured score error of the GPU map against the FP64 oracle on a rotation subset
@@ -737,7 +744,52 @@ def run_ours(args):
     return 0
 
 
-def leg_config2(precision="mixed", batch=64):
+def time_peak_calling(scores, num_peaks=1000, min_distance=24, reps=3):
+    """PeakCallerMaximumFilter (the reference's defaults for the analysis: 1,000 peaks,
+    minimum distance 24) on a device score map, timed from the call to the peaks on the
+    host (maximum filter, candidate gather and greedy distance filter on the device)."""
+    import torch
+
+    from pytme_b200.analyzer import PeakCallerMaximumFilter
+
+    pc = PeakCallerMaximumFilter(shape=tuple(scores.shape), num_peaks=num_peaks,
+                                 min_distance=min_distance)
+    eye = np.eye(3, dtype=np.float32)
+    st = pc(pc.init_state(), scores=scores, rotation_matrix=eye)  # warm-up
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        st = pc(pc.init_state(), scores=scores, rotation_matrix=eye)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    found = int(np.count_nonzero(np.asarray(st[0])[:, 0] >= 0))
+    return {"ms": 1000.0 * min(times), "num_peaks": num_peaks, "min_distance": min_distance,
+            "peaks_found": found, "map": list(scores.shape),
+            "what": "PeakCallerMaximumFilter on the device score map after the timed steps, "
+                    "best of %d calls" % reps}
+
+
+def oracle_sample_rate(target, tmpl, score, mask, rots, tf=None, gf=None, seconds=10.0):
+    """The oracle (the reference's loop restated on the host cores) on a bounded sample of
+    a workload: spawned workers, one pool call of about ``seconds``; rotations/s."""
+    from oracle import tm_oracle as O
+
+    w = _host_workers(3.0)
+    t0 = time.perf_counter()
+    O.scan_parallel(target, tmpl, rots[:w], score, template_mask=mask, template_filter=tf,
+                    target_filter=gf, n_workers=w)
+    per = time.perf_counter() - t0
+    n = int(min(len(rots), max(w, w * int(seconds / max(per, 1e-3)))))
+    t0 = time.perf_counter()
+    O.scan_parallel(target, tmpl, rots[:n], score, template_mask=mask, template_filter=tf,
+                    target_filter=gf, n_workers=w)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "rotations/s", "cores": w, "kind": "port",
+            "sample": f"the oracle over {n} rotations in {w} spawned workers ({dt:.1f} s)"}
+
+
+def leg_config2(precision="mixed", batch=64, cpu=True):
     """Filtered FLC at its workload (256x256x128, 32^3 template, CTF x wedge, the
     1,992-rotation 15-degree set, 64 rotations per launch group), device-timed, with the
     dominant stage's roofline."""
@@ -781,7 +833,12 @@ def leg_config2(precision="mixed", batch=64):
     alg = plan.stage_bytes(dom, batch)
     peak, peak_kind = measured_peaks()
     plan.close()
-    return {"workload": "FLC, 256x256x128 (40 copies, SNR 0.1), 32^3 template, dilated "
+    del smax, sarg
+    torch.cuda.empty_cache()
+    extra = {}
+    if cpu:
+        extra["cpu_baseline"] = oracle_sample_rate(target, tmpl, "FLC", mask, rots, tf, gf)
+    return {**extra, "workload": "FLC, 256x256x128 (40 copies, SNR 0.1), 32^3 template, dilated "
                         "threshold mask, CTF x wedge template filter, wedge target filter, "
                         "15-degree set (1992 rotations)",
             "value": len(rots) / (ms / 1000.0), "unit": "rotations/s", "rotations": len(rots),
@@ -793,7 +850,30 @@ def leg_config2(precision="mixed", batch=64):
             "stages_ms_per_group": {k: round(v[0] / max(v[1], 1), 3) for k, v in stages.items()}}
 
 
-def leg_config4(precision="mixed"):
+def _stage_roofline(plan, mats, batch, groups=2):
+    """Roofline of a plan's dominant stage: per-stage CUDA-event timing of ``groups``
+    launch groups after one warm-up group."""
+    import torch
+
+    shape = plan.fast_shape
+    smax = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    sarg = torch.full(shape, -1, dtype=torch.int32, device="cuda")
+    plan.run(mats[:batch], 0, smax, sarg)
+    plan.set_timing(True)
+    plan.run(mats[batch:(groups + 1) * batch], batch, smax, sarg)
+    timing = plan.get_timing()
+    plan.set_timing(False)
+    stages = {k: v for k, v in timing.items() if k != "prepare"}
+    dom = max(stages, key=lambda k: stages[k][0])
+    avg = stages[dom][0] / max(stages[dom][1], 1)
+    alg = plan.stage_bytes(dom, batch)
+    peak, peak_kind = measured_peaks()
+    return {"bound": "hbm", "kernel": dom, "achieved": alg / (avg / 1000) / 1e9, "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": alg / (avg / 1000) / 1e9 / peak,
+            "alg_bytes_per_launch": alg, "avg_launch_ms": avg}
+
+
+def leg_config4(precision="mixed", cpu=True):
     """The uneven batch (make_config4_jobs: 36 (tomogram, template) jobs, 12-degree set)
     through scan_batch with the autotuned rotation batch and CUDA-graph replay; the timed
     call includes every job's upload, target set-up, filters and result download."""
@@ -817,7 +897,38 @@ def leg_config4(precision="mixed"):
     dt = time.perf_counter() - t0
     n = sum(int(j.rotations.shape[0]) for j in jobs)
     assert len(out) == len(jobs)
-    return {"workload": "36 jobs: 12 tomograms 128^3..320x320x160 x templates 24^3/32^3/40^3, "
+    del out
+    # roofline and CPU baseline on the largest job (320x320x160 with the 40^3 template)
+    from pytme_b200.matching import fourier_padding, rigid_transform_matrices
+    from pytme_b200.scores import ScanPlan, _prepare_target
+
+    big = max(jobs, key=lambda j: j.target.size * j.template.size)
+    tf = np.asarray(big.template_filter(shape=big.template.shape,
+                                        return_real_fourier=True)["data"], np.float32)
+    gf = np.asarray(big.target_filter(shape=big.target.shape,
+                                      return_real_fourier=True)["data"], np.float32)
+    _, fast, _, _ = fourier_padding(big.target.shape, big.template.shape)
+    b = batches[(big.target.shape, big.template.shape)]
+    plan = ScanPlan(big.score, fast, big.template.shape, precision=precision, batch=b)
+    try:
+        plan.set_template(np.ascontiguousarray(big.template[::-1, ::-1, ::-1]),
+                          np.ascontiguousarray(big.mask[::-1, ::-1, ::-1]), tf)
+        plan.set_target(_prepare_target(big.target, tuple(fast), gf))
+        mats = torch.as_tensor(rigid_transform_matrices(
+            big.rotations, (np.asarray(big.template.shape) - 1) / 2), device="cuda")
+        roof = _stage_roofline(plan, mats, b)
+    finally:
+        plan.close()
+    torch.cuda.empty_cache()
+    extra = {"roofline": dict(roof, job=f"{'x'.join(map(str, big.target.shape))} target, "
+                                        f"{big.template.shape[0]}^3 template")}
+    if cpu:
+        c = oracle_sample_rate(big.target, big.template, big.score, big.mask, big.rotations,
+                               tf, gf)
+        c["unit"] = "job-rotations/s"
+        c["sample"] += " of the largest job"
+        extra["cpu_baseline"] = c
+    return {**extra, "workload": "36 jobs: 12 tomograms 128^3..320x320x160 x templates 24^3/32^3/40^3, "
                         "per-tomogram CTF (1.5-4.5 um) x wedge (50-65 deg), 12-degree set "
                         "(4344 rotations), FLCSphericalMask",
             "value": n / dt, "unit": "job-rotations/s", "job_rotations": n, "seconds": dt,
@@ -828,9 +939,9 @@ def leg_config4(precision="mixed"):
 
 
 def run_profile_case(args):
-    """A fixed amount of fused-scan work for profilers: FLCSphericalMask with a 48^3
-    blob template on an N(0,1) target of the given shape, --groups groups of --batch
-    rotations."""
+    """A fixed amount of fused-scan work for profilers: --profile-score (FLCSphericalMask
+    by default) with a blob template (48^3 by default) and its spherical mask on an N(0,1)
+    target of the given shape, --groups groups of --batch rotations."""
     import torch
 
     from pytme_b200 import synthetic as syn
@@ -838,17 +949,19 @@ def run_profile_case(args):
     from pytme_b200.scores import ScanPlan
 
     shape = tuple(int(x) for x in args.profile_case.split(","))
-    t = TSIZE
+    t = args.profile_template or TSIZE
     rng = np.random.default_rng(0)
     tmpl = syn.blob_template(t, rng, sigma=1.5 * t / 16, radius=5.0 * t / 16)
     mask = syn.spherical_mask((t,) * 3, t / 2, center=((t - 1) / 2,) * 3)
     target = rng.normal(size=shape).astype(np.float32)
-    plan = ScanPlan("FLCSphericalMask", shape, (t,) * 3, precision=args.precision,
+    plan = ScanPlan(args.profile_score, shape, (t,) * 3, precision=args.precision,
                     batch=args.batch)
-    plan.set_xpass(args.xpass)
-    plan.set_ypass(args.ypass)
-    plan.set_zpass(args.zpass)
-    plan.set_template(tmpl[::-1, ::-1, ::-1].copy(), mask[::-1, ::-1, ::-1].copy())
+    if args.profile_score != "FLC":
+        plan.set_xpass(args.xpass)
+        plan.set_ypass(args.ypass)
+        plan.set_zpass(args.zpass)
+    plan.set_template(tmpl[::-1, ::-1, ::-1].copy(),
+                      None if args.profile_score == "CC" else mask[::-1, ::-1, ::-1].copy())
     plan.set_target(torch.as_tensor(target, device="cuda"))
     rots = syn.super_fibonacci_rotations(args.batch * args.groups)
     m = torch.as_tensor(rigid_transform_matrices(rots, ((t - 1) / 2,) * 3), device="cuda")
