@@ -697,14 +697,14 @@ zpass_kernel(const HT* __restrict__ H, int B, int64_t rows, int n2, int hp, int 
 // K4'' (FLC): c2r of the numerator and both statistics rows, then
 // norm_scores (tme/backends/npfftw_backend.py:537-587) in double precision with the
 // rotation's own n_obs = sum(rotated mask), and the strict-> update.
-template <int M>
-__device__ __forceinline__ void c2r_rows(float2* raw, float2* buf, const float2* tw2, int nrows,
+template <int M, typename RT = float2>
+__device__ __forceinline__ void c2r_rows(const RT* raw, float2* buf, const float2* tw2, int nrows,
                                          int n2, int hp, const LinePlan& pm, int tid) {
   const int m = n2 / 2;
   for (int e = tid; e < nrows * m; e += kThreads) {
     int r = e / m, k = e % m;
-    const float2* xr = raw + (int64_t)r * hp;
-    float2 a = xr[k], c = xr[m - k];
+    const RT* xr = raw + (int64_t)r * hp;
+    float2 a = Store<RT>::load(xr + k), c = Store<RT>::load(xr + (m - k));
     if (k == 0) { a.y = 0.f; c.y = 0.f; }
     float2 cc = fft::cconj(c);
     float2 E = fft::cadd(a, cc);
@@ -718,6 +718,10 @@ __device__ __forceinline__ void c2r_rows(float2* raw, float2* buf, const float2*
     fft::fft_lines<1, kMaxE, false>(buf, pm, nrows, m, 1, tw2, n2, tid, kThreads);
 }
 
+// Phases of the FLC z pass: for every rotation the local mean (Hm), the local mean
+// square (Hm2) and the numerator (H) of a block of rows, each a c2r along z. The block's
+// rows of the next phase are copied (cp.async, 16-byte pieces of one contiguous range)
+// into the second of two raw buffers while the current phase is transformed.
 template <typename HT, int M = 0>
 __global__ void __launch_bounds__(kThreads, 1)
 zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
@@ -728,10 +732,11 @@ zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
                  const int32_t* __restrict__ first_dev) {
   if (first_dev) first_index = *first_dev;
   extern __shared__ float4 smem_raw[];
-  const int m = n2 / 2;
   float2* tw2 = reinterpret_cast<float2*>(smem_raw);
-  float2* raw = tw2 + n2;
-  float2* buf = raw + (int64_t)R * hp;
+  float2* rawb[2];
+  rawb[0] = tw2 + (n2 + 1) / 2 * 2;  // 16-byte aligned
+  rawb[1] = rawb[0] + (int64_t)R * hp;
+  float2* buf = rawb[1] + (int64_t)R * hp;
   const int tid = threadIdx.x;
   const int64_t row0 = (int64_t)blockIdx.x * R;
   const int nrows = (int)min((int64_t)R, rows - row0);
@@ -744,47 +749,61 @@ zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
 #pragma unroll
   for (int c = 0; c < kMaxV; ++c) { best[c] = -INFINITY; arg[c] = -1; }
   const float* outv = reinterpret_cast<const float*>(buf);
-  for (int b = 0; b < B; ++b) {
+  // phase p: rotation p / 3; 0 mean (Hm), 1 mean square (Hm2), 2 numerator (H)
+  auto issue = [&](int p) {
+    if (p < 3 * B) {
+      const int b = p / 3, kind = p - 3 * b;
+      const char* src = kind == 0   ? reinterpret_cast<const char*>(Hm + (int64_t)b * S + row0 * hp)
+                        : kind == 1 ? reinterpret_cast<const char*>(Hm2 + (int64_t)b * S + row0 * hp)
+                                    : reinterpret_cast<const char*>(Ht + (int64_t)b * S + row0 * hp);
+      const int nbytes = nrows * hp * (kind == 2 ? (int)sizeof(HT) : (int)sizeof(float2));
+      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(rawb[p & 1]);
+      for (int o = tid * 16; o < nbytes; o += kThreads * 16)
+        tc::cp_async16(dst + (uint32_t)o, src + o, 16u);
+    }
+    cp_async_commit();
+  };
+  issue(0);
+  for (int p = 0; p < 3 * B; ++p) {
+    const int b = p / 3, kind = p - 3 * b;
+    // the other buffer was last read by phase p - 1, which ended with a block barrier
+    issue(p + 1);
+    cp_async_wait<1>();
+    __syncthreads();  // phase p's rows landed for every thread
     const double nobs = stats[b * 4 + 2];
-    // local mean
-    const float2* src = Hm + (int64_t)b * S + row0 * hp;
-    for (int e = tid; e < nrows * hp; e += kThreads) raw[e] = src[e];
-    __syncthreads();
-    c2r_rows<M>(raw, buf, tw2, nrows, n2, hp, pm, tid);
+    if (kind == 2)
+      c2r_rows<M, HT>(reinterpret_cast<const HT*>(rawb[p & 1]), buf, tw2, nrows, n2, hp, pm, tid);
+    else
+      c2r_rows<M, float2>(rawb[p & 1], buf, tw2, nrows, n2, hp, pm, tid);
+    if (kind == 0) {
+      // local mean
 #pragma unroll
-    for (int c = 0; c < kMaxV; ++c) {
-      int v = tid + c * kThreads;
-      e1[c] = v < nout ? (double)outv[v] * (double)scale_m / nobs : 0.0;
-    }
-    __syncthreads();
-    // local mean square -> variance
-    src = Hm2 + (int64_t)b * S + row0 * hp;
-    for (int e = tid; e < nrows * hp; e += kThreads) raw[e] = src[e];
-    __syncthreads();
-    c2r_rows<M>(raw, buf, tw2, nrows, n2, hp, pm, tid);
-#pragma unroll
-    for (int c = 0; c < kMaxV; ++c) {
-      int v = tid + c * kThreads;
-      if (v < nout) {
-        double e2 = (double)outv[v] * (double)scale_m / nobs;
-        double var = e2 - e1[c] * e1[c];
-        double sd = sqrt(var > 0 ? var : 0.0);
-        if (sd < eps) sd = 1.0;
-        e1[c] = sd * nobs;  // reuse as the denominator
+      for (int c = 0; c < kMaxV; ++c) {
+        int v = tid + c * kThreads;
+        e1[c] = v < nout ? (double)outv[v] * (double)scale_m / nobs : 0.0;
       }
-    }
-    __syncthreads();
-    // numerator
-    const HT* st = Ht + (int64_t)b * S + row0 * hp;
-    for (int e = tid; e < nrows * hp; e += kThreads) raw[e] = Store<HT>::load(st + e);
-    __syncthreads();
-    c2r_rows<M>(raw, buf, tw2, nrows, n2, hp, pm, tid);
+    } else if (kind == 1) {
+      // local mean square -> variance -> denominator
 #pragma unroll
-    for (int c = 0; c < kMaxV; ++c) {
-      int v = tid + c * kThreads;
-      if (v < nout) {
-        float sc = (float)((double)outv[v] * (double)scale_t / e1[c]);
-        if (sc > best[c]) { best[c] = sc; arg[c] = first_index + b; }
+      for (int c = 0; c < kMaxV; ++c) {
+        int v = tid + c * kThreads;
+        if (v < nout) {
+          double e2 = (double)outv[v] * (double)scale_m / nobs;
+          double var = e2 - e1[c] * e1[c];
+          double sd = sqrt(var > 0 ? var : 0.0);
+          if (sd < eps) sd = 1.0;
+          e1[c] = sd * nobs;  // reuse as the denominator
+        }
+      }
+    } else {
+      // numerator
+#pragma unroll
+      for (int c = 0; c < kMaxV; ++c) {
+        int v = tid + c * kThreads;
+        if (v < nout) {
+          float sc = (float)((double)outv[v] * (double)scale_t / e1[c]);
+          if (sc > best[c]) { best[c] = sc; arg[c] = first_index + b; }
+        }
       }
     }
     __syncthreads();
@@ -1572,7 +1591,10 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     s->smem1 = sizeof(float2) * (s->n1 + s->n2 + (size_t)s->n1 * s->W1) + sizeof(float) * s->t1 * s->t2;
     s->smem2 = sizeof(float2) * (s->n0 + (size_t)s->n0 * s->W2);
     s->smem3 = sizeof(float2) * (s->n1 + (size_t)s->n1 * s->W3);
-    s->smem4 = sizeof(float2) * (s->n2 + (size_t)s->R4 * s->hp + (size_t)s->R4 * (s->n2 / 2));
+    // twiddles (padded to 16 bytes), two raw row buffers (the FLC z pass stages the next
+    // phase in the second), the c2r buffer
+    s->smem4 = sizeof(float2) * ((s->n2 + 1) / 2 * 2 + 2 * (size_t)s->R4 * s->hp +
+                                 (size_t)s->R4 * (s->n2 / 2));
     size_t mx = std::max(std::max(s->smem1, s->smem2), std::max(s->smem3, s->smem4));
     if (mx > 200 * 1024) {
       set_error("scan_create: shared-memory tile of %zu bytes exceeds the limit", mx);

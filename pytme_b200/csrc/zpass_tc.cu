@@ -361,6 +361,9 @@ __device__ __forceinline__ void mbar_track_cp_async(uint64_t* bar) {
 // an even number of stages a stage always belongs to the same group.
 constexpr int kEoEpi = 128;
 constexpr int kEoGroup0 = 192, kEoGroup1 = 160;
+// 16-byte pieces per loader thread of the segment-layout path: kEoN rows x 2 halves x at
+// most 16 segments (h2 <= 128) over the smaller group
+constexpr int kEoSegPieces = (kEoN * 2 * 16 + kEoGroup1 - 1) / kEoGroup1;
 static_assert(kEoS % 2 == 0, "stages alternate between the two loader groups");
 __device__ __forceinline__ bool eo_epilogue_warp(int w) { return w >= 4 && w < 8; }
 __device__ __forceinline__ int eo_loader_group(int w) { return w <= 10 ? 0 : 1; }
@@ -446,9 +449,27 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
         cp_async16(smem_u32(As) + 16u * i, Ag + 8 * (size_t)i, 16);
     if constexpr (SEG) {
       // piece i -> (operand row n = i / (2 nseg), segment c, half part = Re/Im): the
-      // lanes of a warp take 16 consecutive 16-byte pieces of one H row
+      // lanes of a warp take 16 consecutive 16-byte pieces of one H row. The mapping is
+      // the same for every block, so each thread packs its pieces once: bits 0-10 operand
+      // offset (16-byte units), 11-15 rotation, 16 row in the block, 17-23 word offset
+      // 8 c + 4 part in the H row, 24-27 values k < h2 in the half, 28 present.
       const int nseg = hp / 8;
       const int npiece = kEoN * nseg * 2;
+      uint32_t pd[kEoSegPieces];
+#pragma unroll
+      for (int m = 0; m < kEoSegPieces; ++m) {
+        const int i = lt + m * gsz;
+        uint32_t d = 0u;
+        if (i < npiece) {
+          const int part = i & 1, rest = i >> 1;
+          const int c = rest % nseg, n = rest / nseg;
+          const int valid = min(8, max(0, h2 - 8 * c));
+          d = ((uint32_t)kmajor16(n, part * Kp + 8 * c, K2) >> 3) |
+              ((uint32_t)(n & (kZRot - 1)) << 11) | ((uint32_t)(n >> 5) << 16) |
+              ((uint32_t)(8 * c + 4 * part) << 17) | ((uint32_t)valid << 24) | (1u << 28);
+        }
+        pd[m] = d;
+      }
       for (int64_t j = grp; j < mine; j += 2) {
         const int sidx = (int)(j % kEoS);
         const uint32_t u = (uint32_t)(j / kEoS);
@@ -459,16 +480,17 @@ zpass_eo_kernel(const __half2* __restrict__ H, int nb, int64_t rows, int n2, int
         if (*fail) break;
         const int64_t row0 = ((int64_t)blockIdx.x + j * gridDim.x) * kEoRows;
         const uint32_t bj = smem_u32(Bs + (size_t)sidx * kEoN * K2);
-        for (int i = lt; i < npiece; i += gsz) {
-          const int part = i & 1, rest = i >> 1;
-          const int c = rest % nseg, n = rest / nseg;
-          const int r = n >> 5, b = n & (kZRot - 1);
-          const int64_t row = row0 + r;
-          const int valid = min(8, max(0, h2 - 8 * c));  // values k < h2 in the half
+#pragma unroll
+        for (int m = 0; m < kEoSegPieces; ++m) {
+          const uint32_t d = pd[m];
+          if (!(d >> 28)) continue;
+          const int b = (int)((d >> 11) & 31u);
+          const int64_t row = row0 + (int64_t)((d >> 16) & 1u);
+          const uint32_t valid = (d >> 24) & 15u;  // values k < h2 in the half
           const bool live = b < nb && row < rows && valid > 0;
-          const __half2* src = live ? H + (int64_t)b * SH + row * hp + 8 * c + 4 * part : H;
-          cp_async16(bj + 2u * (uint32_t)kmajor16(n, part * Kp + 8 * c, K2), src,
-                     live ? 2u * (uint32_t)valid : 0u);
+          const __half2* src =
+              live ? H + (int64_t)b * SH + row * hp + (int64_t)((d >> 17) & 127u) : H;
+          cp_async16(bj + 16u * (d & 2047u), src, live ? 2u * valid : 0u);
         }
         if (j >= kEoS && !mbar_wait_n(smem_u32(tempty + sidx), (u - 1) & 1u, wi)) {
           *fail = 1;
