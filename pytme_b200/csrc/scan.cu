@@ -295,11 +295,11 @@ __device__ __forceinline__ void dif_rest(float2 (&v)[8], float2* sm, const float
 }
 
 // K1': template rows -> G. grid (ceil(h2/W), t0, B); N = n1.
-template <int N, int W>
+template <int N, int W, typename GT = float2>
 __global__ void __launch_bounds__(N / 8 * W, 1)
 tmpl_zy_reg_kernel(const float* __restrict__ tmpl, int t0, int t1, int t2, int n2, int h2,
                    const float2* __restrict__ tw1_g, const float2* __restrict__ tw2_g,
-                   float2* __restrict__ G) {
+                   GT* __restrict__ G) {
   constexpr int T = N / 8;
   constexpr int NT = T * W;
   extern __shared__ float4 smem_raw[];
@@ -338,14 +338,14 @@ tmpl_zy_reg_kernel(const float* __restrict__ tmpl, int t0, int t1, int t2, int n
   else colfft::dif_stage_regs<N, 0, -1>(v, t, tw1);
   dif_rest<N, W, -1>(v, sm, tw1, l, t);
   if (k2 < h2) {
-    float2* dst = G + ((int64_t)b * t0 + x) * N * h2;
+    GT* dst = G + ((int64_t)b * t0 + x) * N * h2;
     constexpr int R = colfft::stage_radix(N, colfft::num_stages(N) - 1);
 #pragma unroll
     for (int i = 0; i < 8 / R; ++i)
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const int k1 = colfft::out_index<N>(t, i, r);
-        dst[(int64_t)k1 * h2 + k2] = v[i * R + r];
+        Store<GT>::store(dst + (int64_t)k1 * h2 + k2, v[i * R + r]);
       }
   }
 }
@@ -1141,8 +1141,9 @@ static bool seg_layout(const Scan* s) {
   return s->half && s->ztc && s->zcfg.eo && (s->ytc || s->reg1);
 }
 
-// Whether the warp-specialised tensor-core x pass writes every launch group, so it can store
-// H rows as segments in the y pass's stage-1 order.
+// Whether the warp-specialised tensor-core x pass runs every launch group: it can then read
+// the template spectra G as FP16 and store H rows as segments in the y pass's stage-1
+// order.
 static bool x_writes_stage1(const Scan* s) {
   return s->half && s->xtc && s->xcfg.ws && s->B <= s->xcfg.ws_NB && s->hp % 8 == 0 &&
          s->d.score != TM_SCORE_FLC;
@@ -1269,6 +1270,7 @@ static void set_reg_attrs(size_t zy_smem) {
   cudaFuncSetAttribute(ypass_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
   cudaFuncSetAttribute(ypass_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
   cudaFuncSetAttribute(tmpl_zy_reg_kernel<N, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
+  cudaFuncSetAttribute(tmpl_zy_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
   cudaFuncSetAttribute(xpass_flc_reg_kernel<N, W, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
   cudaFuncSetAttribute(xpass_flc_reg_kernel<N, W, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin_max());
 }
@@ -1286,13 +1288,18 @@ static void set_reg_attrs_n(int n, size_t zy_smem) {
 
 template <int N>
 static void launch_tmpl_reg(Scan* s, int nb, cudaStream_t st, const float* in = nullptr,
-                            float2* out = nullptr) {
+                            float2* out = nullptr, bool half_g = false) {
   constexpr int W = reg_lines<N>();
   dim3 g(ceil_div(s->h2, W), s->t0, nb);
   size_t smem = reg_smem_bytes<N>(s->n2, s->t1, s->t2, true);
-  tmpl_zy_reg_kernel<N, W><<<g, N / 8 * W, smem, st>>>(in ? in : s->rot_t, s->t0, s->t1, s->t2,
-                                                       s->n2, s->h2, s->tw1, s->tw2,
-                                                       out ? out : s->G);
+  if (half_g)
+    tmpl_zy_reg_kernel<N, W, __half2><<<g, N / 8 * W, smem, st>>>(
+        in ? in : s->rot_t, s->t0, s->t1, s->t2, s->n2, s->h2, s->tw1, s->tw2,
+        reinterpret_cast<__half2*>(out ? out : s->G));
+  else
+    tmpl_zy_reg_kernel<N, W><<<g, N / 8 * W, smem, st>>>(in ? in : s->rot_t, s->t0, s->t1, s->t2,
+                                                         s->n2, s->h2, s->tw1, s->tw2,
+                                                         out ? out : s->G);
 }
 
 template <int N, typename HT>
@@ -1334,9 +1341,12 @@ template <typename HT>
 static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr,
                                cudaStream_t stream) {
   const bool flc = s->d.score == TM_SCORE_FLC;
+  // the warp-specialised tensor-core x pass reads the template spectra G as FP16 (it
+  // rounds them to FP16 for its MMAs anyway), so the template pass writes them so
+  const bool half_g = s->reg1 && x_writes_stage1(s);
   tmr.begin();
   if (s->reg1) {
-    TM_DISPATCH_N(s->n1, (launch_tmpl_reg<NN>(s, nb, stream)));
+    TM_DISPATCH_N(s->n1, (launch_tmpl_reg<NN>(s, nb, stream, nullptr, nullptr, half_g)));
     if (flc) TM_DISPATCH_N(s->n1, (launch_tmpl_reg<NN>(s, nb, stream, s->rot_m, s->Gm)));
   } else {
     dim3 g1(ceil_div(s->h2, s->W1), s->t0, nb);
@@ -1353,7 +1363,7 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
     const bool s1 = y_stage1_tc(s);
     TM_TRY(xcorr_tc_run(s->xcfg, s->G, s->ctarget, nb, s->t0, s->n0, s->n1, s->h2, s->hp, hs,
                         H, std::is_same<HT, __half2>::value, s->tc_err, stream,
-                        s->wait_iters, s1, s1 ? s->n1 / 16 : 0));
+                        s->wait_iters, s1, s1 ? s->n1 / 16 : 0, half_g));
   } else if (s->reg0) {
     TM_DISPATCH_N(s->n0, (launch_xpass_reg<NN, HT>(s, nb, hs, H, stream)));
   } else {

@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
 xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int nb, int NB,
                 int t0, int n0, int n1, int h2, int hp, float scale,
                 __half2* __restrict__ H, int* __restrict__ err, uint32_t wait_iters,
-                int seg, int rowq) {
+                int seg, int rowq, int ghalf) {
   constexpr int t0p = 8 * NXC;
   const uint32_t wi = wait_iters ? wait_iters : kWaitIters;  // data waits
   constexpr uint32_t kAccCols = 16u * R;               // one fill
@@ -297,16 +297,30 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
         const int xc = rest % nxc, n = rest / nxc;
         const bool live = n < nb && k20 + w < h2;
         uint32_t re[4], im[4];
+        if (ghalf) {
+          // G already FP16 (Re, Im) words: pair the x and x + 1 halves
+          const uint32_t* Gh = reinterpret_cast<const uint32_t*>(G);
 #pragma unroll
-        for (int q = 0; q < 8; q += 2) {
-          const int x = xc * 8 + q;
-          float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
-          if (live && x < t0) a = G[((int64_t)n * t0 + x) * row + col0 + w];
-          if (live && x + 1 < t0) b = G[((int64_t)n * t0 + x + 1) * row + col0 + w];
-          const __half2 r2 = __floats2half2_rn(a.x, b.x);
-          const __half2 i2 = __floats2half2_rn(a.y, b.y);
-          re[q >> 1] = *reinterpret_cast<const uint32_t*>(&r2);
-          im[q >> 1] = *reinterpret_cast<const uint32_t*>(&i2);
+          for (int q = 0; q < 8; q += 2) {
+            const int x = xc * 8 + q;
+            uint32_t a = 0u, b = 0u;
+            if (live && x < t0) a = __ldg(Gh + ((int64_t)n * t0 + x) * row + col0 + w);
+            if (live && x + 1 < t0) b = __ldg(Gh + ((int64_t)n * t0 + x + 1) * row + col0 + w);
+            re[q >> 1] = __byte_perm(a, b, 0x5410);
+            im[q >> 1] = __byte_perm(a, b, 0x7632);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 8; q += 2) {
+            const int x = xc * 8 + q;
+            float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+            if (live && x < t0) a = G[((int64_t)n * t0 + x) * row + col0 + w];
+            if (live && x + 1 < t0) b = G[((int64_t)n * t0 + x + 1) * row + col0 + w];
+            const __half2 r2 = __floats2half2_rn(a.x, b.x);
+            const __half2 i2 = __floats2half2_rn(a.y, b.y);
+            re[q >> 1] = *reinterpret_cast<const uint32_t*>(&r2);
+            im[q >> 1] = *reinterpret_cast<const uint32_t*>(&i2);
+          }
         }
         uint16_t* bw = bb + (size_t)w * L.b_stride;
         *reinterpret_cast<uint4*>(bw + kmajor16(n, xc * 8, K)) =
@@ -495,7 +509,7 @@ int xcorr_ws_config(int n0, int t0, int nb, XcorrTcConfig* cfg) {
 
 int xcorr_ws_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int nb, int t0,
                  int n0, int n1, int h2, int hp, float scale, __half2* H, int* err,
-                 cudaStream_t stream, uint32_t wait_iters, bool seg, int rowq) {
+                 cudaStream_t stream, uint32_t wait_iters, bool seg, int rowq, bool g_half) {
   // 32-byte row segments: pitch a multiple of 8 complex values, aligned base
   TM_REQUIRE(cfg.ws && nb <= cfg.ws_NB && hp % 8 == 0 && hp >= h2 &&
                  reinterpret_cast<uintptr_t>(H) % 32 == 0 &&
@@ -514,7 +528,8 @@ int xcorr_ws_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int
     default: TM_REQUIRE(false, "xcorr_ws_run: t0p %d", cfg.ws_t0p);
   }
   fn<<<grid, kWsThreads, cfg.ws_smem, stream>>>(G, C, nb, cfg.ws_NB, t0, n0, n1, h2, hp, scale,
-                                               H, err, wait_iters, seg ? 1 : 0, rowq);
+                                               H, err, wait_iters, seg ? 1 : 0, rowq,
+                                               g_half ? 1 : 0);
   return check_launch("xcorr_ws_kernel");
 }
 
