@@ -435,9 +435,10 @@ def cpu_scan_loop(target, tmpl, mask, n_rotations, prefer_reference=True):
 
 
 def time_cpu_loop(loop, rots, steps, warmup, min_seconds):
-    """``warmup`` steps of one rotation per worker, then ``steps`` timed steps of r
-    rotations per worker, r sized from the warm-up so the timed loop lasts at least
-    ``min_seconds``. Returns (rotations/s, ms per step, rotations timed, r)."""
+    """``warmup`` steps of one rotation per worker (the last of them, when there are two or
+    more, of two), then ``steps`` timed steps of r rotations per worker, r sized from the
+    warm-up's cost per added rotation so the timed loop lasts at least ``min_seconds``.
+    Returns (rotations/s, ms per step, rotations timed, r)."""
     w = loop.n_jobs
     pos = 0
 
@@ -450,14 +451,21 @@ def time_cpu_loop(loop, rots, steps, warmup, min_seconds):
         return out
 
     t_warm = []
-    for _ in range(max(1, warmup)):
+    nw = max(1, warmup)
+    for i in range(nw):
         t0 = time.perf_counter()
-        loop.step(chunks(1))
+        loop.step(chunks(2 if (nw >= 2 and i == nw - 1) else 1))
         t_warm.append(time.perf_counter() - t0)
-    # the last warm-up step is the closest to steady state (the first ones also plan the
-    # FFTs and fault in the workers' memory); 15 % margin on the target duration
-    per_rot = t_warm[-1]
-    r = int(min(16, max(1, np.ceil(1.15 * min_seconds / max(steps, 1) / per_rot))))
+    # a step costs a fixed part (dispatch, analyzer merge) plus a part per rotation and
+    # worker: the last two warm-up steps (one and two rotations per worker; the first ones
+    # also plan the FFTs and fault in the workers' memory) give both; 15 % margin
+    if nw >= 2:
+        per_rot = max(t_warm[-1] - t_warm[-2], 0.25 * t_warm[-2])
+        fixed = max(t_warm[-2] - per_rot, 0.0)
+    else:
+        per_rot, fixed = t_warm[-1], 0.0
+    target = 1.15 * min_seconds / max(steps, 1)
+    r = int(min(16, max(1, np.ceil((target - fixed) / per_rot))))
     times = []
     for _ in range(steps):
         t0 = time.perf_counter()
