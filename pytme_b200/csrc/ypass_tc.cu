@@ -121,6 +121,22 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
+// v * w16^k, w16 = exp(+2 pi i / 16), for the products k = a0 y0 (a0, y0 < 4) of the
+// radix-16 stage, with the twiddles as constants: cos(pi/8), sin(pi/8), sqrt(1/2).
+__device__ __forceinline__ float2 tw16(float2 v, int k) {
+  constexpr float c8 = 0.923879532511286756f, s8 = 0.382683432365089772f;
+  constexpr float r2 = 0.707106781186547524f;
+  switch (k) {
+    case 0: return v;
+    case 1: return make_float2(v.x * c8 - v.y * s8, v.x * s8 + v.y * c8);
+    case 2: return make_float2((v.x - v.y) * r2, (v.x + v.y) * r2);
+    case 3: return make_float2(v.x * s8 - v.y * c8, v.x * c8 + v.y * s8);
+    case 4: return make_float2(-v.y, v.x);
+    case 6: return make_float2(-(v.x + v.y) * r2, (v.x - v.y) * r2);
+    default: return make_float2(-v.x * c8 + v.y * s8, -v.x * s8 - v.y * c8);  // 9
+  }
+}
+
 __device__ __forceinline__ uint32_t pack_half2(float re, float im) {
   const __half2 h = __floats2half2_rn(re, im);
   return *reinterpret_cast<const uint32_t*>(&h);
@@ -423,12 +439,11 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
     const int t = tid - 128;
     const int c = t >> 3, k2 = t & 7;
     // twiddles w^(c y1) of the column and w16^k, k <= 9, of the radix-16 FFT
-    float wr[16], wi[16], tr16[10], ti16[10];
+    float wr[16], wi[16];
 #pragma unroll
     for (int y1 = 0; y1 < 16; ++y1)
       sincospif(2.0f * (float)(c * y1) / (float)L::N1, &wi[y1], &wr[y1]);
 #pragma unroll
-    for (int k = 0; k < 10; ++k) sincospif((float)k / 8.0f, &ti16[k], &tr16[k]);
     // staging: X[k1][k2] at byte 32 k1 + 4 k2 (banks 8c + k2: conflict-free per warp);
     // operand: row (y1, k2), K position 2c (head) at byte
     // y1 * 64Q + 128 (c >> 2) + 16 k2 + 4 (c & 3), the tail 32Q bytes further
@@ -461,7 +476,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
 #pragma unroll
         for (int y0 = 0; y0 < 4; ++y0) {
           const int k = a0 * y0;
-          v[y0][a0] = k == 0 ? u[y0] : fft::cmul(u[y0], make_float2(tr16[k], ti16[k]));
+          v[y0][a0] = tw16(u[y0], k);
         }
       }
 #pragma unroll
