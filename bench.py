@@ -670,6 +670,8 @@ def run_ours(args):
             "plain": {"value": plain_rate, "unit": "rotations/s", "rotations": args.plain_rotations,
                       "path": "fp32, one rotation at a time, full cuFFT r2c/c2r"},
             "vs_plain": value / world / plain_rate,
+            "model_roofline": model_roofline(fast, args.precision, args.batch, value,
+                                             measured_peaks()),
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
@@ -750,6 +752,25 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def model_roofline(fast, precision, batch, rate, peak):
+    """Whole-scan HBM fraction by the FFT I/O model of the fused FLCSphericalMask / CC path:
+    per rotation 7 passes over the S-element product spectrum of e bytes per value (two HBM
+    passes per full-size FFT, elementwise stages fused, the target spectrum read once)
+    plus the per-voxel state (max, argmax, the d-byte denominator and the state write) once
+    per launch group of B rotations: 7 S e + (d + 16) N / B bytes."""
+    n0, n1, n2 = (int(x) for x in fast)
+    N = n0 * n1 * n2
+    S = n0 * n1 * (n2 // 2 + 1)
+    e = 4 if precision == "mixed" else 8
+    d = 4  # the inverse denominator is stored as float32
+    per_rot = 7 * S * e + (d + 16) * N / batch
+    gbs = per_rot * rate / 1e9
+    return {"bytes_per_rotation": per_rot, "achieved": gbs, "peak": peak[0],
+            "peak_kind": peak[1], "unit": "GB/s", "frac": gbs / peak[0],
+            "model": "7 S e + (d + 16) N / B bytes per rotation (two HBM passes per "
+                     "full-size FFT, fused elementwise stages, state once per launch group)"}
 
 
 def time_peak_calling(scores, num_peaks=1000, min_distance=24, reps=3):
