@@ -31,7 +31,7 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 OUT_DIR = os.path.join(HERE, "_ref")
-BASELINE = os.path.join(ROOT, "baseline", "_ref")
+INSTALL_DIR = os.path.join(ROOT, "baseline", "_ref")
 WHEELHOUSE = "/opt/wheelhouse"
 
 
@@ -53,23 +53,23 @@ def build(reference: str) -> str:
 
 def install_baseline(reference: str, force: bool = False) -> str:
     """Offline install of the reference package into baseline/_ref (see module doc)."""
-    pkg = os.path.join(BASELINE, "tme")
+    pkg = os.path.join(INSTALL_DIR, "tme")
     if os.path.isdir(pkg) and not force:
-        return BASELINE
+        return INSTALL_DIR
     if not os.path.isdir(os.path.join(reference, "tme")):
         raise FileNotFoundError(os.path.join(reference, "tme"))
     tmp = tempfile.mkdtemp(prefix="pytme_ref_src_")
     src = os.path.join(tmp, "src")
     shutil.copytree(reference, src, ignore=shutil.ignore_patterns(".git"))
     cmd = [sys.executable, "-m", "pip", "install", "--no-index", "--no-build-isolation",
-           "--no-deps", "--upgrade", "--target", BASELINE, src]
+           "--no-deps", "--upgrade", "--target", INSTALL_DIR, src]
     if os.path.isdir(WHEELHOUSE):
         cmd[4:4] = ["--find-links", WHEELHOUSE]
     subprocess.check_call(cmd, stdout=subprocess.DEVNULL)
     ext = os.path.join(pkg, "extensions" + sysconfig.get_config_var("EXT_SUFFIX"))
     _compile_bindings(os.path.join(src, "tme", "external", "bindings.cpp"), ext)
     shutil.rmtree(tmp, ignore_errors=True)
-    return BASELINE
+    return INSTALL_DIR
 
 
 if __name__ == "__main__":
