@@ -718,10 +718,11 @@ __device__ __forceinline__ void c2r_rows(const RT* raw, float2* buf, const float
     fft::fft_lines<1, kMaxE, false>(buf, pm, nrows, m, 1, tw2, n2, tid, kThreads);
 }
 
-// Phases of the FLC z pass: for every rotation the local mean (Hm), the local mean
-// square (Hm2) and the numerator (H) of a block of rows, each a c2r along z. The block's
-// rows of the next phase are copied (cp.async, 16-byte pieces of one contiguous range)
-// into the second of two raw buffers while the current phase is transformed.
+// The FLC z pass transforms, for every rotation, the local mean (Hm), the local mean
+// square (Hm2) and the numerator (H) of a block of R rows as one batch of 3 R lines (one
+// set of barriers per rotation). The next rotation's rows are copied (cp.async, 16-byte
+// pieces of three contiguous ranges) into the second of two raw buffer sets while the
+// current rotation is transformed.
 template <typename HT, int M = 0>
 __global__ void __launch_bounds__(kThreads, 1)
 zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
@@ -732,78 +733,88 @@ zpass_flc_kernel(const HT* __restrict__ Ht, const float2* __restrict__ Hm,
                  const int32_t* __restrict__ first_dev) {
   if (first_dev) first_index = *first_dev;
   extern __shared__ float4 smem_raw[];
+  const int m = n2 / 2;
   float2* tw2 = reinterpret_cast<float2*>(smem_raw);
-  float2* rawb[2];
-  rawb[0] = tw2 + (n2 + 1) / 2 * 2;  // 16-byte aligned
-  rawb[1] = rawb[0] + (int64_t)R * hp;
-  float2* buf = rawb[1] + (int64_t)R * hp;
+  // raw set q, part k (0 Hm, 1 Hm2, 2 H): R rows of hp values (float2 room for each)
+  float2* raw0 = tw2 + (n2 + 1) / 2 * 2;  // 16-byte aligned
+  const int64_t part = (int64_t)R * hp;
+  float2* buf = raw0 + 6 * part;
   const int tid = threadIdx.x;
   const int64_t row0 = (int64_t)blockIdx.x * R;
   const int nrows = (int)min((int64_t)R, rows - row0);
   for (int i = tid; i < n2; i += kThreads) tw2[i] = tw2_g[i];
   const int nout = nrows * n2;
   const int64_t vox0 = row0 * n2;
+  const int set = R * n2;  // floats between the three parts' outputs in buf
   float best[kMaxV];
   int32_t arg[kMaxV];
-  double e1[kMaxV];
 #pragma unroll
   for (int c = 0; c < kMaxV; ++c) { best[c] = -INFINITY; arg[c] = -1; }
   const float* outv = reinterpret_cast<const float*>(buf);
-  // phase p: rotation p / 3; 0 mean (Hm), 1 mean square (Hm2), 2 numerator (H)
-  auto issue = [&](int p) {
-    if (p < 3 * B) {
-      const int b = p / 3, kind = p - 3 * b;
-      const char* src = kind == 0   ? reinterpret_cast<const char*>(Hm + (int64_t)b * S + row0 * hp)
-                        : kind == 1 ? reinterpret_cast<const char*>(Hm2 + (int64_t)b * S + row0 * hp)
-                                    : reinterpret_cast<const char*>(Ht + (int64_t)b * S + row0 * hp);
-      const int nbytes = nrows * hp * (kind == 2 ? (int)sizeof(HT) : (int)sizeof(float2));
-      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(rawb[p & 1]);
-      for (int o = tid * 16; o < nbytes; o += kThreads * 16)
-        tc::cp_async16(dst + (uint32_t)o, src + o, 16u);
+  auto issue = [&](int b) {
+    if (b < B) {
+      const uint32_t dst0 = (uint32_t)__cvta_generic_to_shared(raw0 + (b & 1) * 3 * part);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const char* src = k == 0   ? reinterpret_cast<const char*>(Hm + (int64_t)b * S + row0 * hp)
+                          : k == 1 ? reinterpret_cast<const char*>(Hm2 + (int64_t)b * S + row0 * hp)
+                                   : reinterpret_cast<const char*>(Ht + (int64_t)b * S + row0 * hp);
+        const int nbytes = nrows * hp * (k == 2 ? (int)sizeof(HT) : (int)sizeof(float2));
+        const uint32_t dst = dst0 + (uint32_t)(k * part * (int64_t)sizeof(float2));
+        for (int o = tid * 16; o < nbytes; o += kThreads * 16)
+          tc::cp_async16(dst + (uint32_t)o, src + o, 16u);
+      }
     }
     cp_async_commit();
   };
+  // line l = k R + r of buf: the even/odd-combined half spectrum of part k, row r
+  auto build = [&](const float2* src_f, const HT* src_h, int k) {
+    for (int e = tid; e < nrows * m; e += kThreads) {
+      const int r = e / m, j = e - r * m;
+      float2 a, c;
+      if (k == 2) {
+        const HT* xr = src_h + (int64_t)r * hp;
+        a = Store<HT>::load(xr + j);
+        c = Store<HT>::load(xr + (m - j));
+      } else {
+        const float2* xr = src_f + (int64_t)r * hp;
+        a = xr[j];
+        c = xr[m - j];
+      }
+      if (j == 0) { a.y = 0.f; c.y = 0.f; }
+      const float2 cc = fft::cconj(c);
+      const float2 E = fft::cadd(a, cc);
+      const float2 O = fft::cmul(fft::csub(a, cc), fft::cconj(tw2[j]));
+      buf[(int64_t)(k * R + r) * m + j] = make_float2(E.x - O.y, E.y + O.x);
+    }
+  };
   issue(0);
-  for (int p = 0; p < 3 * B; ++p) {
-    const int b = p / 3, kind = p - 3 * b;
-    // the other buffer was last read by phase p - 1, which ended with a block barrier
-    issue(p + 1);
+  for (int b = 0; b < B; ++b) {
+    // the other buffer set was last read by rotation b - 1, which ended with a barrier
+    issue(b + 1);
     cp_async_wait<1>();
-    __syncthreads();  // phase p's rows landed for every thread
-    const double nobs = stats[b * 4 + 2];
-    if (kind == 2)
-      c2r_rows<M, HT>(reinterpret_cast<const HT*>(rawb[p & 1]), buf, tw2, nrows, n2, hp, pm, tid);
+    __syncthreads();  // rotation b's rows landed for every thread
+    const float2* rs = raw0 + (b & 1) * 3 * part;
+    build(rs, nullptr, 0);
+    build(rs + part, nullptr, 1);
+    build(nullptr, reinterpret_cast<const HT*>(rs + 2 * part), 2);
+    __syncthreads();
+    if constexpr (M > 0)
+      fft::fft_lines_ct<M, 1, kMaxE, false>(buf, 3 * R, M, 1, tw2, 2 * M, tid, kThreads);
     else
-      c2r_rows<M, float2>(rawb[p & 1], buf, tw2, nrows, n2, hp, pm, tid);
-    if (kind == 0) {
-      // local mean
+      fft::fft_lines<1, kMaxE, false>(buf, pm, 3 * R, m, 1, tw2, n2, tid, kThreads);
+    const double nobs = stats[b * 4 + 2];
 #pragma unroll
-      for (int c = 0; c < kMaxV; ++c) {
-        int v = tid + c * kThreads;
-        e1[c] = v < nout ? (double)outv[v] * (double)scale_m / nobs : 0.0;
-      }
-    } else if (kind == 1) {
-      // local mean square -> variance -> denominator
-#pragma unroll
-      for (int c = 0; c < kMaxV; ++c) {
-        int v = tid + c * kThreads;
-        if (v < nout) {
-          double e2 = (double)outv[v] * (double)scale_m / nobs;
-          double var = e2 - e1[c] * e1[c];
-          double sd = sqrt(var > 0 ? var : 0.0);
-          if (sd < eps) sd = 1.0;
-          e1[c] = sd * nobs;  // reuse as the denominator
-        }
-      }
-    } else {
-      // numerator
-#pragma unroll
-      for (int c = 0; c < kMaxV; ++c) {
-        int v = tid + c * kThreads;
-        if (v < nout) {
-          float sc = (float)((double)outv[v] * (double)scale_t / e1[c]);
-          if (sc > best[c]) { best[c] = sc; arg[c] = first_index + b; }
-        }
+    for (int c = 0; c < kMaxV; ++c) {
+      const int v = tid + c * kThreads;
+      if (v < nout) {
+        const double e1 = (double)outv[v] * (double)scale_m / nobs;
+        const double e2 = (double)outv[set + v] * (double)scale_m / nobs;
+        const double var = e2 - e1 * e1;
+        double sd = sqrt(var > 0 ? var : 0.0);
+        if (sd < eps) sd = 1.0;
+        const float sc = (float)((double)outv[2 * set + v] * (double)scale_t / (sd * nobs));
+        if (sc > best[c]) { best[c] = sc; arg[c] = first_index + b; }
       }
     }
     __syncthreads();
@@ -1112,6 +1123,8 @@ struct Scan {
   LinePlan p0{}, p1{}, pm{};
   bool reg0 = false, reg1 = false;  // register-resident column kernels for n0 / n1
   int W1 = 1, W2 = 1, W3 = 1, R4 = 1;
+  int R4f = 1;  // rows per block of the FLC z pass (three parts per row)
+  size_t smem4f = 0;
   size_t smem1 = 0, smem2 = 0, smem3 = 0, smem4 = 0;
   cufftHandle fwd = 0, inv = 0, tfwd = 0, tinv = 0;
   bool have_fwd = false, have_tfwd = false;
@@ -1183,12 +1196,13 @@ struct StageTimer {
   }
 
 template <typename HT>
-static void launch_zpass_flc(Scan* s, dim3 g4, HT* H, int nb, int64_t rows, float out_scale,
+static void launch_zpass_flc(Scan* s, HT* H, int nb, int64_t rows, float out_scale,
                              int32_t first, float* state_max, int32_t* state_rot,
                              cudaStream_t st) {
   const double* stats = s->stats_ws + (int64_t)nb * kStatChunks * 3;
-  TM_DISPATCH_M(s->n2 / 2, (zpass_flc_kernel<HT, MM><<<g4, kThreads, s->smem4, st>>>(
-                               H, s->Hm, s->Hm2, nb, rows, s->n2, s->hp, s->R4, s->pm, s->tw2,
+  dim3 g4f(ceil_div(rows, s->R4f));
+  TM_DISPATCH_M(s->n2 / 2, (zpass_flc_kernel<HT, MM><<<g4f, kThreads, s->smem4f, st>>>(
+                               H, s->Hm, s->Hm2, nb, rows, s->n2, s->hp, s->R4f, s->pm, s->tw2,
                                out_scale, out_scale, stats, 1.1920928955078125e-07, first,
                                state_max, state_rot, s->SH, s->graph_first)));
 }
@@ -1598,14 +1612,19 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     s->W2 = std::max(1, std::min(s->h2, kTile / s->n0));
     s->W3 = s->W1;
     s->R4 = std::max(1, std::min(kTile / std::max(1, s->n2 / 2), (kThreads * kMaxV) / s->n2));
+    s->R4f = std::max(1, std::min(kTile / std::max(1, 3 * (s->n2 / 2)),
+                                  (kThreads * kMaxV) / s->n2));
     s->smem1 = sizeof(float2) * (s->n1 + s->n2 + (size_t)s->n1 * s->W1) + sizeof(float) * s->t1 * s->t2;
     s->smem2 = sizeof(float2) * (s->n0 + (size_t)s->n0 * s->W2);
     s->smem3 = sizeof(float2) * (s->n1 + (size_t)s->n1 * s->W3);
-    // twiddles (padded to 16 bytes), two raw row buffers (the FLC z pass stages the next
-    // phase in the second), the c2r buffer
+    // twiddles (padded to 16 bytes), two raw row buffers, the c2r buffer
     s->smem4 = sizeof(float2) * ((s->n2 + 1) / 2 * 2 + 2 * (size_t)s->R4 * s->hp +
                                  (size_t)s->R4 * (s->n2 / 2));
+    // FLC z pass: twiddles, two raw sets of three parts, the c2r buffer of 3 R4f lines
+    s->smem4f = sizeof(float2) * ((s->n2 + 1) / 2 * 2 + 6 * (size_t)s->R4f * s->hp +
+                                  3 * (size_t)s->R4f * (s->n2 / 2));
     size_t mx = std::max(std::max(s->smem1, s->smem2), std::max(s->smem3, s->smem4));
+    if (d.score == TM_SCORE_FLC) mx = std::max(mx, s->smem4f);
     if (mx > 200 * 1024) {
       set_error("scan_create: shared-memory tile of %zu bytes exceeds the limit", mx);
       destroy(s);
@@ -1977,7 +1996,7 @@ static int launch_group(Scan* s, int nb, double hs, float out_scale, int32_t fir
     TM_TRY(launch_template_x_y<__half2>(s, nb, (float)hs, H, tmr, stream));
     tmr.begin();
     if (s->d.score == TM_SCORE_FLC)
-      launch_zpass_flc<__half2>(s, g4, H, nb, rows, out_scale, first, state_max, state_rot, stream);
+      launch_zpass_flc<__half2>(s, H, nb, rows, out_scale, first, state_max, state_rot, stream);
     else
       launch_zpass<__half2>(s, g4, H, nb, rows, out_scale, first, state_max, state_rot, stream);
     TM_TRY(check_launch("z pass"));
@@ -1987,7 +2006,7 @@ static int launch_group(Scan* s, int nb, double hs, float out_scale, int32_t fir
     TM_TRY(launch_template_x_y<float2>(s, nb, (float)hs, H, tmr, stream));
     tmr.begin();
     if (s->d.score == TM_SCORE_FLC)
-      launch_zpass_flc<float2>(s, g4, H, nb, rows, out_scale, first, state_max, state_rot, stream);
+      launch_zpass_flc<float2>(s, H, nb, rows, out_scale, first, state_max, state_rot, stream);
     else
       launch_zpass<float2>(s, g4, H, nb, rows, out_scale, first, state_max, state_rot, stream);
     TM_TRY(check_launch("z pass"));
