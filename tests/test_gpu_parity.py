@@ -531,14 +531,16 @@ def test_default_passes_odd_z_length(torch_cuda, score):
     assert np.abs(r[0] - ref64["scores"]).max() <= tol
 
 
-@pytest.mark.parametrize("shape,score", [((64, 512, 40), "FLCSphericalMask"),
+@pytest.mark.parametrize("shape,score", [((128, 512, 40), "FLCSphericalMask"),
                                          ((48, 256, 33), "FLCSphericalMask"),
-                                         ((64, 512, 24), "CC")])
+                                         ((128, 256, 24), "CC")])
 def test_tensor_core_ypass(torch_cuda, shape, score):
     """The tensor-core y pass (radix-16 and radix-n1/16 FP16 GEMM stages with twiddles
     between them; "tensor": the radix-16 stage in FP32 registers, "tensor2": both stages on
     the tensor cores) for both supported y lengths, with a partial last launch
-    group, against the oracle in FP32 and FP64 and against the CUDA-core y pass."""
+    group, against the oracle in FP32 and FP64 and against the CUDA-core y pass. The
+    shapes with n0 = 128 run it behind the warp-specialised tensor-core x pass, as the
+    default mixed-precision plans do."""
     from pytme_b200 import synthetic as syn
 
     rng = np.random.default_rng(sum(shape))
