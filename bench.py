@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--zpass", choices=("auto", "tensor", "fft"), default="auto",
                     help="z pass on the tensor cores, as CUDA-core FFTs, or the plan default")
-    ap.add_argument("--ypass", choices=("auto", "tensor", "tensor2", "fft"), default="auto",
+    ap.add_argument("--ypass", choices=("auto", "tensor", "tensor-inplace", "tensor2", "fft"),
+                    default="auto",
                     help="y pass on the tensor cores, as CUDA-core FFTs, or the plan default")
     ap.add_argument("--xpass", choices=("auto", "tensor", "fft"), default="auto",
                     help="x pass on the tensor cores, as CUDA-core FFTs, or the plan default "

@@ -195,7 +195,10 @@ int tm_scan_zpass_mode(const tm_scan* plan);
  * between them; mixed-precision plans with n1 of 256 or 512; the default where
  * available), mode 1 as CUDA-core FFTs, mode 2 restores the default, mode 3 runs both
  * DFT stages on the tensor cores (needs the warp-specialised tensor-core x pass, which
- * then writes the y pass's input layout). tm_scan_ypass_mode reports 0, 1 or 3.
+ * then writes the y pass's input layout), mode 4 runs mode 0 in place on row-major
+ * spectra (mode 0 reads the spectra that the warp-specialised x pass writes with x'
+ * innermost and writes row-major rows into a second buffer for the z pass, where the
+ * plan has one). tm_scan_ypass_mode reports 0, 1, 3 or 4.
  * TM_E_UNSUPPORTED when the requested form is not available. */
 int tm_scan_set_ypass(tm_scan* plan, int mode);
 int tm_scan_ypass_mode(const tm_scan* plan);

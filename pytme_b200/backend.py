@@ -44,7 +44,8 @@ def _set_options(**kwargs):
     if _OPTIONS["precision"] not in ("fp32", "mixed"):
         raise ValueError("precision must be 'fp32' or 'mixed'")
     for key in ("xpass", "ypass", "zpass"):
-        allowed = ("auto", "fft", "tensor") + (("tensor2",) if key == "ypass" else ())
+        allowed = ("auto", "fft", "tensor") + (("tensor2", "tensor-inplace") if key == "ypass"
+                                               else ())
         if _OPTIONS[key] not in allowed:
             raise ValueError(f"{key} must be one of {', '.join(allowed)}")
     _OPTIONS["rotation_batch"] = int(_OPTIONS["rotation_batch"])

@@ -1097,6 +1097,10 @@ struct Scan {
   // two DFT operators
   bool ytc_avail = false, ytc = false;
   bool ys1 = false;  // radix-16 stage on the tensor cores too (tm_scan_set_ypass mode 3)
+  bool yinplace = false;  // tensor-core y pass in place on row-major H (mode 4)
+  // y pass output (row-major) when the x pass writes H x'-inner; allocated where that
+  // form is possible
+  void* H2 = nullptr;
   YpassTcConfig ycfg{};
   uint16_t* ytable = nullptr;
   // polls of every data wait of the tensor-core kernels before they give up
@@ -1164,6 +1168,13 @@ static bool x_writes_stage1(const Scan* s) {
 // The tensor-core y pass runs its radix-16 stage on the tensor cores too (opt-in: measured
 // slower than the radix-16 stage on the CUDA cores).
 static bool y_stage1_tc(const Scan* s) { return s->ytc && s->ys1 && x_writes_stage1(s); }
+// Whether the warp-specialised x pass writes H x'-inner, [b][k1][k2 / 8][x'][8], and the
+// tensor-core y pass reads it from there and writes row-major rows into H2 for the z pass.
+// A warp of the x pass's epilogue then stores, per rotation, 32 consecutive x' rows of one
+// 8-column segment as 1 KB of whole cache lines instead of 32 sectors one plane apart.
+static bool x_inner(const Scan* s) {
+  return s->H2 && s->ytc && !s->yinplace && !y_stage1_tc(s) && x_writes_stage1(s);
+}
 
 // Stage timing: record an event before a stage and accumulate after it.
 struct StageTimer {
@@ -1377,7 +1388,7 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
     const bool s1 = y_stage1_tc(s);
     TM_TRY(xcorr_tc_run(s->xcfg, s->G, s->ctarget, nb, s->t0, s->n0, s->n1, s->h2, s->hp, hs,
                         H, std::is_same<HT, __half2>::value, s->tc_err, stream,
-                        s->wait_iters, s1, s1 ? s->n1 / 16 : 0, half_g));
+                        s->wait_iters, s1, s1 ? s->n1 / 16 : 0, half_g, x_inner(s)));
   } else if (s->reg0) {
     TM_DISPATCH_N(s->n0, (launch_xpass_reg<NN, HT>(s, nb, hs, H, stream)));
   } else {
@@ -1391,7 +1402,8 @@ static int launch_template_x_y(Scan* s, int nb, float hs, HT* H, StageTimer& tmr
   tmr.begin();
   if (s->ytc && std::is_same<HT, __half2>::value) {
     TM_TRY(ypass_tc_run(s->ycfg, H, nb, s->n0, s->hp, s->h2, s->ytable, s->wait_iters, s->tc_err,
-                        stream, seg_layout(s), y_stage1_tc(s)));
+                        stream, seg_layout(s), y_stage1_tc(s), x_inner(s) ? s->H2 : nullptr,
+                        x_inner(s)));
   } else if (s->reg1) {
     TM_DISPATCH_N(s->n1, (launch_ypass_reg<NN, HT>(s, nb, H, stream, seg_layout(s))));
     if (flc) {
@@ -1535,6 +1547,11 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
     s->xtc = s->xtc_avail && s->half && (s->xcfg.hk || s->xcfg.ws);
   }
   if (s->xtc_avail) o_ct = take(sizeof(float2) * s->S);
+  // the y pass's row-major output where the x pass can write H x'-inner (see x_inner)
+  size_t o_H2 = 0;
+  const bool h2_buf = s->fused && s->half && d.score != TM_SCORE_FLC && s->ytc_avail &&
+                      s->xtc_avail && s->xcfg.ws && B <= s->xcfg.ws_NB && s->hp % 8 == 0;
+  if (h2_buf) o_H2 = take(sizeof(__half2) * (size_t)B * s->SH);
   if (s->xtc_avail || s->ztc_avail || s->ytc_avail) o_err = take(sizeof(int) * 4);
   s->bytes = off;
   const int64_t cap = device_memory_limit();
@@ -1575,6 +1592,7 @@ int scan_create(const tm_scan_desc* desc, Scan** out) {
   } else {
     s->G = reinterpret_cast<float2*>(b8 + o_G);
     s->H = b8 + o_H;
+    if (h2_buf) s->H2 = b8 + o_H2;
     if (d.score == TM_SCORE_FLC) {
       s->Gm = reinterpret_cast<float2*>(b8 + o_Gm);
       s->Hm = reinterpret_cast<float2*>(b8 + o_Hm);
@@ -1803,21 +1821,26 @@ int scan_zpass_mode(const Scan* s) { return s && s->ztc ? 0 : 1; }
 // GEMM; half-precision CC / FLCSphericalMask plans with n1 in {256, 512}; the default
 // where available), as FFTs on the CUDA cores (mode 1), the default (mode 2), or with both
 // DFT stages on the tensor cores (mode 3: needs the warp-specialised tensor-core x pass,
-// which then writes the y pass's stage-1 layout).
+// which then writes the y pass's stage-1 layout), or as mode 0 but in place on row-major H
+// (mode 4; mode 0 reads the x'-inner H the warp-specialised x pass writes, see x_inner).
 int scan_set_ypass(Scan* s, int mode) {
   TM_REQUIRE(s, "scan_set_ypass: null plan");
-  TM_REQUIRE(mode >= 0 && mode <= 3,
-             "scan_set_ypass: mode must be 0 (tensor cores), 1 (FFT), 2 (default) or 3 "
-             "(both DFT stages on the tensor cores)");
+  TM_REQUIRE(mode >= 0 && mode <= 4,
+             "scan_set_ypass: mode must be 0 (tensor cores), 1 (FFT), 2 (default), 3 "
+             "(both DFT stages on the tensor cores) or 4 (tensor cores, in place)");
   if (mode == 3 && !(s->ytc_avail && x_writes_stage1(s))) {
     set_error("scan_set_ypass: both y stages on the tensor cores need the tensor-core y pass "
               "and the warp-specialised tensor-core x pass");
     return TM_E_UNSUPPORTED;
   }
-  const bool want = mode == 0 || mode == 3 || (mode == 2 && s->ytc_avail);
-  const bool s1 = mode == 3;
-  if (s1 != s->ys1 && s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+  const bool want = mode == 0 || mode == 3 || mode == 4 || (mode == 2 && s->ytc_avail);
+  const bool s1 = mode == 3, inplace = mode == 4;
+  if ((s1 != s->ys1 || inplace != s->yinplace) && s->gexec) {
+    cudaGraphExecDestroy(s->gexec);
+    s->gexec = nullptr;
+  }
   s->ys1 = s1;
+  s->yinplace = inplace;
   if (want && !s->ytc_avail) {
     set_error("scan_set_ypass: the tensor-core y pass does not support this plan");
     return TM_E_UNSUPPORTED;
@@ -1829,7 +1852,7 @@ int scan_set_ypass(Scan* s, int mode) {
 
 int scan_ypass_mode(const Scan* s) {
   if (!s || !s->ytc) return 1;
-  return y_stage1_tc(s) ? 3 : 0;
+  return y_stage1_tc(s) ? 3 : s->yinplace ? 4 : 0;
 }
 
 // Polls of every data wait in the plan's tensor-core kernels (0 restores the default).
@@ -1998,7 +2021,8 @@ static int launch_group(Scan* s, int nb, double hs, float out_scale, int32_t fir
     if (s->d.score == TM_SCORE_FLC)
       launch_zpass_flc<__half2>(s, H, nb, rows, out_scale, first, state_max, state_rot, stream);
     else
-      launch_zpass<__half2>(s, g4, H, nb, rows, out_scale, first, state_max, state_rot, stream);
+      launch_zpass<__half2>(s, g4, x_inner(s) ? static_cast<__half2*>(s->H2) : H, nb, rows,
+                            out_scale, first, state_max, state_rot, stream);
     TM_TRY(check_launch("z pass"));
     tmr.end(TM_STAGE_ZPASS);
   } else {

@@ -53,6 +53,17 @@ __device__ __forceinline__ void load_3d(uint32_t dst, const CUtensorMap* map, in
         "r"(tc::smem_u32(bar))
       : "memory");
 }
+// box load at (x, y, z, w) of a 4D tensor into shared memory, completing on `bar`
+__device__ __forceinline__ void load_4d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                        int z, int w, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];"
+      :
+      : "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w),
+        "r"(tc::smem_u32(bar))
+      : "memory");
+}
 // box store from shared memory to (x, y) of a 2D tensor (bulk async-group completion)
 __device__ __forceinline__ void store_2d(const CUtensorMap* map, int x, int y, uint32_t src) {
   asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"

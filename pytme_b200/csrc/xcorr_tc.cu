@@ -603,11 +603,12 @@ static int launch_xcorr(const XcorrTcConfig& cfg, const float2* G, const float2*
 
 int xcorr_tc_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int nb, int t0,
                  int n0, int n1, int h2, int hp, float scale, void* H, bool half, int* err,
-                 cudaStream_t stream, uint32_t wait_iters, bool seg, int rowq, bool g_half) {
+                 cudaStream_t stream, uint32_t wait_iters, bool seg, int rowq, bool g_half,
+                 bool xin) {
   if (half && cfg.ws && nb <= cfg.ws_NB && hp % 8 == 0)
     return xcorr_ws_run(cfg, G, C, nb, t0, n0, n1, h2, hp, scale, static_cast<__half2*>(H), err,
-                        stream, wait_iters, seg, rowq, g_half);
-  TM_REQUIRE(!seg && rowq == 0 && !g_half,
+                        stream, wait_iters, seg, rowq, g_half, xin);
+  TM_REQUIRE(!seg && rowq == 0 && !g_half && !xin,
              "xcorr_tc_run: segment-layout output needs the warp-specialised kernel");
   TM_REQUIRE(cfg.ok, "xcorr_tc_run: unsupported configuration");
   TM_REQUIRE(nb <= cfg.NB, "xcorr_tc_run: %d rotations exceed the configured %d", nb, cfg.NB);

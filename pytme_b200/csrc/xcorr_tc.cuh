@@ -32,11 +32,13 @@ int xcorr_ws_config(int n0, int t0, int nb, XcorrTcConfig* cfg);
 // complex values; rowq > 0 (n1 = 16 rowq): store row k1 = rowq a + c of each plane at
 // position 16 c + a. Both together give the input layout of the tensor-core y pass with
 // its radix-16 stage on the tensor cores. g_half: G holds FP16 complex values (__half2)
-// instead of float2, at the same element offsets.
+// instead of float2, at the same element offsets. xin: H is laid out x'-inner,
+// [b][k1][k2 / 8][x'][8] (hp a multiple of 8), so that the 32-byte segments a warp stores
+// for 32 consecutive x' form whole cache lines instead of 32 lines one plane apart.
 int xcorr_ws_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int nb, int t0,
                  int n0, int n1, int h2, int hp, float scale, __half2* H, int* err,
                  cudaStream_t stream, uint32_t wait_iters = 0, bool seg = false, int rowq = 0,
-                 bool g_half = false);
+                 bool g_half = false, bool xin = false);
 // C = unnormalised inverse DFT along x (axis 0) of the target spectrum F [n0][n1][h2].
 int xcorr_tc_prepare(const float2* F, float2* C, int n0, int n1, int h2, cudaStream_t stream);
 // H[b][x'][k1][k2] = sum_{x<t0} scale * C[(x'-x) mod n0][k1][k2] * G[b][x][k1][k2];
@@ -44,6 +46,6 @@ int xcorr_tc_prepare(const float2* F, float2* C, int n0, int n1, int h2, cudaStr
 int xcorr_tc_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int nb, int t0,
                  int n0, int n1, int h2, int hp, float scale, void* H, bool half, int* err,
                  cudaStream_t stream, uint32_t wait_iters = 0, bool seg = false,
-                 int rowq = 0, bool g_half = false);
+                 int rowq = 0, bool g_half = false, bool xin = false);
 
 }  // namespace tmb

@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
 xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int nb, int NB,
                 int t0, int n0, int n1, int h2, int hp, float scale,
                 __half2* __restrict__ H, int* __restrict__ err, uint32_t wait_iters,
-                int seg, int rowq, int ghalf) {
+                int seg, int rowq, int ghalf, int xin) {
   constexpr int t0p = 8 * NXC;
   const uint32_t wi = wait_iters ? wait_iters : kWaitIters;  // data waits
   constexpr uint32_t kAccCols = 16u * R;               // one fill
@@ -285,7 +285,8 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
       }
       if (*fail) break;
       const int64_t item = (int64_t)blockIdx.x + j * gridDim.x;
-      const int k1 = (int)(item / ncg), k20 = (int)(item - (int64_t)k1 * ncg) * kWsW;
+      const int k1 = (int)(item / ncg), cg = (int)(item - (int64_t)k1 * ncg);
+      const int k20 = cg * kWsW;
       const int64_t col0 = (int64_t)k1 * h2 + k20;
       uint16_t* bb = Bs + (size_t)bsl * (L.b_buf / 2);
       // task = 8 consecutive x of one rotation and column, stored as two 16-byte rows;
@@ -340,7 +341,8 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
     float2 c[kWsMaxE];
     auto fetch = [&](int64_t j, int t) {
       const int64_t item = (int64_t)blockIdx.x + j * gridDim.x;
-      const int k1 = (int)(item / ncg), k20 = (int)(item - (int64_t)k1 * ncg) * kWsW;
+      const int k1 = (int)(item / ncg), cg = (int)(item - (int64_t)k1 * ncg);
+      const int k20 = cg * kWsW;
       const int64_t col0 = (int64_t)k1 * h2 + k20;
       const int e0 = n0 - kWsRows * (t + 1);
 #pragma unroll
@@ -403,20 +405,26 @@ xcorr_ws_kernel(const float2* __restrict__ G, const float2* __restrict__ C, int 
     // ------------------------------------------------------------------ epilogue
     const int quarter = warp & 3, eg = (warp - 8) >> 2;  // eg: rotations (R/2) eg .. of a fill
     const float inv = 1.f / kWsPrescale;
-    const int64_t rowH = (int64_t)n1 * hp, SH = (int64_t)n0 * rowH;
+    // H element strides of x', k1 and the 8-column segment: row-major [b][x'][k1][k2], or
+    // x'-inner [b][k1][k2 / 8][x'][8], where the 32 consecutive x' rows a warp stores for
+    // one rotation form 1 KB of whole cache lines
+    const int64_t SH = (int64_t)n0 * n1 * hp;
+    const int64_t xstr = xin ? 8 : (int64_t)n1 * hp;
+    const int64_t kstr = xin ? (int64_t)n0 * hp : (int64_t)hp;
+    const int64_t cstr = xin ? (int64_t)n0 * 8 : 8;
     const int r = quarter * 32 + lane;
     bool ok = true;
     for (int64_t j = 0; j < mine && ok; ++j) {
       const int64_t item = (int64_t)blockIdx.x + j * gridDim.x;
-      const int k1 = (int)(item / ncg), k20 = (int)(item - (int64_t)k1 * ncg) * kWsW;
+      const int k1 = (int)(item / ncg), cg = (int)(item - (int64_t)k1 * ncg);
       // row k1 = rowq a + c goes to position 16 c + a when rowq > 0 (the y pass's stage-1
       // order), to position k1 otherwise
       const int krow = rowq > 0 ? (k1 % rowq) * 16 + k1 / rowq : k1;
-      const int64_t colH = (int64_t)krow * hp + k20;
+      const int64_t colH = (int64_t)krow * kstr + (int64_t)cg * cstr;
       for (int t = 0; t < ntile && ok; ++t) {
         const int64_t tau = j * ntile + t;
         const int xp = t * kWsRows + kWsRows - 1 - r;
-        __half2* hrow = H + (int64_t)xp * rowH + colH;
+        __half2* hrow = H + (int64_t)xp * xstr + colH;
         for (int h = 0; h < nh; ++h) {
           const int64_t f = tau * nh + h;
           const int buf = (int)(f % kNbuf);
@@ -509,7 +517,8 @@ int xcorr_ws_config(int n0, int t0, int nb, XcorrTcConfig* cfg) {
 
 int xcorr_ws_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int nb, int t0,
                  int n0, int n1, int h2, int hp, float scale, __half2* H, int* err,
-                 cudaStream_t stream, uint32_t wait_iters, bool seg, int rowq, bool g_half) {
+                 cudaStream_t stream, uint32_t wait_iters, bool seg, int rowq, bool g_half,
+                 bool xin) {
   // 32-byte row segments: pitch a multiple of 8 complex values, aligned base
   TM_REQUIRE(cfg.ws && nb <= cfg.ws_NB && hp % 8 == 0 && hp >= h2 &&
                  reinterpret_cast<uintptr_t>(H) % 32 == 0 &&
@@ -529,7 +538,7 @@ int xcorr_ws_run(const XcorrTcConfig& cfg, const float2* G, const float2* C, int
   }
   fn<<<grid, kWsThreads, cfg.ws_smem, stream>>>(G, C, nb, cfg.ws_NB, t0, n0, n1, h2, hp, scale,
                                                H, err, wait_iters, seg ? 1 : 0, rowq,
-                                               g_half ? 1 : 0);
+                                               g_half ? 1 : 0, xin ? 1 : 0);
   return check_launch("xcorr_ws_kernel");
 }
 

@@ -179,9 +179,9 @@ constexpr uint32_t kS1MStride = 512, kS1KStride = 128;
 
 template <int Q, bool S1>
 __global__ void __launch_bounds__(kYThreads, 1)
-ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc, int h2,
-                const uint16_t* __restrict__ Tg, uint32_t wait_iters, int* __restrict__ err,
-                int seg) {
+ypass_tc_kernel(const __grid_constant__ CUtensorMap lmap, const __grid_constant__ CUtensorMap smap,
+                int64_t nitems, int nc, int n0, int h2, const uint16_t* __restrict__ Tg,
+                uint32_t wait_iters, int* __restrict__ err, int seg, int xin) {
   using L = YLayout<Q>;
   extern __shared__ __align__(1024) uint16_t smem_y[];
   uint16_t* T2s = smem_y;
@@ -269,10 +269,20 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
         item_xy(j, x, y);
         const uint32_t dst = smem_u32(Ss + (size_t)s * L::S);
         tma::arrive_expect_tx(sfull + s, L::ITEM_BYTES);
+        if (xin) {
+          // x'-inner input [b][k1][k2 / 8][x'][8]: the item's rows are the k1 of segment
+          // x / 8 of plane (b, x')
+          const int plane = y / L::N1, xp = plane % n0, z0 = (plane / n0) * L::N1;
 #pragma unroll
-        for (int b = 0; b < L::NBOX; ++b)
-          tma::load_2d(dst + (uint32_t)(b * kBoxRows * 32), &hmap, x, y + b * kBoxRows,
-                       sfull + s);
+          for (int b = 0; b < L::NBOX; ++b)
+            tma::load_4d(dst + (uint32_t)(b * kBoxRows * 32), &lmap, 0, xp, x >> 3,
+                         z0 + b * kBoxRows, sfull + s);
+        } else {
+#pragma unroll
+          for (int b = 0; b < L::NBOX; ++b)
+            tma::load_2d(dst + (uint32_t)(b * kBoxRows * 32), &lmap, x, y + b * kBoxRows,
+                         sfull + s);
+        }
         issued = j + 1;
       }
       // nothing may leave while a load still writes into shared memory: wait (with the
@@ -296,7 +306,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap hmap, int64_t nitems, int nc
         const uint32_t src = smem_u32(Es + (size_t)p * L::S);
 #pragma unroll
         for (int b = 0; b < L::NBOX; ++b)
-          tma::store_2d(&hmap, x, y + b * kBoxRows, src + (uint32_t)(b * kBoxRows * 32));
+          tma::store_2d(&smap, x, y + b * kBoxRows, src + (uint32_t)(b * kBoxRows * 32));
         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
         // the staging buffer is free once the stores have read it
         asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
@@ -616,28 +626,43 @@ int ypass_tc_prepare(const YpassTcConfig& cfg, uint16_t* table, cudaStream_t str
 
 int ypass_tc_run(const YpassTcConfig& cfg, void* H, int nb, int n0, int hp, int h2,
                  const uint16_t* table, uint32_t wait_iters, int* err, cudaStream_t stream,
-                 bool seg, bool s1) {
+                 bool seg, bool s1, void* Hout, bool xin) {
   TM_REQUIRE(cfg.ok, "ypass_tc_run: unsupported configuration");
   TM_REQUIRE(H && table && err && nb >= 1 && n0 >= 1 && hp % 8 == 0 && h2 >= 1 && h2 <= hp &&
                  wait_iters > 0,
              "ypass_tc_run: bad arguments");
+  if (!Hout) Hout = H;
+  // an x'-inner input cannot be overwritten item by item with row-major output
+  TM_REQUIRE(!xin || Hout != H, "ypass_tc_run: an x'-inner input needs a separate output");
   TM_REQUIRE(reinterpret_cast<uintptr_t>(H) % 16 == 0 &&
+                 reinterpret_cast<uintptr_t>(Hout) % 16 == 0 &&
                  reinterpret_cast<uintptr_t>(table) % 16 == 0,
-             "ypass_tc_run: H and the operator table must be 16-byte aligned");
+             "ypass_tc_run: H, the output and the operator table must be 16-byte aligned");
   const int64_t rows = (int64_t)nb * n0 * cfg.n1;
   TM_REQUIRE(rows < ((int64_t)1 << 31), "ypass_tc_run: more than 2^31 rows");
-  // H as a 2D tensor of 4-byte words: hp columns, rows rows; boxes of 8 x 256 words
-  CUtensorMap map;
+  // the output as a 2D tensor of 4-byte words: hp columns, rows rows; boxes of 8 x 256
+  // words. The input likewise, or, x'-inner, as a 4D tensor (8 words, n0 x', hp / 8
+  // segments, nb n1 (b, k1) rows) with boxes of 8 x 1 x 1 x 256 words, which land in the
+  // same shared layout.
+  CUtensorMap lmap, smap;
   const uint64_t dims[2] = {(uint64_t)hp, (uint64_t)rows};
   const uint64_t strides[1] = {(uint64_t)hp * 4u};
   const uint32_t box[2] = {8u, (uint32_t)kBoxRows};
-  TM_TRY(encode_tensor_map_u32(&map, H, 2, dims, strides, box));
+  TM_TRY(encode_tensor_map_u32(&smap, Hout, 2, dims, strides, box));
+  if (xin) {
+    const uint64_t dims4[4] = {8u, (uint64_t)n0, (uint64_t)hp / 8u, (uint64_t)nb * cfg.n1};
+    const uint64_t strides4[3] = {32u, (uint64_t)n0 * 32u, (uint64_t)n0 * hp * 4u};
+    const uint32_t box4[4] = {8u, 1u, 1u, (uint32_t)kBoxRows};
+    TM_TRY(encode_tensor_map_u32(&lmap, H, 4, dims4, strides4, box4));
+  } else {
+    TM_TRY(encode_tensor_map_u32(&lmap, H, 2, dims, strides, box));
+  }
   const int64_t nitems = (int64_t)nb * n0 * (hp / 8);
   const int grid = (int)std::min<int64_t>(nitems, cfg.sms);
   auto fn = cfg.Q == 32 ? (s1 ? ypass_tc_kernel<32, true> : ypass_tc_kernel<32, false>)
                         : (s1 ? ypass_tc_kernel<16, true> : ypass_tc_kernel<16, false>);
-  fn<<<grid, kYThreads, cfg.smem, stream>>>(map, nitems, hp / 8, h2, table, wait_iters, err,
-                                            seg ? 1 : 0);
+  fn<<<grid, kYThreads, cfg.smem, stream>>>(lmap, smap, nitems, hp / 8, n0, h2, table,
+                                            wait_iters, err, seg ? 1 : 0, xin ? 1 : 0);
   return check_launch("ypass_tc_kernel");
 }
 

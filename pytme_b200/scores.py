@@ -148,16 +148,19 @@ class ScanPlan:
 
     def set_ypass(self, mode: str = "auto"):
         """y pass on the tensor cores ("tensor": radix 16 in FP32 registers, radix n1/16 on
-        the tensor cores), with both DFT stages on the tensor cores ("tensor2"; needs the
-        tensor-core x pass), as FFTs on the CUDA cores ("fft"), or the plan's default
-        ("auto")."""
-        code = {"tensor": 0, "fft": 1, "auto": 2, "tensor2": 3}[mode]
+        the tensor cores; behind the warp-specialised tensor-core x pass it reads spectra
+        stored with x' innermost and writes row-major rows into a second buffer), the same
+        in place on row-major spectra ("tensor-inplace"), with both DFT stages on the
+        tensor cores ("tensor2"; needs the tensor-core x pass), as FFTs on the CUDA cores
+        ("fft"), or the plan's default ("auto")."""
+        code = {"tensor": 0, "fft": 1, "auto": 2, "tensor2": 3, "tensor-inplace": 4}[mode]
         N.check(N.lib.tm_scan_set_ypass(self._h, code), "tm_scan_set_ypass")
 
     @property
     def ypass(self) -> str:
-        """The y pass this plan runs: "tensor", "tensor2" or "fft"."""
-        return {0: "tensor", 1: "fft", 3: "tensor2"}[N.lib.tm_scan_ypass_mode(self._h)]
+        """The y pass this plan runs: "tensor", "tensor-inplace", "tensor2" or "fft"."""
+        return {0: "tensor", 1: "fft", 3: "tensor2", 4: "tensor-inplace"}[
+            N.lib.tm_scan_ypass_mode(self._h)]
 
     def set_wait_budget(self, iters: int = 0):
         """Polls of every data wait in the tensor-core kernels (0: the default). A wait

@@ -157,6 +157,13 @@ def test_config3_bench_workload(torch_cuda):
     assert err32 <= tol and err64 <= tol
     ties = _check_ties("FLCSphericalMask", target, tmpl, mask, rots, rot, ref64, workers)
     print(f"config 3: {ties} argmax ties")
+    if probe_ypass == "tensor":
+        # the x'-inner hand-over between the x and y passes moves the same values as the
+        # in-place y pass on row-major spectra: the maps agree bit for bit
+        inpl = _gpu_scan("FLCSphericalMask", target, tmpl, mask, rots, batch=32,
+                         ypass="tensor-inplace")
+        assert np.array_equal(np.asarray(inpl[0]), s)
+        assert np.array_equal(np.asarray(inpl[2]), rot)
     o_s, o_rot = np.asarray(other[0]), np.asarray(other[2])
     o_err64 = float(np.abs(o_s - ref64["scores"]).max())
     print(f"config 3, other y pass: max |gpu - fp64| = {o_err64:.3e}")

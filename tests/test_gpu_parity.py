@@ -540,7 +540,9 @@ def test_tensor_core_ypass(torch_cuda, shape, score):
     the tensor cores) for both supported y lengths, with a partial last launch
     group, against the oracle in FP32 and FP64 and against the CUDA-core y pass. The
     shapes with n0 = 128 run it behind the warp-specialised tensor-core x pass, as the
-    default mixed-precision plans do."""
+    default mixed-precision plans do: the x pass then writes the spectra x'-inner for it
+    ("tensor"), which must give the same maps bit for bit as the in-place form on
+    row-major spectra ("tensor-inplace")."""
     from pytme_b200 import synthetic as syn
 
     rng = np.random.default_rng(sum(shape))
@@ -549,6 +551,9 @@ def test_tensor_core_ypass(torch_cuda, shape, score):
     target, _, _ = syn.make_tomogram(shape, tmpl, 4, rng, scale=0.5)
     rots = syn.random_rotation_matrices(37, rng)
     r = _scan(score, target, tmpl, mask, rots, precision="mixed", batch=32, ypass="tensor")
+    ip = _scan(score, target, tmpl, mask, rots, precision="mixed", batch=32,
+               ypass="tensor-inplace")
+    assert np.array_equal(r[0], ip[0]) and np.array_equal(r[2], ip[2])
     c = _scan(score, target, tmpl, mask, rots, precision="mixed", batch=32, ypass="tensor2")
     f = _scan(score, target, tmpl, mask, rots, precision="mixed", batch=32, ypass="fft")
     ref = O.scan(target, tmpl, rots, score, template_mask=mask)
