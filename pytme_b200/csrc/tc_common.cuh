@@ -73,6 +73,27 @@ __device__ __forceinline__ bool mbar_wait_n(uint32_t mbar, uint32_t phase, uint3
   return false;
 }
 
+// The same for waits off the critical path: each poll lets the thread sleep until the
+// phase completes or up to kSuspendNs have passed (the try_wait suspend-time hint), so a
+// waiting warp takes fewer issue slots from the warps that work; the poll count is cut by
+// kSuspendDiv so that the bound stays near that of mbar_wait_n.
+constexpr uint32_t kSuspendNs = 1000, kSuspendDiv = 4;
+__device__ __forceinline__ bool mbar_wait_s(uint32_t mbar, uint32_t phase, uint32_t iters) {
+  const uint32_t n = iters / kSuspendDiv > 0 ? iters / kSuspendDiv : 1;
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase), "n"(kSuspendNs)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // Bounded wait for the completion of the mbarrier phase with the given parity.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
   for (uint32_t i = 0; i < kWaitIters; ++i) {

@@ -260,7 +260,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap lmap, const __grid_constant_
       for (int64_t j = 0; j < mine; ++j) {
         const int s = (int)(j % kYS);
         if (j >= kYS &&
-            !mbar_wait_n(smem_u32(sempty + s), (uint32_t)(j / kYS - 1) & 1u, wait_iters)) {
+            !mbar_wait_s(smem_u32(sempty + s), (uint32_t)(j / kYS - 1) & 1u, wait_iters)) {
           *fail = 1;
           break;
         }
@@ -296,7 +296,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap lmap, const __grid_constant_
     if (lane == 0) {
       for (int64_t j = 0; j < mine; ++j) {
         const int p = (int)(j % kNE);
-        if (!mbar_wait_n(smem_u32(estaged + p), (uint32_t)(j / kNE) & 1u, wait_iters)) {
+        if (!mbar_wait_s(smem_u32(estaged + p), (uint32_t)(j / kNE) & 1u, wait_iters)) {
           *fail = 1;
           break;
         }
@@ -524,7 +524,7 @@ ypass_tc_kernel(const __grid_constant__ CUtensorMap lmap, const __grid_constant_
     const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16);
     for (int64_t j = 0; j < mine; ++j) {
       const int pd = (int)(j % kND), pe = (int)(j % kNE);
-      const bool got = mbar_wait_n(smem_u32(d2full + pd), (uint32_t)(j / kND) & 1u, wait_iters);
+      const bool got = mbar_wait_s(smem_u32(d2full + pd), (uint32_t)(j / kND) & 1u, wait_iters);
       // staging buffer pe is free once the stores of item j - kNE have read it
       const bool freed = got && (j < kNE || mbar_wait_n(smem_u32(efree + pe),
                                                         (uint32_t)(j / kNE - 1) & 1u,
