@@ -172,3 +172,25 @@ def test_reference_rotation_set_matches_golden(golden):
     assert np.array_equal(m, g["rotations"])
     m7, desc = R.rotation_set(7.0)
     assert m7.shape == (27672, 3, 3) and "reference" in desc
+
+
+def test_backend_pass_options():
+    """Pass forms accepted by change_backend("b200", ...): every pass takes "auto", "fft"
+    and "tensor"; the y pass also "tensor2" and "tensor-inplace"; anything else raises
+    ValueError, as the reference's backends do for unknown options."""
+    import importlib
+
+    B = importlib.import_module("pytme_b200.backend")  # the module, not the manager
+    try:
+        for mode in ("auto", "fft", "tensor", "tensor2", "tensor-inplace"):
+            B._set_options(ypass=mode)
+            assert B.current_options()["ypass"] == mode
+        for key in ("xpass", "zpass"):
+            for mode in ("tensor2", "tensor-inplace"):
+                with pytest.raises(ValueError):
+                    B._set_options(**{key: mode})
+        with pytest.raises(ValueError):
+            B._set_options(ypass="inplace")
+    finally:
+        B._set_options()
+    assert B.current_options()["ypass"] == "auto"
